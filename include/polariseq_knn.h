@@ -1,0 +1,141 @@
+/*
+ * polariseq-knn-b200: C ABI of the B200 (sm_100a) kNN-graph builder.
+ *
+ * Drop-in for the reference's NN-Descent entry points:
+ *   - Rust  polariseq_core::nndescent::nndescent_into
+ *           (crates/polariseq-core/src/nndescent.rs:688-707)
+ *   - Rust  polariseq_core::nndescent::nndescent / effective_k
+ *           (nndescent.rs:648-686)
+ *   - PyO3  _polariseq.nndescent_dense(embedding, k, max_iterations=0, seed=0,
+ *           max_candidates=0, n_trees=0, delta=0.001, out=None)
+ *           (crates/polariseq-python/src/lib.rs:503-566)
+ * A Rust `CudaBackend` (the ComputeBackend slot, crates/polariseq-core/src/
+ * backend.rs:68-94) binds these symbols through `extern "C"`; the Python
+ * package `polariseq_b200` binds them through ctypes.
+ *
+ * Plain pointers and sizes only; every function returns a pq_status.  Errors
+ * that the reference raises as panics (empty data, k == 0, short output
+ * arrays) come back as PQ_EINVAL with a message from pq_ctx_last_error().
+ */
+#ifndef POLARISEQ_KNN_H
+#define POLARISEQ_KNN_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum pq_status {
+    PQ_OK = 0,
+    PQ_EINVAL = 1,   /* bad shape / option / output size (reference: panic or ValueError) */
+    PQ_ENOMEM = 2,   /* device allocation failed */
+    PQ_EDEVICE = 3,  /* CUDA error, no device, or a kernel reported an error flag */
+    PQ_ETIMEOUT = 4, /* a bounded device-side wait gave up */
+    PQ_ENOTSUP = 5   /* option combination not supported by this build */
+} pq_status;
+
+/* Search form.  PLAIN reproduces the reference graph bit for bit. */
+enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
+/* Initial neighbour lists: the reference's RP-tree forest, or learned buckets. */
+enum { PQ_INIT_RP = 0, PQ_INIT_LEARNED = 1 };
+
+/* Mirrors NndescentOptions (nndescent.rs:42-76): zero = auto for the sized
+ * fields, resolved exactly as nndescent.rs:722-752 does. */
+typedef struct pq_nnd_opts {
+    uint64_t k;              /* neighbours per cell (reference default 15) */
+    uint64_t max_candidates; /* 0 -> min(60, 2k) */
+    uint64_t max_iterations; /* 0 -> max(5, round(log2 n)) */
+    double delta;            /* stop when changed <= delta*n*k (default 0.001) */
+    uint64_t n_trees;        /* 0 -> min(48, 8 + round(sqrt(n)/10)) */
+    uint64_t leaf_size;      /* 0 -> max(10, k) */
+    uint64_t gather_max;     /* accepted for API parity; never changes the graph */
+    uint64_t seed;
+    int32_t mode;            /* PQ_MODE_* */
+    int32_t init;            /* PQ_INIT_* */
+} pq_nnd_opts;
+
+/* Per-call statistics of the last build on a context. */
+typedef struct pq_nnd_stats {
+    int32_t rounds_run;
+    int32_t n_trees;
+    uint64_t k, max_candidates, n_iters, leaf_size, stop_at;
+    uint64_t changed[64];    /* heap entries changed per round */
+    uint64_t emitted[64];    /* join updates that passed a threshold per round */
+    uint64_t pairs[64];      /* join distances evaluated per round */
+    double ms_forest, ms_leaves, ms_rounds, ms_extract, ms_total;
+    uint64_t launches;       /* kernels launched by the last build */
+    /* With profiling on (pq_ctx_set_profiling): CUDA-event time and launch
+     * count per kernel group, indexed by PQ_KG_*. */
+    double kg_ms[16];
+    uint64_t kg_launches[16];
+} pq_nnd_stats;
+
+/* Kernel groups timed by the profiling mode. */
+enum {
+    PQ_KG_FOREST_TOP = 0,  /* top-level hyperplanes, margins and partition */
+    PQ_KG_SEQTREE = 1,     /* depth-first subtrees */
+    PQ_KG_LEAF_PAIRS = 2,  /* leaf all-pairs replay + random fill */
+    PQ_KG_CANDIDATES = 3,  /* candidate records, their sort and replay, flag flip */
+    PQ_KG_JOIN_COUNT = 4,  /* join pass 1: distances and emit bits */
+    PQ_KG_JOIN_WRITE = 5,  /* join pass 2: records in generation order */
+    PQ_KG_SORT = 6,        /* stable sort of join records by destination */
+    PQ_KG_REPLAY = 7,      /* per-destination replay of join records */
+    PQ_KG_EXTRACT = 8,     /* sorted CSR extract */
+    PQ_KG_COUNT = 9
+};
+
+typedef struct pq_ctx pq_ctx;
+
+/* Fills the reference defaults (NndescentOptions::default, nndescent.rs:64-76). */
+void pq_nnd_opts_default(pq_nnd_opts* opts);
+
+/* effective_k (nndescent.rs:648-650): k.min(n_obs - 1).max(1). */
+uint64_t pq_effective_k(uint64_t n_obs, uint64_t k);
+
+/* One context per device and caller thread; owns a stream and a device
+ * workspace that grows on demand and is reused across calls. */
+int pq_ctx_create(int device, pq_ctx** out);
+void pq_ctx_destroy(pq_ctx* ctx);
+const char* pq_ctx_last_error(const pq_ctx* ctx);
+int pq_ctx_stats(const pq_ctx* ctx, pq_nnd_stats* out);
+/* Measurement hook: when on, each kernel group of a build is bracketed by
+ * CUDA events on the context's stream (pq_nnd_stats.kg_ms / kg_launches). */
+int pq_ctx_set_profiling(pq_ctx* ctx, int on);
+
+/* nndescent_into (nndescent.rs:688-707) with HOST buffers: data is n_obs x
+ * n_dim row-major f32; indptr holds n_obs+1 entries; indices/dists hold at
+ * least n_obs * effective_k(n_obs, k).  Writes the CSR graph (Euclidean
+ * distances, ascending per row) and *nnz_out; entries past nnz untouched. */
+int pq_nndescent_into(pq_ctx* ctx, const float* data, uint64_t n_obs, uint64_t n_dim,
+                      const pq_nnd_opts* opts, uint32_t* indptr, uint64_t indptr_len,
+                      uint32_t* indices, uint64_t indices_len, float* dists,
+                      uint64_t dists_len, uint64_t* nnz_out);
+
+/* The same with DEVICE buffers on the context's device; `stream` (a
+ * cudaStream_t, may be null) is ordered before and after the build. */
+int pq_nndescent_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_obs, uint64_t n_dim,
+                             const pq_nnd_opts* opts, uint32_t* d_indptr, uint32_t* d_indices,
+                             float* d_dists, uint64_t* nnz_out, void* stream);
+
+/* Parity probe (test hook): runs the plain form up to `stop_after` (-1: after
+ * forest + random fill; r >= 0: after round r's apply) and copies the neighbour
+ * heaps (n*k idx/dist/flag) and, for r >= 0, that round's candidate heaps
+ * (n*m new/old), to HOST buffers; any pointer may be null. */
+int pq_nndescent_probe(pq_ctx* ctx, const float* data, uint64_t n_obs, uint64_t n_dim,
+                       const pq_nnd_opts* opts, int32_t stop_after, uint32_t* heap_idx,
+                       float* heap_dist, uint8_t* heap_flag, uint32_t* cand_new,
+                       uint32_t* cand_old);
+
+/* One RP tree of the forest (test hook): tree t's permutation ids (n) and its
+ * leaf ranges (2 * n_leaves, DFS order) to HOST buffers, as build_tree
+ * (nndescent.rs:643-646) with seed splitmix(opts.seed ^ (t + 1)). */
+int pq_debug_tree(pq_ctx* ctx, const float* data, uint64_t n_obs, uint64_t n_dim,
+                  const pq_nnd_opts* opts, uint32_t tree, uint32_t* ids, uint32_t* leaves,
+                  uint64_t leaves_cap, uint64_t* n_leaves);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* POLARISEQ_KNN_H */

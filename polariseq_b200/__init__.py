@@ -1,0 +1,259 @@
+"""polariseq_b200 — a B200 (sm_100a) drop-in for Polariseq's NN-Descent kNN-graph builder.
+
+Python surface of the reference's PyO3 binding
+(crates/polariseq-python/src/lib.rs:503-566)::
+
+    nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0,
+                    n_trees=0, delta=0.001, out=None) -> dict
+
+Without ``out``: ``{"indptr": u32[n+1], "indices": u32[nnz], "data": f32[nnz],
+"n_obs": n}`` — the CSR distance graph, Euclidean distances ascending per row.
+With ``out=(indptr, indices, data)`` the graph is written in place and
+``{"nnz", "n_obs"}`` is returned; entries past nnz are left untouched.  A bad
+``out`` raises ``ValueError`` with the reference's message; inputs on which the
+reference core panics (empty data, ``k == 0``) raise :class:`PanicException`,
+as PyO3 turns the core's panic into ``pyo3_runtime.PanicException``.
+
+Every call runs on the GPU through the C ABI (include/polariseq_knn.h); the
+GIL is released for the whole build (ctypes drops it around foreign calls).
+"""
+
+from __future__ import annotations
+
+import ctypes as C
+import threading
+
+import numpy as np
+
+from . import _lib
+
+__all__ = [
+    "PanicException", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
+]
+
+
+class PanicException(BaseException):
+    """Raised where the reference core panics (pyo3_runtime.PanicException
+    also derives from BaseException)."""
+
+
+class DeviceError(RuntimeError):
+    pass
+
+
+def effective_k(n_obs: int, k: int) -> int:
+    """Neighbours per row the graph can hold (nndescent.rs:648-650)."""
+    return int(_lib.load().pq_effective_k(int(n_obs), int(k)))
+
+
+def _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size=0, gather_max=0,
+          mode=_lib.PQ_MODE_PLAIN, init=_lib.PQ_INIT_RP) -> _lib.NndOpts:
+    o = _lib.NndOpts()
+    _lib.load().pq_nnd_opts_default(C.byref(o))
+    o.k = int(k)
+    o.max_iterations = int(max_iterations)
+    o.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
+    o.max_candidates = int(max_candidates)
+    o.n_trees = int(n_trees)
+    o.delta = float(delta)
+    o.leaf_size = int(leaf_size)
+    o.gather_max = int(gather_max)
+    o.mode = int(mode)
+    o.init = int(init)
+    return o
+
+
+class Context:
+    """One device context: a CUDA stream plus a device workspace reused
+    across calls.  Calls on one context are serialised."""
+
+    def __init__(self, device: int = 0):
+        L = _lib.load()
+        h = C.c_void_p()
+        rc = L.pq_ctx_create(int(device), C.byref(h))
+        if rc != _lib.PQ_OK:
+            raise DeviceError(f"pq_ctx_create(device={device}) failed with status {rc}; "
+                              "a CUDA device is required (there is no CPU fallback)")
+        self._h = h
+        self.device = device
+        self._lock = threading.Lock()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            _lib.load().pq_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int, what: str) -> None:
+        if rc == _lib.PQ_OK:
+            return
+        msg = _lib.load().pq_ctx_last_error(self._h).decode(errors="replace")
+        if rc == _lib.PQ_EINVAL:
+            raise PanicException(f"{what}: {msg}")
+        if rc == _lib.PQ_ENOTSUP:
+            raise NotImplementedError(f"{what}: {msg}")
+        if rc == _lib.PQ_ENOMEM:
+            raise MemoryError(f"{what}: {msg}")
+        raise DeviceError(f"{what} failed (status {rc}): {msg}")
+
+    def stats(self) -> dict:
+        s = _lib.NndStats()
+        self._check(_lib.load().pq_ctx_stats(self._h, C.byref(s)), "stats")
+        r = s.rounds_run
+        return {
+            "rounds_run": r, "n_trees": s.n_trees, "k": s.k, "max_candidates": s.max_candidates,
+            "n_iters": s.n_iters, "leaf_size": s.leaf_size, "stop_at": s.stop_at,
+            "changed": list(s.changed[:r]), "emitted": list(s.emitted[:r]),
+            "pairs": list(s.pairs[:r]), "ms_forest": s.ms_forest, "ms_leaves": s.ms_leaves,
+            "ms_rounds": s.ms_rounds, "ms_extract": s.ms_extract, "ms_total": s.ms_total,
+        }
+
+    # -- host-buffer build (the drop-in) ------------------------------------
+    def nndescent_into(self, data: np.ndarray, opts: _lib.NndOpts, indptr: np.ndarray,
+                       indices: np.ndarray, dists: np.ndarray) -> int:
+        n, d = data.shape
+        nnz = C.c_uint64(0)
+        with self._lock:
+            rc = _lib.load().pq_nndescent_into(
+                self._h, data.ctypes.data, n, d, C.byref(opts), indptr.ctypes.data, indptr.size,
+                indices.ctypes.data, indices.size, dists.ctypes.data, dists.size, C.byref(nnz))
+            self._check(rc, "nndescent")
+        return int(nnz.value)
+
+    # -- device-buffer build (torch CUDA tensors) ---------------------------
+    def nndescent_device(self, data, opts: _lib.NndOpts, indptr, indices, dists,
+                         stream=None) -> int:
+        """`data`, `indptr`, `indices`, `dists`: contiguous CUDA tensors
+        (float32 [n,d], int32/uint32 [n+1], [>= n*k], float32 [>= n*k])."""
+        n, d = int(data.shape[0]), int(data.shape[1])
+        nnz = C.c_uint64(0)
+        sp = None if stream is None else C.c_void_p(int(stream))
+        with self._lock:
+            rc = _lib.load().pq_nndescent_into_device(
+                self._h, data.data_ptr(), n, d, C.byref(opts), indptr.data_ptr(),
+                indices.data_ptr(), dists.data_ptr(), C.byref(nnz), sp)
+            self._check(rc, "nndescent_device")
+        return int(nnz.value)
+
+    # -- parity probes (test hooks) ----------------------------------------
+    def probe(self, data: np.ndarray, opts: _lib.NndOpts, stop_after: int) -> dict:
+        data = np.ascontiguousarray(data, np.float32)
+        n, d = data.shape
+        k = effective_k(n, opts.k)
+        m = max(1, opts.max_candidates if opts.max_candidates > 0 else min(2 * k, 60))
+        hi = np.zeros((n, k), np.uint32)
+        hd = np.zeros((n, k), np.float32)
+        hf = np.zeros((n, k), np.uint8)
+        cn = np.zeros((n, m), np.uint32)
+        co = np.zeros((n, m), np.uint32)
+        with self._lock:
+            rc = _lib.load().pq_nndescent_probe(
+                self._h, data.ctypes.data, n, d, C.byref(opts), int(stop_after), hi.ctypes.data,
+                hd.ctypes.data, hf.ctypes.data, cn.ctypes.data, co.ctypes.data)
+            self._check(rc, "probe")
+        return {"heap_idx": hi, "heap_dist": hd, "heap_flag": hf, "cand_new": cn,
+                "cand_old": co}
+
+    def debug_tree(self, data: np.ndarray, opts: _lib.NndOpts, tree: int):
+        data = np.ascontiguousarray(data, np.float32)
+        n, d = data.shape
+        ids = np.zeros(n, np.uint32)
+        cap = n + 1
+        leaves = np.zeros(2 * cap, np.uint32)
+        nl = C.c_uint64(0)
+        with self._lock:
+            rc = _lib.load().pq_debug_tree(self._h, data.ctypes.data, n, d, C.byref(opts),
+                                           int(tree), ids.ctypes.data, leaves.ctypes.data, cap,
+                                           C.byref(nl))
+            self._check(rc, "debug_tree")
+        return ids, leaves[: 2 * nl.value].reshape(-1, 2).copy()
+
+
+_default: dict[int, Context] = {}
+_default_lock = threading.Lock()
+
+
+def default_context(device: int = 0) -> Context:
+    with _default_lock:
+        ctx = _default.get(device)
+        if ctx is None:
+            ctx = Context(device)
+            _default[device] = ctx
+        return ctx
+
+
+def _as_embedding(embedding) -> np.ndarray:
+    a = embedding
+    if not isinstance(a, np.ndarray):
+        raise TypeError("argument 'embedding': expected a numpy.ndarray of float32")
+    if a.ndim != 2:
+        raise TypeError(f"argument 'embedding': expected a 2-D array, got {a.ndim}-D")
+    if a.dtype != np.float32:
+        raise TypeError(f"argument 'embedding': expected float32, got {a.dtype}")
+    # read in place when contiguous, else copy (lib.rs:526-533)
+    return a if a.flags["C_CONTIGUOUS"] else np.ascontiguousarray(a)
+
+
+def _as_out(arr, dtype, name):
+    if not isinstance(arr, np.ndarray) or arr.ndim != 1 or arr.dtype != dtype:
+        raise TypeError(f"out: '{name}' must be a 1-D numpy array of {np.dtype(dtype).name}")
+    if not arr.flags["C_CONTIGUOUS"] or not arr.flags["WRITEABLE"]:
+        raise TypeError(f"out: '{name}' must be contiguous and writeable")
+    return arr
+
+
+def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_trees=0,
+                    delta=0.001, out=None, *, device: int = 0):
+    """Approximate kNN graph by NN-Descent, bit-exact with the reference
+    (crates/polariseq-python/src/lib.rs:503-566)."""
+    emb = _as_embedding(embedding)
+    n_obs, _ = emb.shape
+    opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta)
+    cap = n_obs * effective_k(n_obs, k)
+    # the same order as the binding: the out sizes are validated (ValueError)
+    # before the core runs and panics on empty data or k == 0
+    if out is not None:
+        ip, ix, dx = out
+        ip = _as_out(ip, np.uint32, "indptr")
+        ix = _as_out(ix, np.uint32, "indices")
+        dx = _as_out(dx, np.float32, "data")
+        if ip.size != n_obs + 1 or ix.size < cap or dx.size < cap:
+            raise ValueError(f"outputs must hold {n_obs + 1} row pointers and {cap} neighbours")
+    if n_obs == 0 or emb.shape[1] == 0:
+        raise PanicException("empty data")
+    if int(k) == 0:
+        raise PanicException("k must be >= 1")
+    ctx = default_context(device)
+    if out is not None:
+        nnz = ctx.nndescent_into(emb, opts, ip, ix, dx)
+        return {"nnz": nnz, "n_obs": n_obs}
+    ip = np.zeros(n_obs + 1, np.uint32)
+    ix = np.zeros(cap, np.uint32)
+    dx = np.zeros(cap, np.float32)
+    nnz = ctx.nndescent_into(emb, opts, ip, ix, dx)
+    return {"indptr": ip, "indices": ix[:nnz], "data": dx[:nnz], "n_obs": n_obs}
+
+
+def nndescent(data: np.ndarray, k: int = 15, *, max_candidates=0, max_iterations=0, delta=0.001,
+              n_trees=0, leaf_size=0, gather_max=0, seed=0, device: int = 0) -> dict:
+    """The Rust-level ``nndescent(data, n_obs, n_dim, &NndescentOptions)``
+    (nndescent.rs:657-686) with every option, returning the NeighborGraph
+    fields (indptr, indices, data, n_obs)."""
+    emb = _as_embedding(data)
+    n_obs = emb.shape[0]
+    if n_obs == 0 or emb.shape[1] == 0:
+        raise PanicException("empty data")
+    if int(k) == 0:
+        raise PanicException("k must be >= 1")
+    opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size, gather_max)
+    cap = n_obs * effective_k(n_obs, k)
+    ip = np.zeros(n_obs + 1, np.uint32)
+    ix = np.zeros(cap, np.uint32)
+    dx = np.zeros(cap, np.float32)
+    nnz = default_context(device).nndescent_into(emb, opts, ip, ix, dx)
+    return {"indptr": ip, "indices": ix[:nnz], "data": dx[:nnz], "n_obs": n_obs}

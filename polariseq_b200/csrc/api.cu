@@ -1,0 +1,723 @@
+// C ABI and host driver of the kNN-graph builder (include/polariseq_knn.h).
+//
+// The driver resolves NndescentOptions exactly as the reference does
+// (crates/polariseq-core/src/nndescent.rs:708-752), pads the embedding to
+// 16-byte rows in HBM, then runs the plain form's phases on the context's
+// stream: RP forest, leaf pairs, random fill, rounds, extract.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/polariseq_knn.h"
+#include "common.cuh"
+#include "kernels.cuh"
+#include "primitives.cuh"
+
+namespace pq {
+unsigned long long g_launches = 0;
+}
+
+namespace {
+
+struct Buf {
+    void* p = nullptr;
+    size_t bytes = 0;
+};
+
+struct Resolved {
+    uint64_t k, max_cand, n_iters, n_trees, leaf_size, stop_at;
+};
+
+}  // namespace
+
+struct pq_ctx {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::string err;
+    pq_nnd_stats stats{};
+    std::map<std::string, Buf> bufs;
+    int* d_err = nullptr;
+    uint64_t* d_u64 = nullptr;            // small device scalars
+    unsigned long long* d_acc = nullptr;  // device accumulators
+    int profile = 0;
+    struct KGRec {
+        cudaEvent_t a, b;
+        int group;
+        unsigned long long launches;
+    };
+    std::vector<KGRec> kg_pending;
+
+    template <class T>
+    T* get(const std::string& name, size_t count) {
+        size_t need = count * sizeof(T);
+        if (need == 0) need = 16;
+        Buf& b = bufs[name];
+        if (b.bytes < need) {
+            if (b.p) {
+                cudaStreamSynchronize(stream);
+                cudaFree(b.p);
+                b.p = nullptr;
+                b.bytes = 0;
+            }
+            size_t alloc = need + need / 8;  // headroom for slightly larger calls
+            if (cudaMalloc(&b.p, alloc) != cudaSuccess) {
+                cudaGetLastError();
+                throw std::string("device allocation of ") + std::to_string(alloc) +
+                    " bytes failed (" + name + ")";
+            }
+            b.bytes = alloc;
+        }
+        return static_cast<T*>(b.p);
+    }
+};
+
+namespace {
+
+struct DeviceError {
+    std::string msg;
+};
+
+void ck(cudaError_t e, const char* where) {
+    if (e != cudaSuccess) throw DeviceError{std::string(where) + ": " + cudaGetErrorString(e)};
+}
+
+uint64_t effective_k(uint64_t n, uint64_t k) {
+    uint64_t m = n > 0 ? n - 1 : 0;
+    uint64_t e = k < m ? k : m;
+    return e > 0 ? e : 1;
+}
+
+Resolved resolve(uint64_t n, const pq_nnd_opts& o) {
+    Resolved r;
+    r.k = effective_k(n, o.k);
+    uint64_t mc = o.max_candidates > 0 ? o.max_candidates : std::min<uint64_t>(2 * r.k, 60);
+    r.max_cand = mc > 0 ? mc : 1;
+    if (o.max_iterations > 0) {
+        r.n_iters = o.max_iterations;
+    } else {
+        double lg = std::round(std::log2(double(n)));
+        uint64_t it = lg > 0 ? uint64_t(lg) : 0;
+        r.n_iters = it > 5 ? it : 5;
+    }
+    if (o.n_trees > 0) {
+        r.n_trees = o.n_trees;
+    } else {
+        double t = std::round(std::sqrt(double(n)) / 10.0);
+        r.n_trees = std::min<uint64_t>(8 + uint64_t(t), 48);
+    }
+    r.leaf_size = o.leaf_size > 0 ? o.leaf_size : std::max<uint64_t>(r.k, 10);
+    double sa = o.delta * double(n) * double(r.k);
+    r.stop_at = (sa > 0 && sa == sa) ? (sa >= 1.8e19 ? UINT64_MAX : uint64_t(sa)) : 0;
+    return r;
+}
+
+int key_bits(uint64_t maxkey) {
+    int b = 0;
+    while (b < 32 && (maxkey >> b) != 0) ++b;
+    return b > 0 ? b : 1;
+}
+
+__global__ void k_fill_u32(uint32_t* p, size_t n, uint32_t v) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+__global__ void k_fill_f32(float* p, size_t n, float v) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) p[i] = v;
+}
+__global__ void k_iota_trees(uint32_t* ids, uint32_t n, uint32_t T) {
+    size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < size_t(n) * T) ids[i] = uint32_t(i % n);
+}
+
+unsigned blocks(size_t n, int t) { return unsigned((n + t - 1) / t); }
+
+struct Timer {
+    cudaEvent_t a, b;
+    cudaStream_t s;
+    explicit Timer(cudaStream_t st) : s(st) {
+        cudaEventCreate(&a);
+        cudaEventCreate(&b);
+    }
+    ~Timer() {
+        cudaEventDestroy(a);
+        cudaEventDestroy(b);
+    }
+    void start() { cudaEventRecord(a, s); }
+    double stop() {
+        cudaEventRecord(b, s);
+        cudaEventSynchronize(b);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, a, b);
+        return ms;
+    }
+};
+
+// Brackets one kernel group with CUDA events on the context's stream when
+// profiling is on; the records are summed into the stats at the end.
+struct KGScope {
+    pq_ctx* c;
+    int g;
+    cudaEvent_t a{}, b{};
+    unsigned long long l0;
+    KGScope(pq_ctx* c_, int g_) : c(c_), g(g_), l0(pq::g_launches) {
+        if (c->profile) {
+            cudaEventCreate(&a);
+            cudaEventCreate(&b);
+            cudaEventRecord(a, c->stream);
+        }
+    }
+    ~KGScope() {
+        if (c->profile) {
+            cudaEventRecord(b, c->stream);
+            c->kg_pending.push_back({a, b, g, pq::g_launches - l0});
+        }
+    }
+};
+
+void kg_collect(pq_ctx* c) {
+    cudaStreamSynchronize(c->stream);
+    for (auto& r : c->kg_pending) {
+        float ms = 0;
+        cudaEventElapsedTime(&ms, r.a, r.b);
+        c->stats.kg_ms[r.group] += ms;
+        c->stats.kg_launches[r.group] += r.launches;
+        cudaEventDestroy(r.a);
+        cudaEventDestroy(r.b);
+    }
+    c->kg_pending.clear();
+}
+
+// Host-side probe destinations.
+struct Probe {
+    int32_t stop_after = -2;
+    uint32_t* heap_idx = nullptr;
+    float* heap_dist = nullptr;
+    uint8_t* heap_flag = nullptr;
+    uint32_t* cand_new = nullptr;
+    uint32_t* cand_old = nullptr;
+    int32_t tree = -1;  // pq_debug_tree: stop after the forest and copy this tree
+    uint32_t* tree_ids = nullptr;
+    uint32_t* tree_leaves = nullptr;
+    uint64_t leaves_cap = 0;
+    uint64_t* n_leaves = nullptr;
+    bool done = false;
+};
+
+// The plain form on device data.  Returns nnz (outputs written) unless the
+// probe stopped early.
+uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64, uint64_t d64,
+                     const pq_nnd_opts& o, uint32_t* d_indptr, uint32_t* d_indices,
+                     float* d_dists, Probe* probe) {
+    using namespace pq;
+    cudaStream_t st = c->stream;
+    const Resolved R = resolve(n64, o);
+    const uint32_t n = uint32_t(n64);
+    const int d = int(d64), dp = int((d64 + 3) / 4 * 4);
+    const int k = int(R.k), m = int(R.max_cand);
+    const uint32_t T = uint32_t(R.n_trees);
+    const uint64_t seed = o.seed;
+    pq_nnd_stats& S = c->stats;
+    std::memset(&S, 0, sizeof(S));
+    S.n_trees = int32_t(T);
+    S.k = R.k;
+    S.max_candidates = R.max_cand;
+    S.n_iters = R.n_iters;
+    S.leaf_size = R.leaf_size;
+    S.stop_at = R.stop_at;
+    Timer tm(st), tot(st);
+    tot.start();
+    const unsigned long long launches0 = g_launches;
+
+    // padded rows
+    float* X = c->get<float>("X", size_t(n) * dp);
+    if (dp != d) ck(cudaMemsetAsync(X, 0, size_t(n) * dp * sizeof(float), st), "memset X");
+    ck(cudaMemcpy2DAsync(X, size_t(dp) * sizeof(float), data, size_t(d) * sizeof(float),
+                         size_t(d) * sizeof(float), n,
+                         data_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st),
+       "copy embedding");
+
+    // heaps
+    uint32_t* hidx = c->get<uint32_t>("hidx", size_t(n) * k);
+    float* hdist = c->get<float>("hdist", size_t(n) * k);
+    uint8_t* hflag = c->get<uint8_t>("hflag", size_t(n) * k);
+    k_fill_u32<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(hidx, size_t(n) * k, PQ_EMPTY); count_launch();
+    k_fill_f32<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(hdist, size_t(n) * k,
+                                                           __builtin_huge_valf()); count_launch();
+    ck(cudaMemsetAsync(hflag, 0, size_t(n) * k, st), "memset flags");
+    ck(cudaMemsetAsync(c->d_err, 0, sizeof(int), st), "memset err");
+
+    // ── forest ──
+    tm.start();
+    const size_t TN = size_t(T) * n;
+    ForestArgs fa;
+    fa.X = X;
+    fa.d = d;
+    fa.dp = dp;
+    fa.n = n;
+    fa.leaf_size = uint32_t(std::min<uint64_t>(R.leaf_size, 0xFFFFFFFFull));
+    fa.ids = c->get<uint32_t>("ids", TN);
+    fa.tmp = c->get<uint32_t>("tmp", TN);
+    fa.side = c->get<uint8_t>("side", TN);
+    fa.tabA = c->get<uint32_t>("tabA", TN);
+    fa.tabB = c->get<uint32_t>("tabB", TN);
+    fa.leafflag = c->get<uint8_t>("leafflag", TN);
+    fa.err = c->d_err;
+    k_iota_trees<<<blocks(TN, 256), 256, 0, st>>>(fa.ids, n, T); count_launch();
+    ck(cudaMemsetAsync(fa.leafflag, 0, TN, st), "memset leafflag");
+
+    std::vector<PNode> cur;
+    for (uint32_t t = 0; t < T; ++t) {
+        PNode nd{};
+        nd.tree = t;
+        nd.start = 0;
+        nd.size = n;
+        nd.depth = 0;
+        nd.seed = splitmix(seed ^ (uint64_t(t) + 1));
+        cur.push_back(nd);
+    }
+    std::vector<SRoot> roots;
+    while (!cur.empty()) {
+        std::vector<PNode> act;
+        for (const PNode& nd : cur) {
+            if (nd.size < 8192 || nd.depth >= 6)
+                roots.push_back(SRoot{nd.tree, nd.start, nd.size, nd.depth, nd.seed});
+            else
+                act.push_back(nd);
+        }
+        if (act.empty()) break;
+        std::vector<uint32_t> chunk_node;
+        for (uint32_t i = 0; i < act.size(); ++i) {
+            act[i].chunk0 = uint32_t(chunk_node.size());
+            uint32_t nch = (act[i].size + FOREST_CHUNK - 1) / FOREST_CHUNK;
+            for (uint32_t q = 0; q < nch; ++q) chunk_node.push_back(i);
+        }
+        const uint32_t nn = uint32_t(act.size()), nch = uint32_t(chunk_node.size());
+        PNode* d_nodes = c->get<PNode>("pnodes", nn);
+        uint32_t* d_cn = c->get<uint32_t>("chunk_node", nch);
+        uint32_t* d_cl = c->get<uint32_t>("chunkL", nch);
+        float* d_norm = c->get<float>("normals", size_t(nn) * dp);
+        ck(cudaMemcpyAsync(d_nodes, act.data(), nn * sizeof(PNode), cudaMemcpyHostToDevice, st),
+           "upload nodes");
+        ck(cudaMemcpyAsync(d_cn, chunk_node.data(), nch * sizeof(uint32_t),
+                           cudaMemcpyHostToDevice, st),
+           "upload chunks");
+        {
+            KGScope kg(c, PQ_KG_FOREST_TOP);
+            launch_hyperplanes(fa, d_nodes, nn, d_norm, st);
+            launch_sides(fa, d_nodes, d_cn, nch, d_norm, d_cl, st);
+            launch_node_scan(d_nodes, nn, d_cl, st);
+            launch_partition(fa, d_nodes, d_cn, nch, d_cl, st);
+            launch_degenerate(fa, d_nodes, nn, st);
+        }
+        ck(cudaMemcpyAsync(act.data(), d_nodes, nn * sizeof(PNode), cudaMemcpyDeviceToHost, st),
+           "download nodes");
+        ck(cudaStreamSynchronize(st), "forest level");
+        cur.clear();
+        for (const PNode& nd : act) {
+            PNode l{}, r{};
+            l.tree = r.tree = nd.tree;
+            l.depth = r.depth = nd.depth + 1;
+            l.start = nd.start;
+            l.size = nd.nL;
+            l.seed = splitmix(nd.seed ^ 1ull);
+            r.start = nd.start + nd.nL;
+            r.size = nd.size - nd.nL;
+            r.seed = splitmix(nd.seed ^ 2ull);
+            cur.push_back(l);
+            cur.push_back(r);
+        }
+    }
+    {
+        SRoot* d_roots = c->get<SRoot>("sroots", roots.size());
+        ck(cudaMemcpyAsync(d_roots, roots.data(), roots.size() * sizeof(SRoot),
+                           cudaMemcpyHostToDevice, st),
+           "upload roots");
+        KGScope kg(c, PQ_KG_SEQTREE);
+        launch_seqtrees(fa, d_roots, uint32_t(roots.size()), st);
+        ck(cudaGetLastError(), "seqtrees");
+    }
+    int herr = 0;
+    ck(cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "err");
+    S.ms_forest = tm.stop();
+    if (herr) throw DeviceError{"forest: a subtree exceeded the depth-first stack"};
+
+    if (probe && probe->tree >= 0) {
+        uint32_t t = uint32_t(probe->tree);
+        std::vector<uint8_t> lf(n);
+        ck(cudaMemcpy(probe->tree_ids, fa.ids + size_t(t) * n, size_t(n) * 4,
+                      cudaMemcpyDeviceToHost),
+           "tree ids");
+        ck(cudaMemcpy(lf.data(), fa.leafflag + size_t(t) * n, n, cudaMemcpyDeviceToHost),
+           "tree leaves");
+        uint64_t nl = 0;
+        std::vector<uint32_t> starts;
+        for (uint32_t i = 0; i < n; ++i)
+            if (lf[i]) starts.push_back(i);
+        nl = starts.size();
+        if (nl <= probe->leaves_cap)
+            for (uint64_t q = 0; q < nl; ++q) {
+                probe->tree_leaves[2 * q] = starts[q];
+                probe->tree_leaves[2 * q + 1] = q + 1 < nl ? starts[q + 1] : n;
+            }
+        *probe->n_leaves = nl;
+        probe->done = true;
+        return 0;
+    }
+
+    // ── leaf pairs, one tree after another ──
+    tm.start();
+    {
+        uint32_t* leaf_start = fa.tabA;  // reused: the forest scratch is free now
+        uint32_t* scanbuf = fa.tabB;
+        void* stemp = c->get<uint8_t>("scan_temp", scan_temp_bytes(n));
+        uint64_t* cnts = c->get<uint64_t>("leaf_counts", T);
+        for (uint32_t t = 0; t < T; ++t)
+            launch_leaf_compact(fa.leafflag + size_t(t) * n, n, leaf_start + size_t(t) * n,
+                                scanbuf + size_t(t) * n, stemp, cnts + t, st);
+        std::vector<uint64_t> hc(T);
+        ck(cudaMemcpyAsync(hc.data(), cnts, T * sizeof(uint64_t), cudaMemcpyDeviceToHost, st),
+           "leaf counts");
+        ck(cudaStreamSynchronize(st), "leaf compact");
+        KGScope kg(c, PQ_KG_LEAF_PAIRS);
+        for (uint32_t t = 0; t < T; ++t)
+            launch_leaf_pairs(X, d, dp, fa.ids + size_t(t) * n, leaf_start + size_t(t) * n,
+                              uint32_t(hc[t]), n, k, hidx, hdist, hflag, st);
+        launch_random_fill(X, d, dp, n, k, seed, hidx, hdist, hflag, st);
+        ck(cudaGetLastError(), "leaf pairs");
+    }
+    S.ms_leaves = tm.stop();
+
+    auto copy_heaps = [&]() {
+        if (probe->heap_idx)
+            ck(cudaMemcpy(probe->heap_idx, hidx, size_t(n) * k * 4, cudaMemcpyDeviceToHost), "p");
+        if (probe->heap_dist)
+            ck(cudaMemcpy(probe->heap_dist, hdist, size_t(n) * k * 4, cudaMemcpyDeviceToHost), "p");
+        if (probe->heap_flag)
+            ck(cudaMemcpy(probe->heap_flag, hflag, size_t(n) * k, cudaMemcpyDeviceToHost), "p");
+    };
+    if (probe && probe->stop_after == -1) {
+        ck(cudaStreamSynchronize(st), "probe");
+        copy_heaps();
+        probe->done = true;
+        return 0;
+    }
+
+    // ── rounds ──
+    tm.start();
+    uint32_t* new_idx = c->get<uint32_t>("new_idx", size_t(n) * m);
+    float* new_prio = c->get<float>("new_prio", size_t(n) * m);
+    uint32_t* old_idx = c->get<uint32_t>("old_idx", size_t(n) * m);
+    float* old_prio = c->get<float>("old_prio", size_t(n) * m);
+    uint32_t* dcnt = c->get<uint32_t>("dcnt", n);
+    uint32_t* seg_off = c->get<uint32_t>("seg_off", n);
+    uint32_t* row_cnt = c->get<uint32_t>("row_cnt", n);
+    const int words = (4 * m * m + 31) / 32;
+    uint32_t* bits = c->get<uint32_t>("bits", size_t(n) * words);
+    void* stemp = c->get<uint8_t>("scan_temp", scan_temp_bytes(n));
+    const size_t nrec_c = 2 * size_t(n) * k;
+    for (uint64_t iter = 0; iter < R.n_iters; ++iter) {
+        // candidates
+        uint32_t* ck_ = c->get<uint32_t>("ckeys", nrec_c);
+        uint64_t* cv = c->get<uint64_t>("cvals", nrec_c);
+        uint32_t* ck2 = c->get<uint32_t>("ckeys2", nrec_c);
+        uint64_t* cv2 = c->get<uint64_t>("cvals2", nrec_c);
+        void* rtemp = c->get<uint8_t>("radix_temp_c", radix_temp_bytes(nrec_c));
+        {
+            KGScope kg(c, PQ_KG_CANDIDATES);
+            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
+            launch_cand_gen(hidx, hflag, n, k, seed, uint32_t(iter), ck_, cv, dcnt, st);
+            ck(radix_sort_pairs(ck_, cv, ck2, cv2, nrec_c, key_bits(n), rtemp, st), "sort cand");
+            ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan cand");
+            launch_cand_apply(ck_, cv, seg_off, dcnt, n, m, new_idx, new_prio, old_idx, old_prio,
+                              st);
+            launch_flag_flip(hidx, hflag, new_idx, n, k, m, st);
+        }
+        // join
+        ck(cudaMemsetAsync(c->d_acc, 0, 2 * sizeof(unsigned long long), st), "memset acc");
+        {
+            KGScope kg(c, PQ_KG_JOIN_COUNT);
+            launch_join_count(X, d, dp, n, k, m, hdist, new_idx, old_idx, bits, words, row_cnt,
+                              c->d_acc, st);
+        }
+        uint32_t* row_off = seg_off;  // free until the replay's segments are computed
+        ck(scan_exclusive_u32(row_cnt, row_off, n, stemp, c->d_u64, st), "scan join");
+        uint64_t total = 0;
+        ck(cudaMemcpyAsync(&total, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "total");
+        ck(cudaStreamSynchronize(st), "join count");
+        if (total >= 0xFFFFFFFFull) throw DeviceError{"join: more than 2^32 updates in a round"};
+        uint64_t changed = 0;
+        if (total > 0) {
+            uint32_t* jk = c->get<uint32_t>("jkeys", total);
+            uint64_t* jv = c->get<uint64_t>("jvals", total);
+            uint32_t* jk2 = c->get<uint32_t>("jkeys2", total);
+            uint64_t* jv2 = c->get<uint64_t>("jvals2", total);
+            void* rtj = c->get<uint8_t>("radix_temp_j", radix_temp_bytes(total));
+            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
+            {
+                KGScope kg(c, PQ_KG_JOIN_WRITE);
+                launch_join_write(X, d, dp, n, m, new_idx, old_idx, bits, words, row_off, jk, jv,
+                                  dcnt, st);
+            }
+            {
+                KGScope kg(c, PQ_KG_SORT);
+                ck(radix_sort_pairs(jk, jv, jk2, jv2, total, key_bits(n > 1 ? n - 1 : 1), rtj,
+                                    st),
+                   "sort join");
+                ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan replay");
+            }
+            {
+                KGScope kg(c, PQ_KG_REPLAY);
+                launch_replay(jk, jv, seg_off, dcnt, n, k, hidx, hdist, hflag, c->d_acc + 1, st);
+            }
+        }
+        unsigned long long acc[2];
+        ck(cudaMemcpyAsync(acc, c->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st), "acc");
+        ck(cudaStreamSynchronize(st), "round");
+        changed = acc[1];
+        if (iter < 64) {
+            S.changed[iter] = changed;
+            S.emitted[iter] = total;
+            S.pairs[iter] = acc[0];
+        }
+        S.rounds_run = int32_t(iter + 1);
+        if (probe && probe->stop_after == int32_t(iter)) {
+            copy_heaps();
+            if (probe->cand_new)
+                ck(cudaMemcpy(probe->cand_new, new_idx, size_t(n) * m * 4,
+                              cudaMemcpyDeviceToHost),
+                   "p");
+            if (probe->cand_old)
+                ck(cudaMemcpy(probe->cand_old, old_idx, size_t(n) * m * 4,
+                              cudaMemcpyDeviceToHost),
+                   "p");
+            probe->done = true;
+            return 0;
+        }
+        if (changed <= R.stop_at) break;
+    }
+    S.ms_rounds = tm.stop();
+
+    // ── extract ──
+    tm.start();
+    uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
+    uint32_t* eoff = c->get<uint32_t>("eoff", n);
+    {
+        KGScope kg(c, PQ_KG_EXTRACT);
+        launch_extract_count(hidx, n, k, ecnt, st);
+        ck(scan_exclusive_u32(ecnt, eoff, n, stemp, c->d_u64, st), "scan extract");
+        launch_extract(hidx, hdist, n, k, eoff, d_indptr, d_indices, d_dists, st);
+    }
+    uint64_t nnz = 0;
+    ck(cudaMemcpyAsync(&nnz, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "nnz");
+    ck(cudaStreamSynchronize(st), "extract");
+    S.ms_extract = tm.stop();
+    S.ms_total = tot.stop();
+    S.launches = g_launches - launches0;
+    kg_collect(c);
+    if (probe) {
+        copy_heaps();
+        probe->done = true;
+    }
+    return nnz;
+}
+
+int fail(pq_ctx* c, int code, const std::string& msg) {
+    if (c) c->err = msg;
+    return code;
+}
+
+int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
+    if (!c) return PQ_EINVAL;
+    if (!o) return fail(c, PQ_EINVAL, "options pointer is null");
+    if (n == 0 || d == 0) return fail(c, PQ_EINVAL, "empty data");  // nndescent.rs:708
+    if (o->k == 0) return fail(c, PQ_EINVAL, "k must be >= 1");      // nndescent.rs:709
+    if (n >= 0xFFFFFFFEull) return fail(c, PQ_EINVAL, "n_obs must be below 2^32 - 1");
+    if (d > 65536) return fail(c, PQ_EINVAL, "n_dim above 65536 is not supported");
+    Resolved R = resolve(n, *o);
+    if (2 * n * R.k >= 0xFFFFFFFFull)
+        return fail(c, PQ_EINVAL, "n_obs * k must be below 2^31");
+    if (R.n_trees * n > (uint64_t(1) << 36))
+        return fail(c, PQ_EINVAL, "n_trees * n_obs is too large");
+    if (o->mode != PQ_MODE_PLAIN || o->init != PQ_INIT_RP)
+        return fail(c, PQ_ENOTSUP, "only the plain form with RP init is available on this entry");
+    return PQ_OK;
+}
+
+template <class F>
+int guarded(pq_ctx* c, F&& f) {
+    try {
+        if (cudaSetDevice(c->device) != cudaSuccess)
+            return fail(c, PQ_EDEVICE, "cudaSetDevice failed");
+        return f();
+    } catch (const DeviceError& e) {
+        cudaGetLastError();
+        return fail(c, PQ_EDEVICE, e.msg);
+    } catch (const std::string& s) {
+        cudaGetLastError();
+        return fail(c, PQ_ENOMEM, s);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+void pq_nnd_opts_default(pq_nnd_opts* o) {
+    if (!o) return;
+    std::memset(o, 0, sizeof(*o));
+    o->k = 15;
+    o->delta = 0.001;
+    o->mode = PQ_MODE_PLAIN;
+    o->init = PQ_INIT_RP;
+}
+
+uint64_t pq_effective_k(uint64_t n_obs, uint64_t k) { return effective_k(n_obs, k); }
+
+int pq_ctx_create(int device, pq_ctx** out) {
+    if (!out) return PQ_EINVAL;
+    *out = nullptr;
+    int nd = 0;
+    if (cudaGetDeviceCount(&nd) != cudaSuccess || nd == 0) {
+        cudaGetLastError();
+        return PQ_EDEVICE;
+    }
+    if (device < 0 || device >= nd) return PQ_EINVAL;
+    if (cudaSetDevice(device) != cudaSuccess) return PQ_EDEVICE;
+    pq_ctx* c = new pq_ctx();
+    c->device = device;
+    if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&c->d_u64, 8 * sizeof(uint64_t)) != cudaSuccess ||
+        cudaMalloc(&c->d_acc, 8 * sizeof(unsigned long long)) != cudaSuccess) {
+        cudaGetLastError();
+        pq_ctx_destroy(c);
+        return PQ_EDEVICE;
+    }
+    *out = c;
+    return PQ_OK;
+}
+
+void pq_ctx_destroy(pq_ctx* c) {
+    if (!c) return;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto& kv : c->bufs)
+        if (kv.second.p) cudaFree(kv.second.p);
+    if (c->d_err) cudaFree(c->d_err);
+    if (c->d_u64) cudaFree(c->d_u64);
+    if (c->d_acc) cudaFree(c->d_acc);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+}
+
+const char* pq_ctx_last_error(const pq_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int pq_ctx_set_profiling(pq_ctx* c, int on) {
+    if (!c) return PQ_EINVAL;
+    c->profile = on ? 1 : 0;
+    return PQ_OK;
+}
+
+int pq_ctx_stats(const pq_ctx* c, pq_nnd_stats* out) {
+    if (!c || !out) return PQ_EINVAL;
+    *out = c->stats;
+    return PQ_OK;
+}
+
+int pq_nndescent_into(pq_ctx* c, const float* data, uint64_t n, uint64_t d,
+                      const pq_nnd_opts* o, uint32_t* indptr, uint64_t indptr_len,
+                      uint32_t* indices, uint64_t indices_len, float* dists,
+                      uint64_t dists_len, uint64_t* nnz_out) {
+    int rc = check_args(c, n, d, o);
+    if (rc != PQ_OK) return rc;
+    if (!data || !indptr || !indices || !dists || !nnz_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    if (indptr_len != n + 1) return fail(c, PQ_EINVAL, "indptr must have n_obs + 1 entries");
+    uint64_t cap = n * effective_k(n, o->k);
+    if (indices_len < cap || dists_len < cap)
+        return fail(c, PQ_EINVAL, "the graph arrays are too short");
+    return guarded(c, [&]() -> int {
+        uint32_t* dip = c->get<uint32_t>("out_indptr", n + 1);
+        uint32_t* dix = c->get<uint32_t>("out_indices", cap);
+        float* ddx = c->get<float>("out_dists", cap);
+        uint64_t nnz = build_plain(c, data, true, n, d, *o, dip, dix, ddx, nullptr);
+        ck(cudaMemcpyAsync(indptr, dip, (n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
+        ck(cudaMemcpyAsync(indices, dix, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
+        ck(cudaMemcpyAsync(dists, ddx, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
+        ck(cudaStreamSynchronize(c->stream), "d2h");
+        *nnz_out = nnz;
+        return PQ_OK;
+    });
+}
+
+int pq_nndescent_into_device(pq_ctx* c, const float* d_data, uint64_t n, uint64_t d,
+                             const pq_nnd_opts* o, uint32_t* d_indptr, uint32_t* d_indices,
+                             float* d_dists, uint64_t* nnz_out, void* stream) {
+    int rc = check_args(c, n, d, o);
+    if (rc != PQ_OK) return rc;
+    if (!d_data || !d_indptr || !d_indices || !d_dists || !nnz_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    return guarded(c, [&]() -> int {
+        cudaStream_t user = static_cast<cudaStream_t>(stream);
+        cudaEvent_t ev;
+        ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        ck(cudaEventRecord(ev, user), "event");
+        ck(cudaStreamWaitEvent(c->stream, ev, 0), "event");
+        uint64_t nnz = build_plain(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists,
+                                   nullptr);
+        ck(cudaEventRecord(ev, c->stream), "event");
+        ck(cudaStreamWaitEvent(user, ev, 0), "event");
+        cudaEventDestroy(ev);
+        *nnz_out = nnz;
+        return PQ_OK;
+    });
+}
+
+int pq_nndescent_probe(pq_ctx* c, const float* data, uint64_t n, uint64_t d,
+                       const pq_nnd_opts* o, int32_t stop_after, uint32_t* heap_idx,
+                       float* heap_dist, uint8_t* heap_flag, uint32_t* cand_new,
+                       uint32_t* cand_old) {
+    int rc = check_args(c, n, d, o);
+    if (rc != PQ_OK) return rc;
+    return guarded(c, [&]() -> int {
+        uint64_t cap = n * effective_k(n, o->k);
+        uint32_t* dip = c->get<uint32_t>("out_indptr", n + 1);
+        uint32_t* dix = c->get<uint32_t>("out_indices", cap);
+        float* ddx = c->get<float>("out_dists", cap);
+        Probe p;
+        p.stop_after = stop_after;
+        p.heap_idx = heap_idx;
+        p.heap_dist = heap_dist;
+        p.heap_flag = heap_flag;
+        p.cand_new = cand_new;
+        p.cand_old = cand_old;
+        build_plain(c, data, true, n, d, *o, dip, dix, ddx, &p);
+        return PQ_OK;
+    });
+}
+
+int pq_debug_tree(pq_ctx* c, const float* data, uint64_t n, uint64_t d, const pq_nnd_opts* o,
+                  uint32_t tree, uint32_t* ids, uint32_t* leaves, uint64_t leaves_cap,
+                  uint64_t* n_leaves) {
+    int rc = check_args(c, n, d, o);
+    if (rc != PQ_OK) return rc;
+    if (!ids || !leaves || !n_leaves) return fail(c, PQ_EINVAL, "null buffer");
+    Resolved R = resolve(n, *o);
+    if (tree >= R.n_trees) return fail(c, PQ_EINVAL, "tree index out of range");
+    return guarded(c, [&]() -> int {
+        Probe p;
+        p.tree = int32_t(tree);
+        p.tree_ids = ids;
+        p.tree_leaves = leaves;
+        p.leaves_cap = leaves_cap;
+        p.n_leaves = n_leaves;
+        build_plain(c, data, true, n, d, *o, nullptr, nullptr, nullptr, &p);
+        return PQ_OK;
+    });
+}
+
+}  // extern "C"

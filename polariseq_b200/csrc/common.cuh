@@ -1,0 +1,193 @@
+// Shared device helpers for the sm_100a kNN-graph builder.
+//
+// Exactness contract: every f32 distance and dot product is computed in the
+// reference's order (crates/polariseq-core/src/simd.rs:14-81): eight independent
+// lane accumulators over chunks of 8, the fixed reduce
+// ((a0+a4)+(a1+a5))+((a2+a6)+(a3+a7)), then a sequentially summed tail; every
+// operation rounded separately (no FMA contraction: the Rust reference never
+// fuses).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#define PQ_EMPTY 0xFFFFFFFFu
+
+namespace pq {
+
+// Kernels launched by this library (for the launch-count statistic).
+extern unsigned long long g_launches;
+inline void count_launch() { ++g_launches; }
+
+// ── deterministic hashing RNG (nndescent.rs:80-112) ───────────────────────
+__host__ __device__ __forceinline__ uint64_t splitmix(uint64_t x) {
+    x += 0x9E3779B97F4A7C15ull;
+    uint64_t z = x;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// hash_unit (nndescent.rs:89-93): the top 24 bits of the hash over 2^24.
+__host__ __device__ __forceinline__ float hash_unit(uint64_t seed, uint64_t a, uint64_t b) {
+    uint64_t h = splitmix(seed ^ splitmix(a) ^ splitmix(b * 0x9E3779B97F4A7C15ull));
+    return float(uint32_t(h >> 40)) * (1.0f / 16777216.0f);
+}
+
+// hash_index (nndescent.rs:95-98).
+__host__ __device__ __forceinline__ uint64_t hash_index(uint64_t seed, uint64_t a, uint64_t b,
+                                                        uint64_t n) {
+    return splitmix(seed ^ splitmix(a) ^ splitmix(b + 0x12345678ull)) % n;
+}
+
+// Rng (nndescent.rs:101-112): the state is replaced by splitmix(state).
+struct Rng {
+    uint64_t s;
+    __host__ __device__ __forceinline__ uint64_t next_u64() {
+        s = splitmix(s);
+        return s;
+    }
+    __host__ __device__ __forceinline__ uint64_t below(uint64_t n) { return next_u64() % n; }
+};
+
+// ── packed f32x2 arithmetic, round-to-nearest-even per half ───────────────
+typedef unsigned long long f2;
+
+__device__ __forceinline__ f2 f2_pack(float lo, float hi) {
+    f2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r) : "f"(lo), "f"(hi));
+    return r;
+}
+__device__ __forceinline__ void f2_unpack(f2 v, float& lo, float& hi) {
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ f2 f2_sub(f2 a, f2 b) {
+    f2 r;
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_mul(f2 a, f2 b) {
+    f2 r;
+    asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+__device__ __forceinline__ f2 f2_add(f2 a, f2 b) {
+    f2 r;
+    asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(a), "l"(b));
+    return r;
+}
+
+// Final reduce of the packed accumulators (a0,a1) (a2,a3) (a4,a5) (a6,a7)
+// into ((a0+a4)+(a1+a5))+((a2+a6)+(a3+a7)).
+__device__ __forceinline__ float reduce8_packed(f2 a01, f2 a23, f2 a45, f2 a67) {
+    float x, y, z, w;
+    f2_unpack(f2_add(a01, a45), x, y);  // (a0+a4, a1+a5)
+    f2_unpack(f2_add(a23, a67), z, w);  // (a2+a6, a3+a7)
+    return __fadd_rn(__fadd_rn(x, y), __fadd_rn(z, w));
+}
+
+// Squared Euclidean distance of two padded rows (16-byte aligned), exact
+// reference order (simd.rs:43-62).  `d` is the logical dimension.  Every
+// operation is a separately rounded scalar intrinsic, which the compiler
+// never contracts into an FMA.
+__device__ __forceinline__ float sq_dist_exact(const float* __restrict__ a,
+                                               const float* __restrict__ b, int d) {
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const int full = d >> 3;
+    const float4* a4 = reinterpret_cast<const float4*>(a);
+    const float4* b4 = reinterpret_cast<const float4*>(b);
+#pragma unroll 4
+    for (int c = 0; c < full; ++c) {
+        float4 x0 = a4[2 * c], x1 = a4[2 * c + 1];
+        float4 y0 = b4[2 * c], y1 = b4[2 * c + 1];
+        float t[8] = {__fsub_rn(x0.x, y0.x), __fsub_rn(x0.y, y0.y), __fsub_rn(x0.z, y0.z),
+                      __fsub_rn(x0.w, y0.w), __fsub_rn(x1.x, y1.x), __fsub_rn(x1.y, y1.y),
+                      __fsub_rn(x1.z, y1.z), __fsub_rn(x1.w, y1.w)};
+#pragma unroll
+        for (int l = 0; l < 8; ++l) acc[l] = __fadd_rn(acc[l], __fmul_rn(t[l], t[l]));
+    }
+    float tail = 0.0f;
+    for (int j = full << 3; j < d; ++j) {
+        float t = __fsub_rn(a[j], b[j]);
+        tail = __fadd_rn(tail, __fmul_rn(t, t));
+    }
+    float r = __fadd_rn(__fadd_rn(__fadd_rn(acc[0], acc[4]), __fadd_rn(acc[1], acc[5])),
+                        __fadd_rn(__fadd_rn(acc[2], acc[6]), __fadd_rn(acc[3], acc[7])));
+    return __fadd_rn(r, tail);
+}
+
+// Dot product, exact reference order (simd.rs:20-36).
+__device__ __forceinline__ float dot_exact(const float* __restrict__ a,
+                                           const float* __restrict__ b, int d) {
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const int full = d >> 3;
+    const float4* a4 = reinterpret_cast<const float4*>(a);
+    const float4* b4 = reinterpret_cast<const float4*>(b);
+#pragma unroll 4
+    for (int c = 0; c < full; ++c) {
+        float4 x0 = a4[2 * c], x1 = a4[2 * c + 1];
+        float4 y0 = b4[2 * c], y1 = b4[2 * c + 1];
+        acc[0] = __fadd_rn(acc[0], __fmul_rn(x0.x, y0.x));
+        acc[1] = __fadd_rn(acc[1], __fmul_rn(x0.y, y0.y));
+        acc[2] = __fadd_rn(acc[2], __fmul_rn(x0.z, y0.z));
+        acc[3] = __fadd_rn(acc[3], __fmul_rn(x0.w, y0.w));
+        acc[4] = __fadd_rn(acc[4], __fmul_rn(x1.x, y1.x));
+        acc[5] = __fadd_rn(acc[5], __fmul_rn(x1.y, y1.y));
+        acc[6] = __fadd_rn(acc[6], __fmul_rn(x1.z, y1.z));
+        acc[7] = __fadd_rn(acc[7], __fmul_rn(x1.w, y1.w));
+    }
+    float tail = 0.0f;
+    for (int j = full << 3; j < d; ++j) tail = __fadd_rn(tail, __fmul_rn(a[j], b[j]));
+    float r = __fadd_rn(__fadd_rn(__fadd_rn(acc[0], acc[4]), __fadd_rn(acc[1], acc[5])),
+                        __fadd_rn(__fadd_rn(acc[2], acc[6]), __fadd_rn(acc[3], acc[7])));
+    return __fadd_rn(r, tail);
+}
+
+// Flagged neighbour-heap push on one row (HeapRowsMut::push, nndescent.rs:168-205):
+// reject d >= root or an index already present; else replace the root and
+// sift down with strict `>`.
+__device__ __forceinline__ bool heap_push(uint32_t* idx, float* dist, uint8_t* flg, int k,
+                                          uint32_t j, float d, uint8_t flag) {
+    if (d >= dist[0]) return false;
+    for (int s = 0; s < k; ++s)
+        if (idx[s] == j) return false;
+    int p = 0;
+    for (;;) {
+        int l = 2 * p + 1, r = 2 * p + 2, sw = p;
+        float dsw = d;  // the value travelling down from the root
+        if (l < k && dist[l] > dsw) { sw = l; dsw = dist[l]; }
+        if (r < k && dist[r] > dsw) { sw = r; }
+        if (sw == p) break;
+        idx[p] = idx[sw];
+        dist[p] = dist[sw];
+        flg[p] = flg[sw];
+        p = sw;
+    }
+    idx[p] = j;
+    dist[p] = d;
+    flg[p] = flag;
+    return true;
+}
+
+// Candidate-heap push (CandidateHeap::push_row, nndescent.rs:244-269).
+__device__ __forceinline__ void cand_push(uint32_t* idx, float* prio, int m, uint32_t j,
+                                          float p) {
+    if (p >= prio[0]) return;
+    for (int s = 0; s < m; ++s)
+        if (idx[s] == j) return;
+    int q = 0;
+    for (;;) {
+        int l = 2 * q + 1, r = 2 * q + 2, sw = q;
+        float psw = p;
+        if (l < m && prio[l] > psw) { sw = l; psw = prio[l]; }
+        if (r < m && prio[r] > psw) { sw = r; }
+        if (sw == q) break;
+        idx[q] = idx[sw];
+        prio[q] = prio[sw];
+        q = sw;
+    }
+    idx[q] = j;
+    prio[q] = p;
+}
+
+}  // namespace pq
