@@ -1,0 +1,368 @@
+"""Benchmark: kNN-graph build throughput (cells/s) on one B200 per rank.
+
+Workload (one "step" = one complete kNN-graph build): 4,000,000 cells x 50 PCs
+f32, k = 15, a 60-component Gaussian mixture with log-normal cluster sizes, a
+j^-0.5 per-dimension spectrum and 5% doublet-like midpoints (seeded synthetic
+data standing in for a PCA embedding; no dataset is needed or available).
+
+  value  cells/s with the embedding already resident in HBM (device entry point)
+  e2e    cells/s through the C ABI with pinned HOST buffers: the embedding's
+         host->device copy and the graph's device->host copy are inside the
+         timed region
+  roofline  the dominant kernel group's algorithmic bytes per launch over its
+         CUDA-event duration, against the measured HBM copy bandwidth
+  cpu_baseline  the C++ restatement of the reference's CPU NN-Descent (oracle/)
+         on a bounded sample of the same workload, all host threads
+
+Multi-GPU (torchrun): each rank builds the graph of its own embedding (replicas
+of the workload with different seeds); per-step time is the max over ranks.
+
+`--impl reference` times the reference algorithm's CPU implementation (the
+oracle port; the Rust reference cannot be built here) on rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "kNN build cells/s, 4M×50, k=15: plain vs chosen form at recall@15≥0.99"
+UNIT = "cells/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--n", type=int, default=4_000_000)
+    ap.add_argument("--d", type=int, default=50)
+    ap.add_argument("--k", type=int, default=15)
+    ap.add_argument("--comps", type=int, default=60)
+    ap.add_argument("--queries", type=int, default=20_000)
+    ap.add_argument("--cpu-sample", type=int, default=262_144)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--profile-only", action="store_true",
+                    help="run W warm-up and K device-resident builds, print nothing else "
+                         "(for ncu launch lists)")
+    return ap.parse_args()
+
+
+def workload(args, rank):
+    from polariseq_b200 import synth
+
+    return synth.mixture_lognormal(args.n, args.d, args.comps, seed=1000 + rank)
+
+
+def config(args):
+    return {"workload": f"kNN graph build, {args.n} cells x {args.d} PCs f32, k={args.k}, "
+                        f"{args.comps}-component log-normal Gaussian mixture, 5% doublets",
+            "n_cells": args.n, "n_pcs": args.d, "k": args.k, "form": "plain (bit-exact)",
+            "l2": "inputs larger than L2 (embedding 800 MB, graph 480 MB)"}
+
+
+# ── clocks sampled during the timed region ─────────────────────────────────
+class Clocks:
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.p = None
+
+    def start(self):
+        try:
+            self.p = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device}", f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.flush()
+        rows = []
+        for line in open(self.f.name):
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 9:
+                rows.append(parts)
+        os.unlink(self.f.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i] == "Active"})
+        loaded = [s for s in sm if s > 0.5 * (max(mx) if mx else 1)] or sm
+        return {"sm_mhz": statistics.median(loaded) if loaded else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(rows)}
+
+
+# ── recall vs FP64 exact on sampled queries ────────────────────────────────
+def recall_fp64(torch, x_dev, indices, dists, k, nq, seed=7):
+    """recall@k and max relative distance error against an FP64 brute force
+    (self excluded, (distance, index) order) on nq seeded query rows."""
+    n = x_dev.shape[0]
+    g = np.random.default_rng(seed)
+    q = np.sort(g.choice(n, size=min(nq, n), replace=False))
+    xd = x_dev.double()
+    x2 = (xd * xd).sum(1)
+    hits = 0
+    max_rel = 0.0
+    ind = indices.reshape(n, k)
+    dst = dists.reshape(n, k)
+    qt = torch.from_numpy(q).to(x_dev.device)
+    for s in range(0, len(q), 256):
+        qi = qt[s:s + 256]
+        xq = xd[qi]
+        d2 = x2[qi][:, None] + x2[None, :] - 2.0 * (xq @ xd.T)
+        d2[torch.arange(len(qi), device=d2.device), qi] = float("inf")
+        # (distance, index) order: stable sort of the k+8 best by distance
+        vals, idx = torch.topk(d2, k + 8, dim=1, largest=False, sorted=True)
+        exact = idx[:, :k].cpu().numpy()
+        a = ind[q[s:s + 256]]
+        for r in range(len(qi)):
+            hits += len(set(exact[r].tolist()) & set(a[r].tolist()))
+        # max relative error of returned distances vs the FP64 distance of each pair
+        aj = torch.from_numpy(a.astype(np.int64)).to(x_dev.device)
+        true = torch.sqrt(((xq[:, None, :] - xd[aj]) ** 2).sum(-1))
+        got = torch.from_numpy(dst[q[s:s + 256]].astype(np.float64)).to(x_dev.device)
+        rel = ((got - true).abs() / true.clamp_min(1e-30)).max().item()
+        max_rel = max(max_rel, rel)
+    return hits / (len(q) * k), max_rel
+
+
+def cpu_baseline(args, x, threads=None):
+    """The oracle (C++ restatement of the reference CPU algorithm) on the
+    first `cpu_sample` cells of the workload, all host threads."""
+    import oracle
+
+    oracle.lib()
+    if threads:
+        oracle.set_threads(threads)
+    s = min(args.cpu_sample, x.shape[0])
+    sample = np.ascontiguousarray(x[:s])
+    t0 = time.perf_counter()
+    oracle.nndescent(sample, args.k, seed=0)
+    dt = time.perf_counter() - t0
+    return {"value": s / dt, "unit": UNIT, "cores": oracle.max_threads(), "kind": "port",
+            "sample": f"first {s} cells of the workload, one full build ({dt:.2f} s)"}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    x = workload(args, 0)
+    for _ in range(args.warmup):
+        cpu_baseline(args, x)
+    vals = [cpu_baseline(args, x) for _ in range(args.steps)]
+    v = statistics.median([r["value"] for r in vals])
+    cb = dict(vals[-1])
+    cb["value"] = v
+    s = min(args.cpu_sample, args.n)
+    line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * s / v,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic", "config": config(args), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# Algorithmic bytes of one launch of the dominant kernel group, per unit.
+def algorithmic_bytes(group, st, args):
+    n, d, k = args.n, args.d, args.k
+    row = 4 * d
+    if group == "join_count":
+        # every non-empty candidate row of every source row read once, the
+        # candidate ids and thresholds, and the emit bits written
+        m = st["max_candidates"]
+        return n * (2 * m * row + 2 * m * 8 + (4 * m * m) // 8 + 4)
+    if group == "seqtree":
+        # each point's row read once per level it passes below the top levels
+        return None
+    return None
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=600))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+
+    import polariseq_b200 as pq
+    from polariseq_b200 import _lib
+
+    x = workload(args, rank)
+    n, d, k = x.shape[0], x.shape[1], args.k
+    cap = n * pq.effective_k(n, k)
+    ctx = pq.Context(local)
+    opts = pq._opts(k, 0, 0, 0, 0, 0.001)
+    stream = torch.cuda.current_stream(dev)
+    xd = torch.from_numpy(x).to(dev)
+    ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    ix = torch.empty(cap, dtype=torch.int32, device=dev)
+    dx = torch.empty(cap, dtype=torch.float32, device=dev)
+
+    def step():
+        return ctx.nndescent_device(xd, opts, ip, ix, dx, stream=stream.cuda_stream)
+
+    if args.profile_only:
+        for _ in range(args.warmup + args.steps):
+            step()
+        torch.cuda.synchronize(dev)
+        st = ctx.stats()
+        print(json.dumps({"profile_only": True, "n": n, "launches_per_build": None,
+                          "ms_total": st["ms_total"]}), flush=True)
+        return
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    # ── device-resident timed region (with kernel-group events) ──
+    _lib.load().pq_ctx_set_profiling(ctx._h, 1)
+    clocks = Clocks(local)
+    clocks.start()
+    kg_ms = np.zeros(16)
+    kg_l = np.zeros(16, np.int64)
+    launches = 0
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    stats = []
+    for _ in range(args.steps):
+        nnz = step()
+        st = ctx.stats()
+        stats.append(st)
+        s = _lib.NndStats()
+        _lib.load().pq_ctx_stats(ctx._h, s)
+        kg_ms += np.array(s.kg_ms[:16])
+        kg_l += np.array(s.kg_launches[:16], np.int64)
+        launches += s.launches
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    ms = e0.elapsed_time(e1) / args.steps
+    ck = clocks.stop()
+    _lib.load().pq_ctx_set_profiling(ctx._h, 0)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * n / (ms / 1000.0)
+
+    # ── end to end through the C ABI with pinned host buffers ──
+    hx = torch.from_numpy(x).pin_memory()
+    hip = torch.empty(n + 1, dtype=torch.int32).pin_memory()
+    hix = torch.empty(cap, dtype=torch.int32).pin_memory()
+    hdx = torch.empty(cap, dtype=torch.float32).pin_memory()
+    hxn, hipn = hx.numpy(), hip.numpy().view(np.uint32)
+    hixn, hdxn = hix.numpy().view(np.uint32), hdx.numpy()
+    pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local)  # warm the host path
+    barrier()
+    t0 = time.perf_counter()
+    e2e_steps = max(1, min(args.steps, 3))
+    for _ in range(e2e_steps):
+        r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local)
+    e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
+    if world > 1:
+        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    e2e = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": int(x.nbytes),
+           "d2h_bytes_per_step": int(4 * (n + 1) + 8 * r["nnz"])}
+
+    # ── quality: recall@k and max relative distance error vs FP64 exact ──
+    rec, max_rel = recall_fp64(torch, xd, hixn[:r["nnz"]], hdxn[:r["nnz"]], k, args.queries)
+
+    # ── roofline of the dominant kernel group ──
+    names = _lib.KERNEL_GROUPS
+    per = {names[g]: {"ms_per_build": kg_ms[g] / args.steps,
+                      "launches_per_build": int(kg_l[g] // args.steps)}
+           for g in range(len(names))}
+    dom = max(per, key=lambda g: per[g]["ms_per_build"])
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    roof = None
+    ab = algorithmic_bytes(dom, stats[-1], args)
+    if ab is not None and per[dom]["launches_per_build"] > 0:
+        per_launch_ms = per[dom]["ms_per_build"] / per[dom]["launches_per_build"]
+        bytes_per_launch = ab / per[dom]["launches_per_build"]
+        achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
+        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "traffic": None,
+                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        try:
+            cpu = cpu_baseline(args, x)
+        except Exception as e:  # pragma: no cover
+            cpu = {"error": str(e)}
+
+    st = stats[-1]
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config(args), "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
+            "quality": {"recall_at_k": rec, "max_rel_dist_err": max_rel,
+                        "queries": min(args.queries, n), "oracle": "FP64 brute force"},
+            "phases_ms": {"forest": st["ms_forest"], "leaf_pairs": st["ms_leaves"],
+                          "rounds": st["ms_rounds"], "extract": st["ms_extract"]},
+            "rounds_run": st["rounds_run"], "kernel_groups": per}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -4,7 +4,9 @@
 // (crates/polariseq-core/src/nndescent.rs:708-752), pads the embedding to
 // 16-byte rows in HBM, then runs the plain form's phases on the context's
 // stream: RP forest, leaf pairs, random fill, rounds, extract.
+#include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstdio>
 #include <cstring>
 #include <map>
@@ -42,6 +44,8 @@ struct pq_ctx {
     int* d_err = nullptr;
     uint64_t* d_u64 = nullptr;            // small device scalars
     unsigned long long* d_acc = nullptr;  // device accumulators
+    cudaStream_t stream2 = nullptr;  // the largest subtrees run here, concurrently
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int profile = 0;
     struct KGRec {
         cudaEvent_t a, b;
@@ -266,6 +270,12 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
     fa.tabB = c->get<uint32_t>("tabB", TN);
     fa.leafflag = c->get<uint8_t>("leafflag", TN);
     fa.err = c->d_err;
+    const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
+    fa.trace = nullptr;
+    if (trace) {
+        fa.trace = c->get<unsigned long long>("seq_trace", SEQ_TRACE_N);
+        ck(cudaMemsetAsync(fa.trace, 0, SEQ_TRACE_N * 8, st), "trace");
+    }
     k_iota_trees<<<blocks(TN, 256), 256, 0, st>>>(fa.ids, n, T); count_launch();
     ck(cudaMemsetAsync(fa.leafflag, 0, TN, st), "memset leafflag");
 
@@ -332,17 +342,48 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
         }
     }
     {
+        // largest subtrees first: their depth-first chains are the critical path
+        std::stable_sort(roots.begin(), roots.end(),
+                         [](const SRoot& x, const SRoot& y) { return x.size > y.size; });
         SRoot* d_roots = c->get<SRoot>("sroots", roots.size());
         ck(cudaMemcpyAsync(d_roots, roots.data(), roots.size() * sizeof(SRoot),
                            cudaMemcpyHostToDevice, st),
            "upload roots");
         KGScope kg(c, PQ_KG_SEQTREE);
-        launch_seqtrees(fa, d_roots, uint32_t(roots.size()), st);
+        uint32_t n_big = 0;
+        while (n_big < roots.size() && n_big < 148 && roots[n_big].size > 65536) ++n_big;
+        if (trace) {
+            uint64_t r0 = roots.empty() ? 0 : roots[0].size;
+            ck(cudaMemcpyAsync(fa.trace + SEQ_T_ROOT0, &r0, 8, cudaMemcpyHostToDevice, st), "tr");
+        }
+        // the big-root stream starts after everything queued so far and the
+        // main stream waits for it before the leaf pairs
+        ck(cudaEventRecord(c->ev_fork, st), "fork");
+        ck(cudaStreamWaitEvent(c->stream2, c->ev_fork, 0), "fork");
+        launch_seqtrees(fa, d_roots, n_big, uint32_t(roots.size()), st, c->stream2);
+        ck(cudaEventRecord(c->ev_join, c->stream2), "join");
+        ck(cudaStreamWaitEvent(st, c->ev_join, 0), "join");
         ck(cudaGetLastError(), "seqtrees");
     }
     int herr = 0;
     ck(cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "err");
     S.ms_forest = tm.stop();
+    if (trace) {
+        unsigned long long h[SEQ_TRACE_N];
+        ck(cudaMemcpy(h, fa.trace, sizeof(h), cudaMemcpyDeviceToHost), "trace");
+        std::fprintf(stderr,
+                     "[nndescent] rp-forest build (%u trees, leaf %llu): %.2f ms; %zu subtree "
+                     "roots, largest %llu\n",
+                     T, (unsigned long long)R.leaf_size, S.ms_forest, roots.size(), h[SEQ_T_ROOT0]);
+        std::fprintf(stderr,
+                     "[nndescent]   subtrees: global nodes %llu (points %llu), staged subtrees "
+                     "%llu (nodes %llu), tie nodes %llu, random splits %llu\n",
+                     h[0], h[1], h[2], h[3], h[4], h[5]);
+        std::fprintf(stderr,
+                     "[nndescent]   largest subtree cycles: draw %llu margin %llu partition %llu "
+                     "staged %llu total %llu\n",
+                     h[6], h[7], h[8], h[9], h[10]);
+    }
     if (herr) throw DeviceError{"forest: a subtree exceeded the depth-first stack"};
 
     if (probe && probe->tree >= 0) {
@@ -419,6 +460,8 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
     uint32_t* bits = c->get<uint32_t>("bits", size_t(n) * words);
     void* stemp = c->get<uint8_t>("scan_temp", scan_temp_bytes(n));
     const size_t nrec_c = 2 * size_t(n) * k;
+    // join CTAs visit source rows in tree 0's leaf order (spatially coherent)
+    const uint32_t* perm = fa.ids;
     for (uint64_t iter = 0; iter < R.n_iters; ++iter) {
         // candidates
         uint32_t* ck_ = c->get<uint32_t>("ckeys", nrec_c);
@@ -440,8 +483,8 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
         ck(cudaMemsetAsync(c->d_acc, 0, 2 * sizeof(unsigned long long), st), "memset acc");
         {
             KGScope kg(c, PQ_KG_JOIN_COUNT);
-            launch_join_count(X, d, dp, n, k, m, hdist, new_idx, old_idx, bits, words, row_cnt,
-                              c->d_acc, st);
+            launch_join_count(X, d, dp, n, k, m, hdist, new_idx, old_idx, perm, bits, words,
+                              row_cnt, c->d_acc, st);
         }
         uint32_t* row_off = seg_off;  // free until the replay's segments are computed
         ck(scan_exclusive_u32(row_cnt, row_off, n, stemp, c->d_u64, st), "scan join");
@@ -459,8 +502,8 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
             ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
             {
                 KGScope kg(c, PQ_KG_JOIN_WRITE);
-                launch_join_write(X, d, dp, n, m, new_idx, old_idx, bits, words, row_off, jk, jv,
-                                  dcnt, st);
+                launch_join_write(X, d, dp, n, m, new_idx, old_idx, perm, bits, words, row_cnt,
+                                  row_off, jk, jv, dcnt, st);
             }
             {
                 KGScope kg(c, PQ_KG_SORT);
@@ -542,6 +585,11 @@ int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
         return fail(c, PQ_EINVAL, "n_obs * k must be below 2^31");
     if (R.n_trees * n > (uint64_t(1) << 36))
         return fail(c, PQ_EINVAL, "n_trees * n_obs is too large");
+    if (2 * R.max_cand * ((d + 3) / 4 * 4) * 4 > 200 * 1024 || R.max_cand > 200)
+        return fail(c, PQ_ENOTSUP,
+                    "n_dim * max_candidates exceeds the join's shared-memory tile "
+                    "(2 * max_candidates * n_dim * 4 bytes must stay under 200 KiB, "
+                    "max_candidates <= 200)");
     if (o->mode != PQ_MODE_PLAIN || o->init != PQ_INIT_RP)
         return fail(c, PQ_ENOTSUP, "only the plain form with RP init is available on this entry");
     return PQ_OK;
@@ -590,6 +638,9 @@ int pq_ctx_create(int device, pq_ctx** out) {
     pq_ctx* c = new pq_ctx();
     c->device = device;
     if (cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming) != cudaSuccess ||
         cudaMalloc(&c->d_err, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&c->d_u64, 8 * sizeof(uint64_t)) != cudaSuccess ||
         cudaMalloc(&c->d_acc, 8 * sizeof(unsigned long long)) != cudaSuccess) {
@@ -610,6 +661,10 @@ void pq_ctx_destroy(pq_ctx* c) {
     if (c->d_err) cudaFree(c->d_err);
     if (c->d_u64) cudaFree(c->d_u64);
     if (c->d_acc) cudaFree(c->d_acc);
+    if (c->stream2) cudaStreamSynchronize(c->stream2);
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
+    if (c->stream2) cudaStreamDestroy(c->stream2);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
 }

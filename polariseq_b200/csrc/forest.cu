@@ -17,6 +17,8 @@
 // where A[j] is the position of the j-th right point in [0, nL), B[j] the
 // position of the j-th left point in [nL, size) counted from the top, and c
 // the number of right points in [0, nL).
+#include <algorithm>
+
 #include "common.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
@@ -28,9 +30,10 @@ constexpr int FT = 256;             // threads per forest CTA
 constexpr int PER = FOREST_CHUNK / FT;  // positions per thread in a chunk
 constexpr int STK = 128;            // DFS stack depth (depth > 100 is a leaf)
 
-// Exclusive block scan of one u32 per thread (FT threads).
+// Exclusive block scan of one u32 per thread (any multiple of 32 threads, at
+// most 1024); *total receives the block sum.
 __device__ __forceinline__ uint32_t bscan(uint32_t v, uint32_t* ws, uint32_t* total) {
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
     uint32_t x = v;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -40,17 +43,17 @@ __device__ __forceinline__ uint32_t bscan(uint32_t v, uint32_t* ws, uint32_t* to
     if (lane == 31) ws[w] = x;
     __syncthreads();
     if (w == 0) {
-        uint32_t s = lane < (FT / 32) ? ws[lane] : 0;
+        uint32_t s = lane < nw ? ws[lane] : 0;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             uint32_t y = __shfl_up_sync(0xFFFFFFFFu, s, o);
             if (lane >= o) s += y;
         }
-        if (lane < FT / 32) ws[lane] = s;
+        if (lane < nw) ws[lane] = s;
     }
     __syncthreads();
     uint32_t r = (w > 0 ? ws[w - 1] : 0) + x - v;
-    *total = ws[FT / 32 - 1];
+    *total = ws[nw - 1];
     __syncthreads();
     return r;
 }
@@ -249,16 +252,206 @@ __global__ void k_degenerate(ForestArgs a, PNode* nodes, uint32_t nn) {
 
 // One CTA finishes one subtree depth-first with a single Rng
 // (rp_tree_sequential / rp_tree_leaves, nndescent.rs:419-581).
-__global__ void __launch_bounds__(FT) k_seqtree(ForestArgs a, const SRoot* roots) {
-    extern __shared__ __align__(16) float nv[];
-    __shared__ uint32_t stS[STK], stN[STK];
-    __shared__ uint16_t stD[STK];
-    __shared__ int sp;
-    __shared__ uint64_t rng;
-    __shared__ uint32_t sA, sB, snL, sc;
-    __shared__ float soff;
-    __shared__ int anytie;
-    __shared__ uint32_t ws[32];
+//
+// Every thread draws from its own copy of the Rng and sums the hyperplane
+// offset itself (the values are identical in all threads), so no node has a
+// serial section.  Nodes larger than the staged capacity run in global mode:
+// all NT threads compute margins from the rows in HBM and partition through
+// the per-tree scratch arrays.  A node of at most SCAP points has its ids and
+// rows staged in shared memory once (the reference gathers small subtrees
+// for the same reason, :474-491) and warp 0 alone finishes its whole subtree
+// with ballots, without block barriers.  The largest subtrees (their
+// depth-first chains are the critical path) run with NT = 512.
+constexpr int SCAP = 128;   // staged capacity (points): 4 per lane of warp 0
+
+struct SeqShared {
+    uint32_t stS[STK], stN[STK];
+    uint16_t stD[STK];
+    uint32_t lS[STK], lN[STK];
+    uint16_t lD[STK];
+    uint32_t sid[SCAP], sslot[SCAP], sid2[SCAP], sslot2[SCAP];
+    uint8_t code[SCAP];
+    uint32_t tabA[SCAP], tabB[SCAP];
+    uint32_t ws[32];
+    uint64_t rng;
+    uint32_t cntL, sc;
+    int sp, anytie;
+};
+
+// Draws of random_hyperplane (nndescent.rs:369-375) as positions: ids within
+// a node are distinct, so the reference's `b == a` is a position test.
+__device__ __forceinline__ void draw_pair(Rng& r, uint32_t n, uint32_t& pa, uint32_t& pb) {
+    pa = uint32_t(r.below(n));
+    pb = uint32_t(r.below(n));
+    int tries = 0;
+    while (pb == pa && tries < 8) {
+        pb = uint32_t(r.below(n));
+        ++tries;
+    }
+}
+
+// Warp 0 finishes a staged subtree: local positions [0, n0) of the staged
+// ids/slots, rows in `rows` (slot-indexed), normal in `nv`.
+template <int D>
+__device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, float* nv,
+                             uint32_t st, uint32_t n0, uint32_t dep0, Rng& rng, uint8_t* leaf) {
+    const int lane = threadIdx.x & 31;
+    const int d = a.d, dp = a.dp;
+    const unsigned lt = (1u << lane) - 1u;
+    int lsp = 1;
+    if (lane == 0) {
+        S.lS[0] = 0;
+        S.lN[0] = n0;
+        S.lD[0] = uint16_t(dep0);
+    }
+    __syncwarp();
+    while (lsp > 0) {
+        const uint32_t ls = S.lS[lsp - 1], ln = S.lN[lsp - 1], ld = S.lD[lsp - 1];
+        __syncwarp();
+        lsp -= 1;
+        if (ln <= a.leaf_size || ld > 100) {
+            if (lane == 0) leaf[st + ls] = 1;
+            continue;
+        }
+        if (a.trace && lane == 0) atomicAdd(&a.trace[SEQ_T_STAGED_NODES], 1ull);
+        uint32_t pa, pb;
+        draw_pair(rng, ln, pa, pb);
+        const float* xa = rows + size_t(S.sslot[ls + pa]) * dp;
+        const float* xb = rows + size_t(S.sslot[ls + pb]) * dp;
+        for (int j = lane; j < dp; j += 32) nv[j] = j < d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
+        __syncwarp();
+        // margins of the positions this lane owns (lane + 32*i); the dot
+        // products and the offset chain are independent and overlap
+        float dots[SCAP / 32];
+#pragma unroll 1
+        for (int i = 0; i < SCAP / 32; ++i) {
+            const uint32_t p = lane + 32 * i;
+            dots[i] = p < ln ? dot_exact_t<D>(nv, rows + size_t(S.sslot[ls + p]) * dp, d) : 0.f;
+        }
+        const float off = hyper_offset_t<D>(xa, xb, d);
+        unsigned any_tie = 0;
+#pragma unroll
+        for (int i = 0; i < SCAP / 32; ++i) {
+            const uint32_t p = lane + 32 * i;
+            if (p < ln) {
+                const float m = __fadd_rn(dots[i], off);
+                const uint8_t c = fabsf(m) < 1e-8f ? 2 : (m > 0.0f ? 1 : 0);
+                S.code[p] = c;
+                any_tie |= c == 2;
+            }
+        }
+        __syncwarp();
+        if (__any_sync(0xFFFFFFFFu, any_tie)) {
+            // ties draw from the Rng in position order (every lane replays the
+            // same draws so that all copies of the Rng stay equal)
+            if (a.trace && lane == 0) atomicAdd(&a.trace[SEQ_T_TIES], 1ull);
+            for (uint32_t p = 0; p < ln; ++p)
+                if (S.code[p] == 2) {
+                    uint8_t v = (rng.next_u64() & 1ull) == 0 ? 1 : 0;
+                    __syncwarp();
+                    if (lane == 0) S.code[p] = v;
+                    __syncwarp();
+                }
+        }
+        unsigned mask[SCAP / 32];
+        uint32_t nL = 0;
+#pragma unroll
+        for (int i = 0; i < SCAP / 32; ++i) {
+            const uint32_t p = lane + 32 * i;
+            mask[i] = __ballot_sync(0xFFFFFFFFu, p < ln && S.code[p] == 1);
+            nL += __popc(mask[i]);
+        }
+        uint32_t c = 0;
+        uint32_t pre = 0;
+#pragma unroll
+        for (int i = 0; i < SCAP / 32; ++i) {
+            const uint32_t p = lane + 32 * i;
+            const uint32_t lp = pre + __popc(mask[i] & lt);
+            const bool isL = (mask[i] >> lane) & 1u;
+            if (p < ln) {
+                if (isL) {
+                    if (p >= nL) S.tabB[(nL - lp) - 1] = p;
+                } else if (p < nL) {
+                    S.tabA[p - lp] = p;
+                }
+            }
+            // c = right points in [0, nL) = nL - (left points in [0, nL))
+            if (nL >= 32u * i && nL < 32u * i + 32u)
+                c = nL - (pre + __popc(mask[i] & ((1u << (nL - 32u * i)) - 1u)));
+            pre += __popc(mask[i]);
+        }
+        __syncwarp();
+        pre = 0;
+#pragma unroll
+        for (int i = 0; i < SCAP / 32; ++i) {
+            const uint32_t p = lane + 32 * i;
+            const uint32_t lp = pre + __popc(mask[i] & lt);
+            const bool isL = (mask[i] >> lane) & 1u;
+            if (p < ln) {
+                uint32_t dst;
+                if (isL) {
+                    dst = p < nL ? p : S.tabA[(nL - lp) - 1];
+                } else if (p < nL) {
+                    uint32_t rr = p - lp + 1;
+                    dst = (rr == 1 ? ln : S.tabB[rr - 2]) - 1;
+                } else if (p > nL) {
+                    dst = p - 1;
+                } else {
+                    dst = (c == 0 ? ln : S.tabB[c - 1]) - 1;
+                }
+                S.sid2[dst] = S.sid[ls + p];
+                S.sslot2[dst] = S.sslot[ls + p];
+            }
+            pre += __popc(mask[i]);
+        }
+        __syncwarp();
+        for (uint32_t p = lane; p < ln; p += 32) {
+            S.sid[ls + p] = S.sid2[p];
+            S.sslot[ls + p] = S.sslot2[p];
+        }
+        __syncwarp();
+        uint32_t split = nL;
+        if (nL == 0 || nL == ln) {
+            if (a.trace && lane == 0) atomicAdd(&a.trace[SEQ_T_DEGENERATE], 1ull);
+            for (uint32_t i = ln - 1; i >= 1; --i) {
+                uint32_t j = uint32_t(rng.below(uint64_t(i) + 1));
+                if (lane == 0) {
+                    uint32_t t1 = S.sid[ls + i], t2 = S.sslot[ls + i];
+                    S.sid[ls + i] = S.sid[ls + j];
+                    S.sslot[ls + i] = S.sslot[ls + j];
+                    S.sid[ls + j] = t1;
+                    S.sslot[ls + j] = t2;
+                }
+                __syncwarp();
+            }
+            split = ln / 2;
+        }
+        if (lsp + 2 > STK) {
+            if (lane == 0) atomicExch(a.err, 1);
+            return;
+        }
+        if (lane == 0) {
+            S.lS[lsp] = ls + split;
+            S.lN[lsp] = ln - split;
+            S.lD[lsp] = uint16_t(ld + 1);
+            S.lS[lsp + 1] = ls;
+            S.lN[lsp + 1] = split;
+            S.lD[lsp + 1] = uint16_t(ld + 1);
+        }
+        lsp += 2;
+        __syncwarp();
+    }
+}
+
+template <int NT, int D>
+__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax) {
+    constexpr int PERT = 8;  // positions per thread per partition tile
+    extern __shared__ __align__(16) float dyn[];
+    __shared__ SeqShared S;
+    float* nv = dyn;                 // dp
+    float* xab = dyn + a.dp;         // 2 * dp: the two hyperplane rows (global mode)
+    float* rows = dyn + 3 * a.dp;    // smax * dp
+    const int tid = threadIdx.x, lane = tid & 31;
     const SRoot rt = roots[blockIdx.x];
     const size_t tb = size_t(rt.tree) * a.n;
     uint32_t* ids = a.ids + tb;
@@ -266,140 +459,182 @@ __global__ void __launch_bounds__(FT) k_seqtree(ForestArgs a, const SRoot* roots
     uint8_t* side = a.side + tb;
     uint32_t* tabA = a.tabA + tb;
     uint32_t* tabB = a.tabB + tb;
-    if (threadIdx.x == 0) {
-        sp = 1;
-        stS[0] = rt.start;
-        stN[0] = rt.size;
-        stD[0] = uint16_t(rt.depth);
-        rng = rt.seed;
+    uint8_t* leaf = a.leafflag + tb;
+    const int d = a.d, dp = a.dp;
+    Rng rng{rt.seed};  // every thread holds the same state
+    unsigned long long* tr = a.trace;
+    const bool tb0 = tr && rt.size == tr[SEQ_T_ROOT0] && tid == 0;
+    long long t_start = clock64(), tclk = 0;
+    if (tid == 0) {
+        S.sp = 1;
+        S.stS[0] = rt.start;
+        S.stN[0] = rt.size;
+        S.stD[0] = uint16_t(rt.depth);
     }
     __syncthreads();
-    for (;;) {
-        if (sp == 0) break;
-        const uint32_t st = stS[sp - 1], sz = stN[sp - 1], dep = stD[sp - 1];
+    while (S.sp > 0) {
+        const uint32_t st = S.stS[S.sp - 1], sz = S.stN[S.sp - 1], dep = S.stD[S.sp - 1];
         __syncthreads();
-        if (threadIdx.x == 0) sp -= 1;
+        if (tid == 0) S.sp -= 1;
         if (sz <= a.leaf_size || dep > 100) {
-            if (threadIdx.x == 0) a.leafflag[tb + st] = 1;
+            if (tid == 0) leaf[st] = 1;
             __syncthreads();
             continue;
         }
-        if (threadIdx.x == 0) {
-            Rng r{rng};
-            uint32_t A = ids[st + r.below(sz)];
-            uint32_t B = ids[st + r.below(sz)];
-            int tries = 0;
-            while (B == A && tries < 8) {
-                B = ids[st + r.below(sz)];
-                ++tries;
-            }
-            rng = r.s;
-            sA = A;
-            sB = B;
-            anytie = 0;
-        }
-        __syncthreads();
-        {
-            const float* xa = a.X + size_t(sA) * a.dp;
-            const float* xb = a.X + size_t(sB) * a.dp;
-            for (int j = threadIdx.x; j < a.dp; j += FT)
-                nv[j] = j < a.d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
-            if (threadIdx.x == 0) {
-                float s = -0.0f;
-                for (int j = 0; j < a.d; ++j) {
-                    float nvj = __fsub_rn(xa[j], xb[j]);
-                    s = __fadd_rn(s, __fmul_rn(__fmul_rn(nvj, 0.5f), __fadd_rn(xa[j], xb[j])));
-                }
-                soff = -s;
-            }
-        }
-        __syncthreads();
-        const float off = soff;
-        for (uint32_t p = threadIdx.x; p < sz; p += FT) {
-            uint32_t id = ids[st + p];
-            float m = __fadd_rn(dot_exact(nv, a.X + size_t(id) * a.dp, a.d), off);
-            uint8_t code;
-            if (fabsf(m) < 1e-8f) {
-                code = 2;
-                anytie = 1;
-            } else {
-                code = m > 0.0f ? 1 : 0;
-            }
-            side[st + p] = code;
-        }
-        __syncthreads();
-        if (anytie) {  // ties draw from the Rng in position order
-            if (threadIdx.x == 0) {
-                Rng r{rng};
-                for (uint32_t p = 0; p < sz; ++p)
-                    if (side[st + p] == 2) side[st + p] = (r.next_u64() & 1ull) == 0 ? 1 : 0;
-                rng = r.s;
+        if (sz <= uint32_t(smax)) {
+            if (tb0) tclk = clock64();
+            for (uint32_t p = tid; p < sz; p += NT) {
+                S.sid[p] = ids[st + p];
+                S.sslot[p] = p;
             }
             __syncthreads();
+            const int q4 = dp / 4;
+            for (uint32_t t = tid; t < sz * q4; t += NT) {
+                uint32_t r = t / q4, j = t - r * q4;
+                reinterpret_cast<float4*>(rows)[t] =
+                    reinterpret_cast<const float4*>(a.X + size_t(S.sid[r]) * dp)[j];
+            }
+            __syncthreads();
+            if (tid < 32) {
+                warp_subtree<D>(a, S, rows, nv, st, sz, dep, rng, leaf);
+                if (tid == 0) S.rng = rng.s;
+            }
+            __syncthreads();
+            rng.s = S.rng;  // the other warps adopt warp 0's Rng state
+            for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = S.sid[p];
+            __syncthreads();
+            if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
+            if (tr && tid == 0) atomicAdd(&tr[SEQ_T_STAGED_TREES], 1ull);
+            continue;
         }
-        // nL
-        uint32_t cnt = 0;
-        for (uint32_t p = threadIdx.x; p < sz; p += FT) cnt += side[st + p];
-        uint32_t tot;
-        bscan(cnt, ws, &tot);
-        if (threadIdx.x == 0) {
-            snL = tot;
-            sc = 0;
+        // ── global mode ──
+        if (tb0) tclk = clock64();
+        if (tr && tid == 0) {
+            atomicAdd(&tr[SEQ_T_GLOBAL_NODES], 1ull);
+            atomicAdd(&tr[SEQ_T_GLOBAL_POINTS], (unsigned long long)sz);
+        }
+        uint32_t pa, pb;
+        draw_pair(rng, sz, pa, pb);
+        {
+            const uint32_t A = ids[st + pa], B = ids[st + pb];
+            for (int j = tid; j < 2 * dp; j += NT)
+                xab[j] = j < dp ? a.X[size_t(A) * dp + j] : a.X[size_t(B) * dp + (j - dp)];
+        }
+        if (tid == 0) {
+            S.anytie = 0;
+            S.cntL = 0;
+            S.sc = 0;
         }
         __syncthreads();
-        const uint32_t nL = snL;
-        // pass 1: tables and c; positions in tiles of FT*PER, PER consecutive per thread
+        for (int j = tid; j < dp; j += NT) nv[j] = j < d ? __fsub_rn(xab[j], xab[dp + j]) : 0.0f;
+        const float off = hyper_offset_t<D>(xab, xab + dp, d);
+        __syncthreads();
+        if (tb0) {
+            long long t1 = clock64();
+            tr[SEQ_T_CYC_DRAW] += t1 - tclk;
+            tclk = t1;
+        }
+        uint32_t cnt = 0;
+        bool tie = false;
+        constexpr int U = NT >= 512 ? 2 : 4;  // rows in flight per thread
+        for (uint32_t p0 = tid; p0 < sz; p0 += U * NT) {
+            uint32_t id[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t p = p0 + u * NT;
+                id[u] = ids[st + (p < sz ? p : p0)];
+            }
+            float m[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u)
+                m[u] = __fadd_rn(dot_exact_t<D>(nv, a.X + size_t(id[u]) * dp, d), off);
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const uint32_t p = p0 + u * NT;
+                if (p < sz) {
+                    const uint8_t c = fabsf(m[u]) < 1e-8f ? 2 : (m[u] > 0.0f ? 1 : 0);
+                    side[st + p] = c;
+                    tie |= c == 2;
+                    cnt += c == 1;
+                }
+            }
+        }
+        if (tie) S.anytie = 1;
+        cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+        if (lane == 0) atomicAdd(&S.cntL, cnt);
+        __syncthreads();
+        if (tb0) {
+            long long t1 = clock64();
+            tr[SEQ_T_CYC_MARGIN] += t1 - tclk;
+            tclk = t1;
+        }
+        if (S.anytie) {
+            if (tr && tid == 0) atomicAdd(&tr[SEQ_T_TIES], 1ull);
+            // every thread replays the tie draws; thread 0 writes the sides
+            uint32_t add = 0;
+            for (uint32_t p = 0; p < sz; ++p)
+                if (side[st + p] == 2) {
+                    uint8_t v = (rng.next_u64() & 1ull) == 0 ? 1 : 0;
+                    add += v;
+                    __syncthreads();
+                    if (tid == 0) side[st + p] = v;
+                    __syncthreads();
+                }
+            if (tid == 0) S.cntL += add;
+            __syncthreads();
+        }
+        const uint32_t nL = S.cntL;
         uint32_t carry = 0;
-        for (uint32_t t0 = 0; t0 < sz; t0 += FT * PER) {
-            uint8_t s[PER];
+        for (uint32_t t0 = 0; t0 < sz; t0 += NT * PERT) {
+            uint8_t s[PERT];
             uint32_t c2 = 0;
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                uint32_t p = t0 + threadIdx.x * PER + j;
+            for (int j = 0; j < PERT; ++j) {
+                uint32_t p = t0 + tid * PERT + j;
                 s[j] = p < sz ? side[st + p] : 0;
                 c2 += s[j];
             }
             uint32_t tt;
-            uint32_t lp = carry + bscan(c2, ws, &tt);
+            uint32_t lp = carry + bscan(c2, S.ws, &tt);
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                uint32_t p = t0 + threadIdx.x * PER + j;
+            for (int j = 0; j < PERT; ++j) {
+                uint32_t p = t0 + tid * PERT + j;
                 if (p < sz) {
                     if (s[j]) {
                         if (p >= nL) tabB[st + (nL - lp) - 1] = p;
                     } else if (p < nL) {
                         tabA[st + (p - lp)] = p;
                     }
-                    if (p == nL) sc = nL - lp;
+                    if (p == nL) S.sc = nL - lp;
                     lp += s[j];
                 }
             }
             carry += tt;
         }
         __syncthreads();
-        const uint32_t c = sc;
+        const uint32_t c = S.sc;
         carry = 0;
-        for (uint32_t t0 = 0; t0 < sz; t0 += FT * PER) {
-            uint8_t s[PER];
+        for (uint32_t t0 = 0; t0 < sz; t0 += NT * PERT) {
+            uint8_t s[PERT];
             uint32_t c2 = 0;
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                uint32_t p = t0 + threadIdx.x * PER + j;
+            for (int j = 0; j < PERT; ++j) {
+                uint32_t p = t0 + tid * PERT + j;
                 s[j] = p < sz ? side[st + p] : 0;
                 c2 += s[j];
             }
             uint32_t tt;
-            uint32_t lp = carry + bscan(c2, ws, &tt);
+            uint32_t lp = carry + bscan(c2, S.ws, &tt);
 #pragma unroll
-            for (int j = 0; j < PER; ++j) {
-                uint32_t p = t0 + threadIdx.x * PER + j;
+            for (int j = 0; j < PERT; ++j) {
+                uint32_t p = t0 + tid * PERT + j;
                 if (p < sz) {
                     uint32_t dst;
                     if (s[j]) {
                         dst = p < nL ? p : tabA[st + (nL - lp) - 1];
                     } else if (p < nL) {
-                        uint32_t r = p - lp + 1;
-                        dst = (r == 1 ? sz : tabB[st + r - 2]) - 1;
+                        uint32_t rr = p - lp + 1;
+                        dst = (rr == 1 ? sz : tabB[st + rr - 2]) - 1;
                     } else if (p > nL) {
                         dst = p - 1;
                     } else {
@@ -412,36 +647,39 @@ __global__ void __launch_bounds__(FT) k_seqtree(ForestArgs a, const SRoot* roots
             carry += tt;
         }
         __syncthreads();
-        for (uint32_t p = threadIdx.x; p < sz; p += FT) ids[st + p] = tmp[st + p];
+        for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = tmp[st + p];
         __syncthreads();
-        if (threadIdx.x == 0) {
-            uint32_t split = nL;
-            if (nL == 0 || nL == sz) {
-                Rng r{rng};
-                for (uint32_t i = sz - 1; i >= 1; --i) {
-                    uint32_t j = uint32_t(r.below(uint64_t(i) + 1));
+        uint32_t split = nL;
+        if (nL == 0 || nL == sz) {
+            if (tr && tid == 0) atomicAdd(&tr[SEQ_T_DEGENERATE], 1ull);
+            for (uint32_t i = sz - 1; i >= 1; --i) {
+                uint32_t j = uint32_t(rng.below(uint64_t(i) + 1));
+                if (tid == 0) {
                     uint32_t t = ids[st + i];
                     ids[st + i] = ids[st + j];
                     ids[st + j] = t;
                 }
-                rng = r.s;
-                split = sz / 2;
             }
-            if (sp + 2 > STK) {
+            split = sz / 2;
+        }
+        if (tid == 0) {
+            if (S.sp + 2 > STK) {
                 atomicExch(a.err, 1);
-                sp = 0;
+                S.sp = 0;
             } else {
-                stS[sp] = st + split;  // right, popped after the whole left subtree
-                stN[sp] = sz - split;
-                stD[sp] = uint16_t(dep + 1);
-                stS[sp + 1] = st;
-                stN[sp + 1] = split;
-                stD[sp + 1] = uint16_t(dep + 1);
-                sp += 2;
+                S.stS[S.sp] = st + split;  // right, popped after the whole left subtree
+                S.stN[S.sp] = sz - split;
+                S.stD[S.sp] = uint16_t(dep + 1);
+                S.stS[S.sp + 1] = st;
+                S.stN[S.sp + 1] = split;
+                S.stD[S.sp + 1] = uint16_t(dep + 1);
+                S.sp += 2;
             }
         }
         __syncthreads();
+        if (tb0) tr[SEQ_T_CYC_PART] += clock64() - tclk;
     }
+    if (tb0) tr[SEQ_T_CYC_TOTAL] = clock64() - t_start;
 }
 
 // Compact leaf starts of one tree: flags (u8) -> u32 -> exclusive scan -> positions.
@@ -455,32 +693,104 @@ __global__ void k_leaf_scatter(const uint8_t* f, const uint32_t* pre, uint32_t n
     if (i < n && f[i]) leaf_start[pre[i]] = i;
 }
 
-// Leaf all-pairs: a warp per leaf; each member receives every other member
-// in leaf order, which is the order the reference's (i<j, p-then-q)
-// generation addresses it (nndescent.rs:793-810).
-__global__ void __launch_bounds__(256) k_leaf_pairs(const float* __restrict__ X, int d, int dp,
-                                                    const uint32_t* __restrict__ ids,
-                                                    const uint32_t* __restrict__ leaf_start,
-                                                    uint32_t nleaves, uint32_t n, int k,
-                                                    uint32_t* hidx, float* hdist,
-                                                    uint8_t* hflag) {
-    uint32_t li = blockIdx.x * 8 + (threadIdx.x >> 5);
-    if (li >= nleaves) return;
-    const int lane = threadIdx.x & 31;
-    uint32_t ls = leaf_start[li];
-    uint32_t le = li + 1 < nleaves ? leaf_start[li + 1] : n;
-    uint32_t L = le - ls;
-    for (uint32_t mi = lane; mi < L; mi += 32) {
-        uint32_t p = ids[ls + mi];
-        const float* xp = X + size_t(p) * dp;
+// Leaf all-pairs of one tree (nndescent.rs:785-815).  The member at a
+// position receives every other member of its leaf in leaf order, which is
+// the order the reference's (i<j, p-then-q) generation addresses it.
+//
+// A CTA takes LPB consecutive leaves: it stages their ids, rows and heap
+// roots in shared memory once, computes each pair's distance once into a
+// per-position table, and then each thread replays its own member's pushes.
+// A push whose distance is not below the row's root (its current worst) is
+// rejected unchanged (nndescent.rs:176), so the heap row in HBM is touched
+// only when a mate beats the root.  Tiles whose span exceeds LCAP or whose
+// leaves exceed LMAX members take the direct path.
+constexpr int LPB = 16;     // leaves per CTA
+constexpr int LCAP = 256;   // staged positions per CTA (= threads)
+constexpr int LMAX = 32;    // largest leaf of the staged path
+
+template <int D>
+__global__ void __launch_bounds__(LCAP) k_leaf_pairs(
+    const float* __restrict__ X, int d, int dp, const uint32_t* __restrict__ ids,
+    const uint32_t* __restrict__ leaf_start, uint32_t nleaves, uint32_t n, int k, uint32_t* hidx,
+    float* hdist, uint8_t* hflag) {
+    extern __shared__ __align__(16) float lsm[];
+    __shared__ uint32_t sls[LPB + 1];
+    __shared__ int staged;
+    float* R = lsm;                               // LCAP * dp
+    float* Dt = lsm + size_t(LCAP) * dp;          // LCAP * LMAX
+    __shared__ uint32_t sid[LCAP];
+    __shared__ float sroot[LCAP];
+    __shared__ uint16_t sl0[LCAP], sl1[LCAP];     // leaf bounds of each staged position
+    const uint32_t L0 = blockIdx.x * LPB;
+    const uint32_t L1 = min(nleaves, L0 + LPB);
+    const int tid = threadIdx.x;
+    if (tid <= int(L1 - L0)) {
+        const uint32_t li = L0 + tid;
+        sls[tid] = li < nleaves ? leaf_start[li] : n;
+    }
+    __syncthreads();
+    const uint32_t P0 = sls[0], P1 = sls[L1 - L0];
+    const uint32_t span = P1 - P0;
+    if (tid == 0) {
+        bool ok = span <= uint32_t(LCAP);
+        for (uint32_t l = 0; l < L1 - L0; ++l) ok &= sls[l + 1] - sls[l] <= uint32_t(LMAX);
+        staged = ok;
+    }
+    __syncthreads();
+    if (!staged) {
+        for (uint32_t pos = P0 + tid; pos < P1; pos += LCAP) {
+            uint32_t l = 0;
+            while (sls[l + 1] <= pos) ++l;
+            const uint32_t ls = sls[l], le = sls[l + 1];
+            const uint32_t p = ids[pos];
+            const float* xp = X + size_t(p) * dp;
+            for (uint32_t qp = ls; qp < le; ++qp) {
+                if (qp == pos) continue;
+                const uint32_t q = ids[qp];
+                heap_push(hidx + size_t(p) * k, hdist + size_t(p) * k, hflag + size_t(p) * k, k,
+                          q, sq_dist_exact_t<D>(xp, X + size_t(q) * dp, d), 1);
+            }
+        }
+        return;
+    }
+    if (uint32_t(tid) < span) {
+        const uint32_t p = ids[P0 + tid];
+        sid[tid] = p;
+        sroot[tid] = hdist[size_t(p) * k];
+        uint32_t l = 0;
+        while (sls[l + 1] <= P0 + tid) ++l;
+        sl0[tid] = uint16_t(sls[l] - P0);
+        sl1[tid] = uint16_t(sls[l + 1] - P0);
+    }
+    __syncthreads();
+    const int q4 = dp / 4;
+    for (uint32_t t = tid; t < span * q4; t += LCAP) {
+        const uint32_t r = t / q4, j = t - r * q4;
+        reinterpret_cast<float4*>(R)[t] = reinterpret_cast<const float4*>(X + size_t(sid[r]) * dp)[j];
+    }
+    __syncthreads();
+    if (uint32_t(tid) < span) {  // each pair once: this position with its later mates
+        const uint32_t l0 = sl0[tid], l1 = sl1[tid];
+        for (uint32_t j = tid + 1; j < l1; ++j) {
+            const float dd = sq_dist_exact_t<D>(R + size_t(tid) * dp, R + size_t(j) * dp, d);
+            Dt[size_t(tid) * LMAX + (j - l0)] = dd;
+            Dt[size_t(j) * LMAX + (tid - l0)] = dd;
+        }
+    }
+    __syncthreads();
+    if (uint32_t(tid) < span) {
+        const uint32_t l0 = sl0[tid], l1 = sl1[tid];
+        const uint32_t p = sid[tid];
+        float root = sroot[tid];
         uint32_t* ri = hidx + size_t(p) * k;
         float* rd = hdist + size_t(p) * k;
         uint8_t* rf = hflag + size_t(p) * k;
-        for (uint32_t qi = 0; qi < L; ++qi) {
-            if (qi == mi) continue;
-            uint32_t q = ids[ls + qi];
-            float dd = sq_dist_exact(xp, X + size_t(q) * dp, d);
-            heap_push(ri, rd, rf, k, q, dd, 1);
+        for (uint32_t j = l0; j < l1; ++j) {
+            if (j == uint32_t(tid)) continue;
+            const float dd = Dt[size_t(tid) * LMAX + (j - l0)];
+            if (dd >= root) continue;  // heap_push would reject it unchanged
+            heap_push(ri, rd, rf, k, sid[j], dd, 1);
+            root = rd[0];
         }
     }
 }
@@ -526,9 +836,32 @@ void launch_partition(const ForestArgs& a, PNode* nodes, const uint32_t* chunk_n
 void launch_degenerate(const ForestArgs& a, PNode* nodes, uint32_t nn, cudaStream_t st) {
     k_degenerate<<<(nn + 63) / 64, 64, 0, st>>>(a, nodes, nn); count_launch();
 }
-void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t nr, cudaStream_t st) {
+template <int NT, int D>
+static void seqtree_launch(const ForestArgs& a, const SRoot* roots, uint32_t nr, int smax,
+                           size_t dyn, cudaStream_t st) {
     if (nr == 0) return;
-    k_seqtree<<<nr, FT, size_t(a.dp) * sizeof(float), st>>>(a, roots); count_launch();
+    if (dyn > 40 * 1024)
+        cudaFuncSetAttribute(k_seqtree<NT, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(dyn));
+    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax); count_launch();
+}
+
+void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, uint32_t nr,
+                     cudaStream_t st, cudaStream_t st_big) {
+    if (nr == 0) return;
+    // staged capacity: as many rows as fit beside the hyperplane rows in ~28 KB
+    size_t row = size_t(a.dp) * sizeof(float);
+    int smax = int(std::min<size_t>(SCAP, (28 * 1024) / row));
+    if (smax < 2) smax = 0;
+    size_t dyn = row * (3 + size_t(smax));
+    // roots[0, n_big) are the largest subtrees: 512 threads each, own stream
+    if (a.d == 50) {
+        seqtree_launch<512, 50>(a, roots, n_big, smax, dyn, st_big);
+        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, dyn, st);
+    } else {
+        seqtree_launch<512, 0>(a, roots, n_big, smax, dyn, st_big);
+        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, dyn, st);
+    }
 }
 void launch_leaf_compact(const uint8_t* leafflag_t, uint32_t n, uint32_t* leaf_start,
                          uint32_t* scan_buf, void* scan_temp, uint64_t* count_dev,
@@ -541,8 +874,21 @@ void launch_leaf_pairs(const float* X, int d, int dp, const uint32_t* ids_t,
                        const uint32_t* leaf_start, uint32_t nleaves, uint32_t n, int k,
                        uint32_t* hidx, float* hdist, uint8_t* hflag, cudaStream_t st) {
     if (nleaves == 0) return;
-    k_leaf_pairs<<<(nleaves + 7) / 8, 256, 0, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
-                                                    hidx, hdist, hflag); count_launch();
+    const size_t sm = (size_t(LCAP) * dp + size_t(LCAP) * LMAX) * sizeof(float);
+    const unsigned grid = (nleaves + LPB - 1) / LPB;
+    if (d == 50) {
+        if (sm > 40 * 1024)
+            cudaFuncSetAttribute(k_leaf_pairs<50>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sm));
+        k_leaf_pairs<50><<<grid, LCAP, sm, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
+                                                 hidx, hdist, hflag); count_launch();
+    } else {
+        if (sm > 40 * 1024)
+            cudaFuncSetAttribute(k_leaf_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 int(sm));
+        k_leaf_pairs<0><<<grid, LCAP, sm, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
+                                                hidx, hdist, hflag); count_launch();
+    }
 }
 void launch_random_fill(const float* X, int d, int dp, uint32_t n, int k, uint64_t seed,
                         uint32_t* hidx, float* hdist, uint8_t* hflag, cudaStream_t st) {

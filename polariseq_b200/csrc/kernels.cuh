@@ -1,6 +1,6 @@
 // Kernel entry points of the plain (bit-exact) NN-Descent, shared between the
 // phase drivers.  All device arrays are described where they are declared in
-// the host driver (nnd_plain.cu).
+// the host driver (api.cu).
 #pragma once
 
 #include <cuda_runtime.h>
@@ -39,6 +39,24 @@ struct ForestArgs {
     uint32_t* tabB;      // T x n: positions of left points in the right segment, by rank from the top
     uint8_t* leafflag;   // T x n: 1 where a leaf starts
     int* err;            // device error flag
+    unsigned long long* trace;  // optional: SEQ_TRACE_N counters (POLARISEQ_TRACE)
+};
+
+// Trace counters of the depth-first subtree kernel.
+enum {
+    SEQ_T_GLOBAL_NODES = 0,   // nodes split in global mode
+    SEQ_T_GLOBAL_POINTS = 1,  // margins evaluated in global mode
+    SEQ_T_STAGED_TREES = 2,   // staged subtrees
+    SEQ_T_STAGED_NODES = 3,   // nodes split in staged subtrees
+    SEQ_T_TIES = 4,           // nodes with tie draws
+    SEQ_T_DEGENERATE = 5,     // random splits
+    SEQ_T_CYC_DRAW = 6,       // block 0 cycles: draws + hyperplane rows
+    SEQ_T_CYC_MARGIN = 7,     // block 0 cycles: global-mode margins
+    SEQ_T_CYC_PART = 8,       // block 0 cycles: global-mode partition
+    SEQ_T_CYC_STAGED = 9,     // block 0 cycles: staged subtrees
+    SEQ_T_CYC_TOTAL = 10,     // block 0 cycles: whole kernel
+    SEQ_T_ROOT0 = 11,         // block 0 root size
+    SEQ_TRACE_N = 16
 };
 
 constexpr int FOREST_CHUNK = 2048;
@@ -51,7 +69,9 @@ void launch_node_scan(PNode* nodes, uint32_t nn, uint32_t* chunkL, cudaStream_t 
 void launch_partition(const ForestArgs& a, PNode* nodes, const uint32_t* chunk_node,
                       uint32_t nchunks, const uint32_t* chunkPre, cudaStream_t st);
 void launch_degenerate(const ForestArgs& a, PNode* nodes, uint32_t nn, cudaStream_t st);
-void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t nr, cudaStream_t st);
+// roots sorted by size, descending; the first n_big run with 512 threads on st_big.
+void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, uint32_t nr,
+                     cudaStream_t st, cudaStream_t st_big);
 
 // Leaf all-pairs of one tree into the heaps (nndescent.rs:785-815).
 void launch_leaf_pairs(const float* X, int d, int dp, const uint32_t* ids_t,
@@ -73,14 +93,15 @@ void launch_cand_apply(const uint32_t* keys, const uint64_t* vals, const uint32_
                        float* new_prio, uint32_t* old_idx, float* old_prio, cudaStream_t st);
 void launch_flag_flip(const uint32_t* hidx, uint8_t* hflag, const uint32_t* new_idx, uint32_t n,
                       int k, int m, cudaStream_t st);
+// perm (may be null): the order in which CTAs visit source rows.
 void launch_join_count(const float* X, int d, int dp, uint32_t n, int k, int m,
                        const float* hdist, const uint32_t* new_idx, const uint32_t* old_idx,
-                       uint32_t* bits, int words, uint32_t* row_cnt,
+                       const uint32_t* perm, uint32_t* bits, int words, uint32_t* row_cnt,
                        unsigned long long* pairs, cudaStream_t st);
 void launch_join_write(const float* X, int d, int dp, uint32_t n, int m, const uint32_t* new_idx,
-                       const uint32_t* old_idx, const uint32_t* bits, int words,
-                       const uint32_t* row_off, uint32_t* keys, uint64_t* vals, uint32_t* dcnt,
-                       cudaStream_t st);
+                       const uint32_t* old_idx, const uint32_t* perm, const uint32_t* bits,
+                       int words, const uint32_t* row_cnt, const uint32_t* row_off,
+                       uint32_t* keys, uint64_t* vals, uint32_t* dcnt, cudaStream_t st);
 void launch_replay(const uint32_t* keys, const uint64_t* vals, const uint32_t* seg_off,
                    const uint32_t* dcnt, uint32_t n, int k, uint32_t* hidx, float* hdist,
                    uint8_t* hflag, unsigned long long* changed, cudaStream_t st);
