@@ -54,6 +54,7 @@ def parse():
     ap.add_argument("--queries", type=int, default=20_000)
     ap.add_argument("--cpu-sample", type=int, default=262_144)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--form", default="plain", choices=["plain", "bf16"])
     ap.add_argument("--profile-only", action="store_true",
                     help="run W warm-up and K device-resident builds, print nothing else "
                          "(for ncu launch lists)")
@@ -69,7 +70,9 @@ def workload(args, rank):
 def config(args):
     return {"workload": f"kNN graph build, {args.n} cells x {args.d} PCs f32, k={args.k}, "
                         f"{args.comps}-component log-normal Gaussian mixture, 5% doublets",
-            "n_cells": args.n, "n_pcs": args.d, "k": args.k, "form": "plain (bit-exact)",
+            "n_cells": args.n, "n_pcs": args.d, "k": args.k,
+            "form": "plain (bit-exact)" if args.form == "plain" else
+                    "bf16 tensor-core shortlist + FP32 re-rank + FP64 boundary",
             "l2": "inputs larger than L2 (embedding 800 MB, graph 480 MB)"}
 
 
@@ -231,7 +234,7 @@ def main():
     n, d, k = x.shape[0], x.shape[1], args.k
     cap = n * pq.effective_k(n, k)
     ctx = pq.Context(local)
-    opts = pq._opts(k, 0, 0, 0, 0, 0.001)
+    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[args.form])
     stream = torch.cuda.current_stream(dev)
     xd = torch.from_numpy(x).to(dev)
     ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
@@ -299,12 +302,13 @@ def main():
     hdx = torch.empty(cap, dtype=torch.float32).pin_memory()
     hxn, hipn = hx.numpy(), hip.numpy().view(np.uint32)
     hixn, hdxn = hix.numpy().view(np.uint32), hdx.numpy()
-    pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local)  # warm the host path
+    pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local,
+                       mode=args.form)  # warm the host path
     barrier()
     t0 = time.perf_counter()
     e2e_steps = max(1, min(args.steps, 3))
     for _ in range(e2e_steps):
-        r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local)
+        r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
     e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
     if world > 1:
         t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)

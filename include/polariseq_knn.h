@@ -53,6 +53,9 @@ typedef struct pq_nnd_opts {
     uint64_t seed;
     int32_t mode;            /* PQ_MODE_* */
     int32_t init;            /* PQ_INIT_* */
+    /* Tensor-core forms only (ignored by PQ_MODE_PLAIN): */
+    int32_t probes;          /* buckets each cell searches; 0 -> min(12, buckets) */
+    int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (2) */
 } pq_nnd_opts;
 
 /* Per-call statistics of the last build on a context. */

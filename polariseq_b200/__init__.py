@@ -47,7 +47,8 @@ def effective_k(n_obs: int, k: int) -> int:
 
 
 def _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size=0, gather_max=0,
-          mode=_lib.PQ_MODE_PLAIN, init=_lib.PQ_INIT_RP) -> _lib.NndOpts:
+          mode=_lib.PQ_MODE_PLAIN, init=_lib.PQ_INIT_RP, probes=0,
+          refine_rounds=-1) -> _lib.NndOpts:
     o = _lib.NndOpts()
     _lib.load().pq_nnd_opts_default(C.byref(o))
     o.k = int(k)
@@ -60,6 +61,8 @@ def _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size=0, 
     o.gather_max = int(gather_max)
     o.mode = int(mode)
     o.init = int(init)
+    o.probes = int(probes)
+    o.refine_rounds = int(refine_rounds)
     return o
 
 
@@ -207,13 +210,23 @@ def _as_out(arr, dtype, name):
     return arr
 
 
+MODES = {"plain": _lib.PQ_MODE_PLAIN, "bf16": _lib.PQ_MODE_BF16, "fp8": _lib.PQ_MODE_FP8}
+INITS = {"rp": _lib.PQ_INIT_RP, "learned": _lib.PQ_INIT_LEARNED}
+
+
 def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_trees=0,
-                    delta=0.001, out=None, *, device: int = 0):
+                    delta=0.001, out=None, *, device: int = 0, mode: str = "plain",
+                    init: str = "rp", probes: int = 0, refine_rounds: int = -1):
     """Approximate kNN graph by NN-Descent, bit-exact with the reference
-    (crates/polariseq-python/src/lib.rs:503-566)."""
+    (crates/polariseq-python/src/lib.rs:503-566).
+
+    ``mode='plain'`` (default) reproduces the reference graph bit for bit;
+    ``mode='bf16'`` is the tensor-core shortlist form (bucketed BF16 distance
+    tiles, exact FP32 re-rank, FP64 boundary) with the same output layout."""
     emb = _as_embedding(embedding)
     n_obs, _ = emb.shape
-    opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta)
+    opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta, mode=MODES[mode],
+                 init=INITS[init], probes=probes, refine_rounds=refine_rounds)
     cap = n_obs * effective_k(n_obs, k)
     # the same order as the binding: the out sizes are validated (ValueError)
     # before the core runs and panics on empty data or k == 0
@@ -240,7 +253,9 @@ def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_
 
 
 def nndescent(data: np.ndarray, k: int = 15, *, max_candidates=0, max_iterations=0, delta=0.001,
-              n_trees=0, leaf_size=0, gather_max=0, seed=0, device: int = 0) -> dict:
+              n_trees=0, leaf_size=0, gather_max=0, seed=0, device: int = 0,
+              mode: str = "plain", init: str = "rp", probes: int = 0,
+              refine_rounds: int = -1) -> dict:
     """The Rust-level ``nndescent(data, n_obs, n_dim, &NndescentOptions)``
     (nndescent.rs:657-686) with every option, returning the NeighborGraph
     fields (indptr, indices, data, n_obs)."""
@@ -250,7 +265,8 @@ def nndescent(data: np.ndarray, k: int = 15, *, max_candidates=0, max_iterations
         raise PanicException("empty data")
     if int(k) == 0:
         raise PanicException("k must be >= 1")
-    opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size, gather_max)
+    opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size, gather_max,
+                 mode=MODES[mode], init=INITS[init], probes=probes, refine_rounds=refine_rounds)
     cap = n_obs * effective_k(n_obs, k)
     ip = np.zeros(n_obs + 1, np.uint32)
     ix = np.zeros(cap, np.uint32)

@@ -38,6 +38,8 @@ class NndOpts(C.Structure):
         ("seed", C.c_uint64),
         ("mode", C.c_int32),
         ("init", C.c_int32),
+        ("probes", C.c_int32),
+        ("refine_rounds", C.c_int32),
     ]
 
 

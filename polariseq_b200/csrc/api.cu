@@ -4,17 +4,10 @@
 // (crates/polariseq-core/src/nndescent.rs:708-752), pads the embedding to
 // 16-byte rows in HBM, then runs the plain form's phases on the context's
 // stream: RP forest, leaf pairs, random fill, rounds, extract.
-#include <algorithm>
-#include <cmath>
-#include <cstdlib>
 #include <cstdio>
-#include <cstring>
-#include <map>
-#include <string>
-#include <vector>
+#include <functional>
 
-#include "../../include/polariseq_knn.h"
-#include "common.cuh"
+#include "ctx.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
@@ -22,107 +15,9 @@ namespace pq {
 unsigned long long g_launches = 0;
 }
 
-namespace {
-
-struct Buf {
-    void* p = nullptr;
-    size_t bytes = 0;
-};
-
-struct Resolved {
-    uint64_t k, max_cand, n_iters, n_trees, leaf_size, stop_at;
-};
-
-}  // namespace
-
-struct pq_ctx {
-    int device = 0;
-    cudaStream_t stream = nullptr;
-    std::string err;
-    pq_nnd_stats stats{};
-    std::map<std::string, Buf> bufs;
-    int* d_err = nullptr;
-    uint64_t* d_u64 = nullptr;            // small device scalars
-    unsigned long long* d_acc = nullptr;  // device accumulators
-    cudaStream_t stream2 = nullptr;  // the largest subtrees run here, concurrently
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-    int profile = 0;
-    struct KGRec {
-        cudaEvent_t a, b;
-        int group;
-        unsigned long long launches;
-    };
-    std::vector<KGRec> kg_pending;
-
-    template <class T>
-    T* get(const std::string& name, size_t count) {
-        size_t need = count * sizeof(T);
-        if (need == 0) need = 16;
-        Buf& b = bufs[name];
-        if (b.bytes < need) {
-            if (b.p) {
-                cudaStreamSynchronize(stream);
-                cudaFree(b.p);
-                b.p = nullptr;
-                b.bytes = 0;
-            }
-            size_t alloc = need + need / 8;  // headroom for slightly larger calls
-            if (cudaMalloc(&b.p, alloc) != cudaSuccess) {
-                cudaGetLastError();
-                throw std::string("device allocation of ") + std::to_string(alloc) +
-                    " bytes failed (" + name + ")";
-            }
-            b.bytes = alloc;
-        }
-        return static_cast<T*>(b.p);
-    }
-};
+using namespace pqh;
 
 namespace {
-
-struct DeviceError {
-    std::string msg;
-};
-
-void ck(cudaError_t e, const char* where) {
-    if (e != cudaSuccess) throw DeviceError{std::string(where) + ": " + cudaGetErrorString(e)};
-}
-
-uint64_t effective_k(uint64_t n, uint64_t k) {
-    uint64_t m = n > 0 ? n - 1 : 0;
-    uint64_t e = k < m ? k : m;
-    return e > 0 ? e : 1;
-}
-
-Resolved resolve(uint64_t n, const pq_nnd_opts& o) {
-    Resolved r;
-    r.k = effective_k(n, o.k);
-    uint64_t mc = o.max_candidates > 0 ? o.max_candidates : std::min<uint64_t>(2 * r.k, 60);
-    r.max_cand = mc > 0 ? mc : 1;
-    if (o.max_iterations > 0) {
-        r.n_iters = o.max_iterations;
-    } else {
-        double lg = std::round(std::log2(double(n)));
-        uint64_t it = lg > 0 ? uint64_t(lg) : 0;
-        r.n_iters = it > 5 ? it : 5;
-    }
-    if (o.n_trees > 0) {
-        r.n_trees = o.n_trees;
-    } else {
-        double t = std::round(std::sqrt(double(n)) / 10.0);
-        r.n_trees = std::min<uint64_t>(8 + uint64_t(t), 48);
-    }
-    r.leaf_size = o.leaf_size > 0 ? o.leaf_size : std::max<uint64_t>(r.k, 10);
-    double sa = o.delta * double(n) * double(r.k);
-    r.stop_at = (sa > 0 && sa == sa) ? (sa >= 1.8e19 ? UINT64_MAX : uint64_t(sa)) : 0;
-    return r;
-}
-
-int key_bits(uint64_t maxkey) {
-    int b = 0;
-    while (b < 32 && (maxkey >> b) != 0) ++b;
-    return b > 0 ? b : 1;
-}
 
 __global__ void k_fill_u32(uint32_t* p, size_t n, uint32_t v) {
     size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -135,64 +30,6 @@ __global__ void k_fill_f32(float* p, size_t n, float v) {
 __global__ void k_iota_trees(uint32_t* ids, uint32_t n, uint32_t T) {
     size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < size_t(n) * T) ids[i] = uint32_t(i % n);
-}
-
-unsigned blocks(size_t n, int t) { return unsigned((n + t - 1) / t); }
-
-struct Timer {
-    cudaEvent_t a, b;
-    cudaStream_t s;
-    explicit Timer(cudaStream_t st) : s(st) {
-        cudaEventCreate(&a);
-        cudaEventCreate(&b);
-    }
-    ~Timer() {
-        cudaEventDestroy(a);
-        cudaEventDestroy(b);
-    }
-    void start() { cudaEventRecord(a, s); }
-    double stop() {
-        cudaEventRecord(b, s);
-        cudaEventSynchronize(b);
-        float ms = 0;
-        cudaEventElapsedTime(&ms, a, b);
-        return ms;
-    }
-};
-
-// Brackets one kernel group with CUDA events on the context's stream when
-// profiling is on; the records are summed into the stats at the end.
-struct KGScope {
-    pq_ctx* c;
-    int g;
-    cudaEvent_t a{}, b{};
-    unsigned long long l0;
-    KGScope(pq_ctx* c_, int g_) : c(c_), g(g_), l0(pq::g_launches) {
-        if (c->profile) {
-            cudaEventCreate(&a);
-            cudaEventCreate(&b);
-            cudaEventRecord(a, c->stream);
-        }
-    }
-    ~KGScope() {
-        if (c->profile) {
-            cudaEventRecord(b, c->stream);
-            c->kg_pending.push_back({a, b, g, pq::g_launches - l0});
-        }
-    }
-};
-
-void kg_collect(pq_ctx* c) {
-    cudaStreamSynchronize(c->stream);
-    for (auto& r : c->kg_pending) {
-        float ms = 0;
-        cudaEventElapsedTime(&ms, r.a, r.b);
-        c->stats.kg_ms[r.group] += ms;
-        c->stats.kg_launches[r.group] += r.launches;
-        cudaEventDestroy(r.a);
-        cudaEventDestroy(r.b);
-    }
-    c->kg_pending.clear();
 }
 
 // Host-side probe destinations.
@@ -210,6 +47,109 @@ struct Probe {
     uint64_t* n_leaves = nullptr;
     bool done = false;
 };
+
+// NN-Descent rounds (nndescent.rs:853-975) on the heaps in place: candidate
+// sampling, flag flip, ordered join and per-destination replay, until a round
+// changes at most stop_at entries.  Round statistics go to stats slots
+// [stats_offset, ...).  `perm` orders the join CTAs (spatially coherent rows
+// share candidate rows in L2).  Returns the rounds run (negative if
+// after_round asked to stop).
+}  // namespace
+
+namespace pqh {
+int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m, uint64_t seed,
+               uint64_t n_iters, uint64_t stop_at, uint32_t* hidx, float* hdist, uint8_t* hflag,
+               const uint32_t* perm, int stats_offset,
+               const std::function<bool(int, const uint32_t*, const uint32_t*)>& after_round) {
+    using namespace pq;
+    cudaStream_t st = c->stream;
+    pq_nnd_stats& S = c->stats;
+    uint32_t* new_idx = c->get<uint32_t>("new_idx", size_t(n) * m);
+    float* new_prio = c->get<float>("new_prio", size_t(n) * m);
+    uint32_t* old_idx = c->get<uint32_t>("old_idx", size_t(n) * m);
+    float* old_prio = c->get<float>("old_prio", size_t(n) * m);
+    uint32_t* dcnt = c->get<uint32_t>("dcnt", n);
+    uint32_t* seg_off = c->get<uint32_t>("seg_off", n);
+    uint32_t* row_cnt = c->get<uint32_t>("row_cnt", n);
+    const int words = (4 * m * m + 31) / 32;
+    uint32_t* bits = c->get<uint32_t>("bits", size_t(n) * words);
+    void* stemp = c->get<uint8_t>("scan_temp", scan_temp_bytes(n));
+    const size_t nrec_c = 2 * size_t(n) * k;
+    int rounds = 0;
+    for (uint64_t iter = 0; iter < n_iters; ++iter) {
+        // candidates
+        uint32_t* ck_ = c->get<uint32_t>("ckeys", nrec_c);
+        uint64_t* cv = c->get<uint64_t>("cvals", nrec_c);
+        uint32_t* ck2 = c->get<uint32_t>("ckeys2", nrec_c);
+        uint64_t* cv2 = c->get<uint64_t>("cvals2", nrec_c);
+        void* rtemp = c->get<uint8_t>("radix_temp_c", radix_temp_bytes(nrec_c));
+        {
+            KGScope kg(c, PQ_KG_CANDIDATES);
+            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
+            launch_cand_gen(hidx, hflag, n, k, seed, uint32_t(iter), ck_, cv, dcnt, st);
+            ck(radix_sort_pairs(ck_, cv, ck2, cv2, nrec_c, key_bits(n), rtemp, st), "sort cand");
+            ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan cand");
+            launch_cand_apply(ck_, cv, seg_off, dcnt, n, m, new_idx, new_prio, old_idx, old_prio,
+                              st);
+            launch_flag_flip(hidx, hflag, new_idx, n, k, m, st);
+        }
+        // join
+        ck(cudaMemsetAsync(c->d_acc, 0, 2 * sizeof(unsigned long long), st), "memset acc");
+        {
+            KGScope kg(c, PQ_KG_JOIN_COUNT);
+            launch_join_count(X, d, dp, n, k, m, hdist, new_idx, old_idx, perm, bits, words,
+                              row_cnt, c->d_acc, st);
+        }
+        uint32_t* row_off = seg_off;  // free until the replay's segments are computed
+        ck(scan_exclusive_u32(row_cnt, row_off, n, stemp, c->d_u64, st), "scan join");
+        uint64_t total = 0;
+        ck(cudaMemcpyAsync(&total, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "total");
+        ck(cudaStreamSynchronize(st), "join count");
+        if (total >= 0xFFFFFFFFull) throw DeviceError{"join: more than 2^32 updates in a round"};
+        uint64_t changed = 0;
+        if (total > 0) {
+            uint32_t* jk = c->get<uint32_t>("jkeys", total);
+            uint64_t* jv = c->get<uint64_t>("jvals", total);
+            uint32_t* jk2 = c->get<uint32_t>("jkeys2", total);
+            uint64_t* jv2 = c->get<uint64_t>("jvals2", total);
+            void* rtj = c->get<uint8_t>("radix_temp_j", radix_temp_bytes(total));
+            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
+            {
+                KGScope kg(c, PQ_KG_JOIN_WRITE);
+                launch_join_write(X, d, dp, n, m, new_idx, old_idx, perm, bits, words, row_cnt,
+                                  row_off, jk, jv, dcnt, st);
+            }
+            {
+                KGScope kg(c, PQ_KG_SORT);
+                ck(radix_sort_pairs(jk, jv, jk2, jv2, total, key_bits(n > 1 ? n - 1 : 1), rtj,
+                                    st),
+                   "sort join");
+                ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan replay");
+            }
+            {
+                KGScope kg(c, PQ_KG_REPLAY);
+                launch_replay(jk, jv, seg_off, dcnt, n, k, hidx, hdist, hflag, c->d_acc + 1, st);
+            }
+        }
+        unsigned long long acc[2];
+        ck(cudaMemcpyAsync(acc, c->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st), "acc");
+        ck(cudaStreamSynchronize(st), "round");
+        changed = acc[1];
+        const uint64_t slot = stats_offset + iter;
+        if (slot < 64) {
+            S.changed[slot] = changed;
+            S.emitted[slot] = total;
+            S.pairs[slot] = acc[0];
+        }
+        rounds = int(iter + 1);
+        if (after_round && after_round(int(iter), new_idx, old_idx)) return -rounds;
+        if (changed <= stop_at) break;
+    }
+    return rounds;
+}
+}  // namespace pqh
+
+namespace {
 
 // The plain form on device data.  Returns nnz (outputs written) unless the
 // probe stopped early.
@@ -426,7 +366,7 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
         KGScope kg(c, PQ_KG_LEAF_PAIRS);
         for (uint32_t t = 0; t < T; ++t)
             launch_leaf_pairs(X, d, dp, fa.ids + size_t(t) * n, leaf_start + size_t(t) * n,
-                              uint32_t(hc[t]), n, k, hidx, hdist, hflag, st);
+                              uint32_t(hc[t]), n, k, fa.leaf_size, hidx, hdist, hflag, st);
         launch_random_fill(X, d, dp, n, k, seed, hidx, hdist, hflag, st);
         ck(cudaGetLastError(), "leaf pairs");
     }
@@ -449,103 +389,32 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
 
     // ── rounds ──
     tm.start();
-    uint32_t* new_idx = c->get<uint32_t>("new_idx", size_t(n) * m);
-    float* new_prio = c->get<float>("new_prio", size_t(n) * m);
-    uint32_t* old_idx = c->get<uint32_t>("old_idx", size_t(n) * m);
-    float* old_prio = c->get<float>("old_prio", size_t(n) * m);
-    uint32_t* dcnt = c->get<uint32_t>("dcnt", n);
-    uint32_t* seg_off = c->get<uint32_t>("seg_off", n);
-    uint32_t* row_cnt = c->get<uint32_t>("row_cnt", n);
-    const int words = (4 * m * m + 31) / 32;
-    uint32_t* bits = c->get<uint32_t>("bits", size_t(n) * words);
-    void* stemp = c->get<uint8_t>("scan_temp", scan_temp_bytes(n));
-    const size_t nrec_c = 2 * size_t(n) * k;
-    // join CTAs visit source rows in tree 0's leaf order (spatially coherent)
-    const uint32_t* perm = fa.ids;
-    for (uint64_t iter = 0; iter < R.n_iters; ++iter) {
-        // candidates
-        uint32_t* ck_ = c->get<uint32_t>("ckeys", nrec_c);
-        uint64_t* cv = c->get<uint64_t>("cvals", nrec_c);
-        uint32_t* ck2 = c->get<uint32_t>("ckeys2", nrec_c);
-        uint64_t* cv2 = c->get<uint64_t>("cvals2", nrec_c);
-        void* rtemp = c->get<uint8_t>("radix_temp_c", radix_temp_bytes(nrec_c));
-        {
-            KGScope kg(c, PQ_KG_CANDIDATES);
-            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
-            launch_cand_gen(hidx, hflag, n, k, seed, uint32_t(iter), ck_, cv, dcnt, st);
-            ck(radix_sort_pairs(ck_, cv, ck2, cv2, nrec_c, key_bits(n), rtemp, st), "sort cand");
-            ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan cand");
-            launch_cand_apply(ck_, cv, seg_off, dcnt, n, m, new_idx, new_prio, old_idx, old_prio,
-                              st);
-            launch_flag_flip(hidx, hflag, new_idx, n, k, m, st);
-        }
-        // join
-        ck(cudaMemsetAsync(c->d_acc, 0, 2 * sizeof(unsigned long long), st), "memset acc");
-        {
-            KGScope kg(c, PQ_KG_JOIN_COUNT);
-            launch_join_count(X, d, dp, n, k, m, hdist, new_idx, old_idx, perm, bits, words,
-                              row_cnt, c->d_acc, st);
-        }
-        uint32_t* row_off = seg_off;  // free until the replay's segments are computed
-        ck(scan_exclusive_u32(row_cnt, row_off, n, stemp, c->d_u64, st), "scan join");
-        uint64_t total = 0;
-        ck(cudaMemcpyAsync(&total, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "total");
-        ck(cudaStreamSynchronize(st), "join count");
-        if (total >= 0xFFFFFFFFull) throw DeviceError{"join: more than 2^32 updates in a round"};
-        uint64_t changed = 0;
-        if (total > 0) {
-            uint32_t* jk = c->get<uint32_t>("jkeys", total);
-            uint64_t* jv = c->get<uint64_t>("jvals", total);
-            uint32_t* jk2 = c->get<uint32_t>("jkeys2", total);
-            uint64_t* jv2 = c->get<uint64_t>("jvals2", total);
-            void* rtj = c->get<uint8_t>("radix_temp_j", radix_temp_bytes(total));
-            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
-            {
-                KGScope kg(c, PQ_KG_JOIN_WRITE);
-                launch_join_write(X, d, dp, n, m, new_idx, old_idx, perm, bits, words, row_cnt,
-                                  row_off, jk, jv, dcnt, st);
-            }
-            {
-                KGScope kg(c, PQ_KG_SORT);
-                ck(radix_sort_pairs(jk, jv, jk2, jv2, total, key_bits(n > 1 ? n - 1 : 1), rtj,
-                                    st),
-                   "sort join");
-                ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan replay");
-            }
-            {
-                KGScope kg(c, PQ_KG_REPLAY);
-                launch_replay(jk, jv, seg_off, dcnt, n, k, hidx, hdist, hflag, c->d_acc + 1, st);
-            }
-        }
-        unsigned long long acc[2];
-        ck(cudaMemcpyAsync(acc, c->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st), "acc");
-        ck(cudaStreamSynchronize(st), "round");
-        changed = acc[1];
-        if (iter < 64) {
-            S.changed[iter] = changed;
-            S.emitted[iter] = total;
-            S.pairs[iter] = acc[0];
-        }
-        S.rounds_run = int32_t(iter + 1);
-        if (probe && probe->stop_after == int32_t(iter)) {
-            copy_heaps();
-            if (probe->cand_new)
-                ck(cudaMemcpy(probe->cand_new, new_idx, size_t(n) * m * 4,
-                              cudaMemcpyDeviceToHost),
-                   "p");
-            if (probe->cand_old)
-                ck(cudaMemcpy(probe->cand_old, old_idx, size_t(n) * m * 4,
-                              cudaMemcpyDeviceToHost),
-                   "p");
-            probe->done = true;
-            return 0;
-        }
-        if (changed <= R.stop_at) break;
+    {
+        // join CTAs visit source rows in tree 0's leaf order (spatially coherent)
+        const int r = run_rounds(
+            c, X, d, dp, n, k, m, seed, R.n_iters, R.stop_at, hidx, hdist, hflag, fa.ids, 0,
+            [&](int iter, const uint32_t* new_idx, const uint32_t* old_idx) {
+                if (!probe || probe->stop_after != iter) return false;
+                copy_heaps();
+                if (probe->cand_new)
+                    ck(cudaMemcpy(probe->cand_new, new_idx, size_t(n) * m * 4,
+                                  cudaMemcpyDeviceToHost),
+                       "p");
+                if (probe->cand_old)
+                    ck(cudaMemcpy(probe->cand_old, old_idx, size_t(n) * m * 4,
+                                  cudaMemcpyDeviceToHost),
+                       "p");
+                probe->done = true;
+                return true;
+            });
+        S.rounds_run = r < 0 ? -r : r;
+        if (r < 0) return 0;
     }
     S.ms_rounds = tm.stop();
 
     // ── extract ──
     tm.start();
+    void* stemp = c->get<uint8_t>("scan_temp", scan_temp_bytes(n));
     uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
     uint32_t* eoff = c->get<uint32_t>("eoff", n);
     {
@@ -590,8 +459,14 @@ int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
                     "n_dim * max_candidates exceeds the join's shared-memory tile "
                     "(2 * max_candidates * n_dim * 4 bytes must stay under 200 KiB, "
                     "max_candidates <= 200)");
-    if (o->mode != PQ_MODE_PLAIN || o->init != PQ_INIT_RP)
-        return fail(c, PQ_ENOTSUP, "only the plain form with RP init is available on this entry");
+    if (o->mode != PQ_MODE_PLAIN && o->mode != PQ_MODE_BF16)
+        return fail(c, PQ_ENOTSUP, "mode not available in this build");
+    if (o->init != PQ_INIT_RP)
+        return fail(c, PQ_ENOTSUP, "init not available in this build");
+    if (o->mode != PQ_MODE_PLAIN && d > 62)
+        return fail(c, PQ_ENOTSUP, "the tensor-core form supports n_dim <= 62");
+    if (o->mode != PQ_MODE_PLAIN && R.k > 31)
+        return fail(c, PQ_ENOTSUP, "the tensor-core form supports k <= 31");
     return PQ_OK;
 }
 
@@ -621,6 +496,8 @@ void pq_nnd_opts_default(pq_nnd_opts* o) {
     o->delta = 0.001;
     o->mode = PQ_MODE_PLAIN;
     o->init = PQ_INIT_RP;
+    o->probes = 0;
+    o->refine_rounds = -1;
 }
 
 uint64_t pq_effective_k(uint64_t n_obs, uint64_t k) { return effective_k(n_obs, k); }
@@ -699,7 +576,9 @@ int pq_nndescent_into(pq_ctx* c, const float* data, uint64_t n, uint64_t d,
         uint32_t* dip = c->get<uint32_t>("out_indptr", n + 1);
         uint32_t* dix = c->get<uint32_t>("out_indices", cap);
         float* ddx = c->get<float>("out_dists", cap);
-        uint64_t nnz = build_plain(c, data, true, n, d, *o, dip, dix, ddx, nullptr);
+        uint64_t nnz = o->mode == PQ_MODE_PLAIN
+                           ? build_plain(c, data, true, n, d, *o, dip, dix, ddx, nullptr)
+                           : build_chosen(c, data, true, n, d, *o, dip, dix, ddx);
         ck(cudaMemcpyAsync(indptr, dip, (n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
         ck(cudaMemcpyAsync(indices, dix, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
         ck(cudaMemcpyAsync(dists, ddx, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
@@ -722,8 +601,10 @@ int pq_nndescent_into_device(pq_ctx* c, const float* d_data, uint64_t n, uint64_
         ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
         ck(cudaEventRecord(ev, user), "event");
         ck(cudaStreamWaitEvent(c->stream, ev, 0), "event");
-        uint64_t nnz = build_plain(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists,
-                                   nullptr);
+        uint64_t nnz =
+            o->mode == PQ_MODE_PLAIN
+                ? build_plain(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists, nullptr)
+                : build_chosen(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists);
         ck(cudaEventRecord(ev, c->stream), "event");
         ck(cudaStreamWaitEvent(user, ev, 0), "event");
         cudaEventDestroy(ev);

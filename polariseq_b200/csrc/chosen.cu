@@ -1,0 +1,715 @@
+// Chosen form: a tensor-core shortlist over buckets, exact FP32 re-rank and an
+// FP64 boundary step.
+//
+//   1. buckets: Lloyd k-means on an evenly strided sample of the cells (FP32),
+//      then every cell's P nearest centroids by the tensor-core tile kernel
+//      (one bucket holding all centroids); the nearest is its primary bucket;
+//   2. layout: cells sorted by primary bucket (stable radix sort); each cell's
+//      BF16 row centred on its bucket's centroid; query entries (cell, probe)
+//      grouped by probe bucket, centred on the probe's centroid;
+//   3. the tile kernel (ivf.cu) keeps each entry's S nearest by approximate
+//      |q~|^2 + |x~|^2 - 2 q~.x~;
+//   4. re-rank: per cell, the R best of its P*S shortlist by approximate
+//      distance get their exact FP32 squared distance in the reference's
+//      summation order (simd.rs:43-62), sorted by (distance, index); where the
+//      k-th and (k+1)-th differ by less than the FP32 error bound, the band is
+//      re-ordered by FP64 distances;
+//   5. optional NN-Descent rounds (the plain form's round kernels) polish the
+//      lists; the extract writes the CSR graph.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <cstdio>
+
+#include "ctx.cuh"
+#include "ivf.cuh"
+#include "kernels.cuh"
+#include "primitives.cuh"
+
+namespace pq {
+namespace {
+
+constexpr float FP32_BOUND = 1e-5f;  // relative band of the FP64 boundary step
+
+// Evenly strided sample of the padded rows.
+__global__ void k_sample_rows(const float* __restrict__ X, int dp, uint32_t n, uint32_t ns,
+                              float* __restrict__ out) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(ns) * dp) return;
+    const uint32_t j = uint32_t(t / dp), c = uint32_t(t - size_t(j) * dp);
+    const uint64_t i = uint64_t(j) * n / ns;
+    out[t] = X[i * dp + c];
+}
+
+// Column sums of the padded rows (for the global mean used as BF16 centre).
+__global__ void k_col_sum(const float* __restrict__ X, uint32_t n, int dp, float* sums) {
+    const int j = threadIdx.x;
+    if (j >= dp) return;
+    float s = 0.f;
+    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) s += X[size_t(i) * dp + j];
+    atomicAdd(&sums[j], s);
+}
+__global__ void k_scale(float* v, int m, float f) {
+    if (int(threadIdx.x) < m) v[threadIdx.x] *= f;
+}
+
+// Lloyd update sums from the tensor-core nearest-centroid labels.
+__global__ void k_kmeans_accumulate(const float* __restrict__ xs, uint32_t ns, int d, int dp,
+                                    const uint32_t* __restrict__ lab, float* __restrict__ sums,
+                                    uint32_t* __restrict__ cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    const uint32_t b = lab[i];
+    if (b == 0xFFFFFFFFu) return;
+    atomicAdd(&cnt[b], 1u);
+    for (int j = 0; j < d; ++j) atomicAdd(&sums[size_t(b) * dp + j], xs[size_t(i) * dp + j]);
+}
+
+// Query-entry keys and values (cell * P + rank) from the probes: primary
+// entries (rank 0) sort first by bucket (key = bucket), the others after them
+// (key = C + bucket), so the primary probes can run as a first pass.
+__global__ void k_entry_keys(const uint32_t* __restrict__ probes, size_t ne, int P, uint32_t C,
+                             uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
+    const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    keys[e] = probes[e] + (e % P != 0 ? C : 0u);
+    vals[e] = e;
+}
+
+// Seed thresholds of the non-primary entries: the R-th best approximate
+// distance of the cell's primary shortlist (a candidate of another bucket can
+// only enter the cell's R best if it beats that).
+__global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_t n, int P,
+                                  const float* __restrict__ sd, int S, int R,
+                                  float* __restrict__ qthr) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t e0 = entry_of[size_t(i) * P];
+    // the R-th smallest of the entry's two ascending runs of S
+    const float* r0 = sd + size_t(e0) * 2 * S;
+    const float* r1 = r0 + S;
+    int x = 0, y = 0;
+    float t = __int_as_float(0x7f800000);
+    for (int o = 0; o < R && (x < S || y < S); ++o) {
+        const float vx = x < S ? r0[x] : __int_as_float(0x7f800000);
+        const float vy = y < S ? r1[y] : __int_as_float(0x7f800000);
+        if (vx <= vy) {
+            t = vx;
+            ++x;
+        } else {
+            t = vy;
+            ++y;
+        }
+    }
+    qthr[e0] = __int_as_float(0x7f800000);
+    for (int r = 1; r < P; ++r) qthr[entry_of[size_t(i) * P + r]] = t;
+}
+
+__global__ void k_kmeans_update(float* __restrict__ cent, const float* __restrict__ sums,
+                                const uint32_t* __restrict__ cnt, uint32_t C, int d, int dp) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(C) * dp) return;
+    const uint32_t c = uint32_t(t / dp), j = uint32_t(t - size_t(c) * dp);
+    if (j < uint32_t(d) && cnt[c] > 0) cent[t] = sums[t] / float(cnt[c]);
+}
+
+// BF16 rows (64 dims, zero padded) of (row(src_i) - center(c_i)), and their
+// squared norms computed in FP32 from the rounded values.  Columns d and d+1
+// carry the augmentation of the tensor-core tiles: -1/2, -1/2 for a query row
+// (aug 1), and hi, lo with hi + lo = the row's norm for a candidate row (aug 2).
+__global__ void k_to_bf16(const float* __restrict__ X, int d, int dp,
+                          const uint32_t* __restrict__ src, const uint32_t* __restrict__ cid,
+                          const float* __restrict__ cent, size_t rows, int aug,
+                          __nv_bfloat16* __restrict__ out, float* __restrict__ norm) {
+    const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    const uint32_t i = src ? src[r] : uint32_t(r);
+    const uint32_t c = cid ? cid[r] : 0u;
+    float s = 0.f;
+    __nv_bfloat16 bv[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int j = lane + 32 * h;
+        float v = 0.f;
+        if (j < d) v = X[size_t(i) * dp + j] - (cent ? cent[size_t(c) * dp + j] : 0.f);
+        bv[h] = __float2bfloat16_rn(v);
+        const float f = __bfloat162float(bv[h]);
+        s = fmaf(f, f, s);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    const __nv_bfloat16 hi = __float2bfloat16_rn(s);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(s - __bfloat162float(hi));
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int j = lane + 32 * h;
+        __nv_bfloat16 o = bv[h];
+        if (aug == 1 && (j == d || j == d + 1)) o = __float2bfloat16_rn(-0.5f);
+        if (aug == 2 && j == d) o = hi;
+        if (aug == 2 && j == d + 1) o = lo;
+        out[r * 64 + j] = o;
+    }
+    if (lane == 0) norm[r] = s;
+}
+
+// The s_out nearest of two ascending runs of S per row (distinct ids).
+__global__ void k_merge_runs(const float* __restrict__ rd, const uint32_t* __restrict__ ri,
+                             uint32_t rows, int S, int s_out, float* __restrict__ od,
+                             uint32_t* __restrict__ oi) {
+    const uint32_t r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= rows) return;
+    const size_t base = size_t(r) * 2 * S;
+    int x = 0, y = 0;
+    for (int o = 0; o < s_out; ++o) {
+        const float vx = x < S ? rd[base + x] : __int_as_float(0x7f800000);
+        const float vy = y < S ? rd[base + S + y] : __int_as_float(0x7f800000);
+        const uint32_t ix = x < S ? ri[base + x] : 0xFFFFFFFFu;
+        const uint32_t iy = y < S ? ri[base + S + y] : 0xFFFFFFFFu;
+        const bool takex = vx < vy || (vx == vy && ix <= iy);
+        od[size_t(r) * s_out + o] = takex ? vx : vy;
+        oi[size_t(r) * s_out + o] = takex ? ix : iy;
+        if (takex) ++x;
+        else ++y;
+    }
+}
+
+__global__ void k_primary_keys(const uint32_t* __restrict__ probes, int P, uint32_t n,
+                               uint32_t* __restrict__ keys, uint64_t* __restrict__ vals,
+                               uint32_t* __restrict__ hist) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const uint32_t b = probes[size_t(i) * P];
+    keys[i] = b;
+    vals[i] = i;
+    atomicAdd(&hist[b], 1u);
+}
+
+__global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n,
+                              const uint32_t* __restrict__ keys, uint32_t* __restrict__ perm,
+                              uint32_t* __restrict__ pos_of, uint32_t* __restrict__ cbucket) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    const uint32_t i = uint32_t(vals[p]);
+    perm[p] = i;
+    pos_of[i] = p;
+    cbucket[p] = keys[p];
+}
+
+__global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t* __restrict__ keys,
+                               size_t ne, int P, uint32_t C, const uint32_t* __restrict__ probes,
+                               const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpoint,
+                               uint32_t* __restrict__ qbucket, uint32_t* __restrict__ qself,
+                               uint32_t* __restrict__ entry_of, uint32_t* __restrict__ qhist) {
+    const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= ne) return;
+    const uint64_t v = vals[e];
+    const uint32_t i = uint32_t(v / P), r = uint32_t(v % P);
+    const uint32_t key = keys[e];
+    const uint32_t b = key >= C ? key - C : key;
+    qpoint[e] = i;
+    qbucket[e] = b;
+    qself[e] = b == probes[size_t(i) * P] ? pos_of[i] : 0xFFFFFFFFu;
+    entry_of[v] = uint32_t(e);
+    atomicAdd(&qhist[key], 1u);
+    (void)r;
+}
+
+// Bitonic sort (ascending) of 64 keys held two per lane (element e of lane l
+// is index l + 32 e).
+__device__ __forceinline__ void warp_sort64(uint64_t (&v)[2]) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 64; size <<= 1) {
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+#pragma unroll
+            for (int e = 0; e < 2; ++e) {
+                const int idx = lane + 32 * e;
+                const bool up = (idx & size) == 0;
+                if (stride >= 32) {
+                    if (e == 0) {  // partner is the other element of this lane
+                        const bool swap = up ? v[0] > v[1] : v[0] < v[1];
+                        if (swap) {
+                            const uint64_t t = v[0];
+                            v[0] = v[1];
+                            v[1] = t;
+                        }
+                    }
+                } else {
+                    const uint64_t other = __shfl_xor_sync(0xFFFFFFFFu, v[e], stride);
+                    const bool lower = (idx & stride) == 0;
+                    const uint64_t lo = v[e] < other ? v[e] : other;
+                    const uint64_t hi = v[e] < other ? other : v[e];
+                    v[e] = (lower == up) ? lo : hi;
+                }
+            }
+        }
+    }
+}
+
+// Exact FP64 squared distance of two padded rows.
+__device__ __forceinline__ double sq_dist_f64(const float* a, const float* b, int d) {
+    double s = 0.0;
+    for (int j = 0; j < d; ++j) {
+        const double t = double(a[j]) - double(b[j]);
+        s += t * t;
+    }
+    return s;
+}
+
+// Re-rank, one warp per cell (cells visited in bucket order): merge the
+// ascending shortlist runs of the P probes (SO / RS runs of RS per probe) to
+// the R best approximate candidates, give
+// them exact FP32 squared distances in the reference's summation order, sort
+// by (distance, index), and where the k-th and (k+1)-th differ by less than
+// the FP32 error bound re-order that band by FP64 distance.  Writes the k
+// nearest (ascending) per cell.
+template <int D>
+__global__ void __launch_bounds__(128) k_rerank(
+    const float* __restrict__ X, int d, int dp, uint32_t n, int k, int P, int SO, int RS, int R,
+    const uint32_t* __restrict__ entry_of, const float* __restrict__ sd,
+    const uint32_t* __restrict__ si, const uint32_t* __restrict__ perm,
+    uint32_t* __restrict__ out_idx, float* __restrict__ out_dist,
+    unsigned long long* boundary_fixes) {
+    __shared__ uint32_t band_i[4][64];
+    __shared__ double band_d[4][64];
+    __shared__ float band_f[4][64];
+    const uint32_t wg = blockIdx.x * 4 + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    if (wg >= n) return;
+    const uint32_t i = perm[wg];
+    // 1. merge of the ascending runs (lane L < P * NR owns run L % NR of probe
+    //    L / NR; runs are RS long, an entry's NR runs RS * NR apart)
+    const int NR = SO / RS;
+    size_t base = 0;
+    uint32_t head = 0;
+    if (lane < P * NR)
+        base = size_t(entry_of[size_t(i) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
+    uint32_t cand[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
+    for (int t = 0; t < R; ++t) {
+        float v = __int_as_float(0x7f800000);
+        uint32_t id = 0xFFFFFFFFu;
+        if (lane < P * NR && head < uint32_t(RS)) {
+            v = sd[base + head];
+            id = si[base + head];
+        }
+        // warp argmin by (value, candidate)
+        float bv = v;
+        uint32_t bid = id;
+        int bl = lane;
+        for (int o = 16; o > 0; o >>= 1) {
+            const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
+            const uint32_t oid = __shfl_xor_sync(0xFFFFFFFFu, bid, o);
+            const int ol = __shfl_xor_sync(0xFFFFFFFFu, bl, o);
+            if (ov < bv || (ov == bv && oid < bid)) {
+                bv = ov;
+                bid = oid;
+                bl = ol;
+            }
+        }
+        if (bid == 0xFFFFFFFFu) break;  // every list exhausted
+        if (lane == bl) ++head;
+        if ((t & 31) == lane) cand[t >> 5] = bid;
+    }
+    // 2. exact FP32 distances (reference order) of this lane's candidates
+    const float* xi = X + size_t(i) * dp;
+    uint64_t key[2];
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        key[h] = ~0ull;
+        if (cand[h] != 0xFFFFFFFFu) {
+            const uint32_t j = perm[cand[h]];
+            const float dd = sq_dist_exact_t<D>(xi, X + size_t(j) * dp, d);
+            key[h] = (uint64_t(__float_as_uint(dd)) << 32) | j;
+        }
+    }
+    // 3. sort by (distance, index): non-negative floats order as their bits
+    warp_sort64(key);
+    // 4. FP64 band at the k-th boundary
+    const uint64_t kk1 = __shfl_sync(0xFFFFFFFFu, (k - 1) >= 32 ? key[1] : key[0], (k - 1) & 31);
+    const uint64_t kk =
+        k < 64 ? __shfl_sync(0xFFFFFFFFu, k >= 32 ? key[1] : key[0], k & 31) : ~0ull;
+    const float fk1 = __uint_as_float(uint32_t(kk1 >> 32));
+    const float fk = __uint_as_float(uint32_t(kk >> 32));
+    if (kk != ~0ull && fk - fk1 <= FP32_BOUND * fk) {
+        const float lo = fk1 * (1.0f - FP32_BOUND), hi = fk * (1.0f + FP32_BOUND);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            band_i[w][lane + 32 * h] = uint32_t(key[h]);
+            band_f[w][lane + 32 * h] = __uint_as_float(uint32_t(key[h] >> 32));
+        }
+        __syncwarp();
+        if (lane == 0) {
+            int b0 = k - 1, b1 = k;
+            while (b0 > 0 && band_f[w][b0 - 1] >= lo) --b0;
+            while (b1 + 1 < 64 && band_i[w][b1 + 1] != 0xFFFFFFFFu && band_f[w][b1 + 1] <= hi) ++b1;
+            for (int t = b0; t <= b1; ++t)
+                band_d[w][t] = sq_dist_f64(xi, X + size_t(band_i[w][t]) * dp, d);
+            for (int a = b0 + 1; a <= b1; ++a) {
+                const double x = band_d[w][a];
+                const float xf = band_f[w][a];
+                const uint32_t y = band_i[w][a];
+                int b = a - 1;
+                while (b >= b0 && (band_d[w][b] > x || (band_d[w][b] == x && band_i[w][b] > y))) {
+                    band_d[w][b + 1] = band_d[w][b];
+                    band_f[w][b + 1] = band_f[w][b];
+                    band_i[w][b + 1] = band_i[w][b];
+                    --b;
+                }
+                band_d[w][b + 1] = x;
+                band_f[w][b + 1] = xf;
+                band_i[w][b + 1] = y;
+            }
+            atomicAdd(boundary_fixes, 1ull);
+        }
+        __syncwarp();
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            key[h] = (uint64_t(__float_as_uint(band_f[w][lane + 32 * h])) << 32) |
+                     band_i[w][lane + 32 * h];
+    }
+    // 5. the k nearest, ascending
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int t = lane + 32 * h;
+        if (t < k) {
+            const bool ok = key[h] != ~0ull;
+            out_idx[size_t(i) * k + t] = ok ? uint32_t(key[h]) : PQ_EMPTY;
+            out_dist[size_t(i) * k + t] =
+                ok ? __uint_as_float(uint32_t(key[h] >> 32)) : __int_as_float(0x7f800000);
+        }
+    }
+}
+
+// Sorted (ascending) lists -> neighbour heaps: a descending array is a valid
+// max-heap; every entry starts new.
+__global__ void k_list_to_heap(const uint32_t* __restrict__ li, const float* __restrict__ ld,
+                               uint32_t n, int k, uint32_t* __restrict__ hidx,
+                               float* __restrict__ hdist, uint8_t* __restrict__ hflag) {
+    const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= size_t(n) * k) return;
+    const size_t i = e / k;
+    const int s = int(e - i * k);
+    const size_t src = i * k + (k - 1 - s);
+    hidx[e] = li[src];
+    hdist[e] = ld[src];
+    hflag[e] = li[src] != PQ_EMPTY ? 1 : 0;
+}
+
+}  // namespace
+}  // namespace pq
+
+namespace pqh {
+
+using namespace pq;
+
+uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64, uint64_t d64,
+                      const pq_nnd_opts& o, uint32_t* d_indptr, uint32_t* d_indices,
+                      float* d_dists) {
+    cudaStream_t st = c->stream;
+    const uint32_t n = uint32_t(n64);
+    const int d = int(d64), dp = int((d64 + 3) / 4 * 4);
+    const int k = int(effective_k(n64, o.k));
+    pq_nnd_stats& S_ = c->stats;
+    std::memset(&S_, 0, sizeof(S_));
+    S_.k = k;
+    Timer tot(st), tm(st);
+    tot.start();
+    const unsigned long long launches0 = g_launches;
+
+    float* X = c->get<float>("X", size_t(n) * dp);
+    if (dp != d) ck(cudaMemsetAsync(X, 0, size_t(n) * dp * sizeof(float), st), "memset X");
+    ck(cudaMemcpy2DAsync(X, size_t(dp) * sizeof(float), data, size_t(d) * sizeof(float),
+                         size_t(d) * sizeof(float), n,
+                         data_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st),
+       "copy embedding");
+
+    // ── 1. buckets ──
+    tm.start();
+    const uint32_t C = std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
+    const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : 12u, std::min(C, 16u)));
+    const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
+    if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};
+    int num_sms = 148;
+    cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, c->device);
+    float* xs = c->get<float>("km_sample", size_t(ns) * dp);
+    float* cent = c->get<float>("km_cent", size_t(C) * dp);
+    float* sums = c->get<float>("km_sums", size_t(C) * dp);
+    uint32_t* cnt = c->get<uint32_t>("km_cnt", C);
+    uint32_t* zeros = c->get<uint32_t>("zeros", std::max<uint32_t>(C, n));
+    ck(cudaMemsetAsync(zeros, 0, size_t(std::max<uint32_t>(C, n)) * 4, st), "zeros");
+    uint32_t* noself = c->get<uint32_t>("noself", n);
+    ck(cudaMemsetAsync(noself, 0xFF, size_t(n) * 4, st), "noself");
+    // global mean: the BF16 centre of the centroid search
+    float* mean = c->get<float>("mean", dp);
+    ck(cudaMemsetAsync(mean, 0, dp * 4, st), "mean");
+    k_col_sum<<<512, 64 * ((dp + 63) / 64), 0, st>>>(X, n, dp, mean); count_launch();
+    k_scale<<<1, 128, 0, st>>>(mean, dp, 1.0f / float(n)); count_launch();
+    k_sample_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, n, ns, xs); count_launch();
+    k_sample_rows<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(xs, dp, ns, C, cent); count_launch();
+    __nv_bfloat16* xsb = c->get<__nv_bfloat16>("km_sample_bf16", size_t(ns) * 64);
+    float* xsn = c->get<float>("km_sample_norm", ns);
+    k_to_bf16<<<blocks(ns, 8), 256, 0, st>>>(xs, d, dp, nullptr, zeros, mean, ns, 1, xsb, xsn); count_launch();
+    __nv_bfloat16* cb = c->get<__nv_bfloat16>("cent_bf16", size_t(C) * 64);
+    float* cbn = c->get<float>("cent_norm", C);
+    float* lab_d = c->get<float>("km_lab_d", ns);
+    uint32_t* lab = c->get<uint32_t>("km_lab", ns);
+    // one-bucket nearest-centroid search on the tensor cores: queries [0, nq)
+    // against all C centroids, S_out nearest per query
+    auto centroid_search = [&](const __nv_bfloat16* qrows, const float* qnorm, uint32_t nq,
+                               int s_out, float* od, uint32_t* oi) {
+        const uint32_t nj = (nq + 127) / 128;
+        std::vector<uint32_t> hb(nj, 0), hq(nj), he(nj);
+        for (uint32_t j = 0; j < nj; ++j) {
+            hq[j] = j * 128;
+            he[j] = std::min(nq, j * 128 + 128);
+        }
+        uint32_t* jb = c->get<uint32_t>("ajob_b", nj);
+        uint32_t* jq = c->get<uint32_t>("ajob_q", nj);
+        uint32_t* je = c->get<uint32_t>("ajob_e", nj);
+        uint32_t* offs = c->get<uint32_t>("aoffs", 4);
+        uint32_t ho[4] = {0, C, 0, 0};
+        ck(cudaMemcpyAsync(jb, hb.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+        ck(cudaMemcpyAsync(jq, hq.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+        ck(cudaMemcpyAsync(je, he.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+        ck(cudaMemcpyAsync(offs, ho, 16, cudaMemcpyHostToDevice, st), "jobs");
+        CUtensorMap tq, tcm;
+        if (!make_bf16_map(&tq, qrows, nq, 128) || !make_bf16_map(&tcm, cb, C, 256))
+            throw DeviceError{"cuTensorMapEncodeTiled failed"};
+        IvfTileArgs a{};
+        a.job_bucket = jb;
+        a.job_qstart = jq;
+        a.job_qend = je;
+        a.njobs = nj;
+        a.c_off = offs;
+        a.qnorm = qnorm;
+        a.qself = noself;
+        a.S = 16;
+        a.out_d = c->get<float>("arun_d", size_t(nq) * 2 * 16);
+        a.out_i = c->get<uint32_t>("arun_i", size_t(nq) * 2 * 16);
+        a.err = c->d_err;
+        ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "centroid tiles");
+        k_merge_runs<<<blocks(nq, 256), 256, 0, st>>>(a.out_d, a.out_i, nq, 16, s_out, od, oi); count_launch();
+        ck(cudaStreamSynchronize(st), "centroid tiles");  // the host job arrays are reused
+    };
+    ck(cudaMemsetAsync(c->d_err, 0, 4, st), "err");
+    const int lloyd = 8;
+    for (int it = 0; it < lloyd; ++it) {
+        k_to_bf16<<<blocks(C, 8), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
+        centroid_search(xsb, xsn, ns, 1, lab_d, lab);
+        ck(cudaMemsetAsync(sums, 0, size_t(C) * dp * 4, st), "km");
+        ck(cudaMemsetAsync(cnt, 0, size_t(C) * 4, st), "km");
+        k_kmeans_accumulate<<<blocks(ns, 256), 256, 0, st>>>(xs, ns, d, dp, lab, sums, cnt); count_launch();
+        k_kmeans_update<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(cent, sums, cnt, C, d, dp); count_launch();
+    }
+    k_to_bf16<<<blocks(C, 8), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
+    // every cell's P nearest centroids, ascending; the first is its primary bucket
+    __nv_bfloat16* qa = c->get<__nv_bfloat16>("assign_q", size_t(n) * 64);
+    float* qan = c->get<float>("assign_qn", n);
+    k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan); count_launch();
+    uint32_t* probes = c->get<uint32_t>("probes", size_t(n) * P);
+    float* probe_d = c->get<float>("probe_d", size_t(n) * P);
+    centroid_search(qa, qan, n, P, probe_d, probes);
+    int herr0 = 0;
+    ck(cudaMemcpy(&herr0, c->d_err, 4, cudaMemcpyDeviceToHost), "err");
+    if (herr0) throw DeviceError{"centroid tiles: a bounded wait gave up"};
+    const size_t ne = size_t(n) * P;
+    uint32_t* ekeys = c->get<uint32_t>("ekeys", ne);
+    uint64_t* evals = c->get<uint64_t>("evals", ne);
+    uint32_t* ekeys2 = c->get<uint32_t>("ekeys2", ne);
+    uint64_t* evals2 = c->get<uint64_t>("evals2", ne);
+    k_entry_keys<<<blocks(ne, 256), 256, 0, st>>>(probes, ne, P, C, ekeys, evals); count_launch();
+    S_.ms_forest = tm.stop();
+
+    // ── 2. layout ──
+    tm.start();
+    void* stemp = c->get<uint8_t>("scan_temp_c", scan_temp_bytes(std::max<size_t>(ne, C + 1)));
+    uint32_t* ckeys = c->get<uint32_t>("ckeys_c", n);
+    uint64_t* cvals = c->get<uint64_t>("cvals_c", n);
+    uint32_t* ckeys2 = c->get<uint32_t>("ckeys_c2", n);
+    uint64_t* cvals2 = c->get<uint64_t>("cvals_c2", n);
+    uint32_t* chist = c->get<uint32_t>("chist", C + 1);
+    ck(cudaMemsetAsync(chist, 0, size_t(C + 1) * 4, st), "hist");
+    k_primary_keys<<<blocks(n, 256), 256, 0, st>>>(probes, P, n, ckeys, cvals, chist); count_launch();
+    ck(radix_sort_pairs(ckeys, cvals, ckeys2, cvals2, n, key_bits(C),
+                        c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
+       "sort cand");
+    uint32_t* c_off = c->get<uint32_t>("c_off", C + 1);
+    ck(scan_exclusive_u32(chist, c_off, C + 1, stemp, nullptr, st), "scan c");
+    uint32_t* perm = c->get<uint32_t>("cperm", n);
+    uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
+    uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
+    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, ckeys, perm, pos_of, cbucket); count_launch();
+    __nv_bfloat16* xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
+    float* xcn = c->get<float>("xc_norm", n);
+    k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, 2, xc, xcn); count_launch();
+    // query entries grouped by probe bucket (stable: cell order within a bucket)
+    ck(radix_sort_pairs(ekeys, evals, ekeys2, evals2, ne, key_bits(2 * C),
+                        c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
+       "sort entries");
+    uint32_t* qpoint = c->get<uint32_t>("qpoint", ne);
+    uint32_t* qbucket = c->get<uint32_t>("qbucket", ne);
+    uint32_t* qself = c->get<uint32_t>("qself", ne);
+    uint32_t* entry_of = c->get<uint32_t>("entry_of", ne);
+    uint32_t* qhist = c->get<uint32_t>("qhist", 2 * C + 1);
+    ck(cudaMemsetAsync(qhist, 0, size_t(2 * C + 1) * 4, st), "hist");
+    k_entry_layout<<<blocks(ne, 256), 256, 0, st>>>(evals, ekeys, ne, P, C, probes, pos_of,
+                                                     qpoint, qbucket, qself, entry_of, qhist); count_launch();
+    uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
+    ck(scan_exclusive_u32(qhist, q_off, 2 * C + 1, stemp, nullptr, st), "scan q");
+    __nv_bfloat16* qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
+    float* qbn = c->get<float>("q_norm", ne);
+    k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, 1, qb, qbn); count_launch();
+    std::vector<uint32_t> hq(2 * C + 1);
+    ck(cudaMemcpyAsync(hq.data(), q_off, size_t(2 * C + 1) * 4, cudaMemcpyDeviceToHost, st),
+       "q_off");
+    ck(cudaStreamSynchronize(st), "layout");
+    std::vector<uint32_t> hc(C + 1);
+    ck(cudaMemcpy(hc.data(), c_off, size_t(C + 1) * 4, cudaMemcpyDeviceToHost), "c_off");
+    // jobs: pass 0 = primary entries (keys [0, C)), pass 1 = the others
+    std::vector<uint32_t> jb[2], jq[2], je[2];
+    uint64_t tile_pairs = 0, maxb = 0;
+    for (int pass = 0; pass < 2; ++pass)
+        for (uint32_t b = 0; b < C; ++b) {
+            const uint32_t key = b + (pass ? C : 0);
+            const uint64_t nct = (hc[b + 1] - hc[b] + 255) / 256;
+            maxb = std::max<uint64_t>(maxb, hc[b + 1] - hc[b]);
+            for (uint32_t q0 = hq[key]; q0 < hq[key + 1]; q0 += 128) {
+                jb[pass].push_back(b);
+                jq[pass].push_back(q0);
+                je[pass].push_back(std::min(q0 + 128, hq[key + 1]));
+                tile_pairs += nct;
+            }
+        }
+    S_.pairs[0] = tile_pairs;  // 128 x 256 tensor-core tiles
+    S_.pairs[1] = maxb;        // largest bucket
+    S_.pairs[2] = C;
+    if (std::getenv("POLARISEQ_TRACE"))
+        std::fprintf(stderr, "[chosen] %u buckets, largest %llu, %zu + %zu query tiles, %llu tile pairs\n",
+                     C, (unsigned long long)maxb, jb[0].size(), jb[1].size(),
+                     (unsigned long long)tile_pairs);
+    S_.ms_leaves = tm.stop();
+
+    // ── 3. tensor-core shortlist ──
+    tm.start();
+    const int Ssh = ivf_shortlist(k + 1);        // per entry and column half
+    const int Sout = ivf_groups() * Ssh;         // per entry: ivf_groups() ascending runs
+    if (Ssh == 0) throw DeviceError{"the tensor-core form supports k <= 31"};
+    float* sd = c->get<float>("sl_d", ne * Sout);
+    uint32_t* si = c->get<uint32_t>("sl_i", ne * Sout);
+    {
+        CUtensorMap tq, tcm;
+        if (!make_bf16_map(&tq, qb, ne, 128) || !make_bf16_map(&tcm, xc, n, 256))
+            throw DeviceError{"cuTensorMapEncodeTiled failed"};
+        float* qthr = c->get<float>("q_thr", ne);
+        const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
+        unsigned long long* tbuf = nullptr;
+        if (trace) {
+            tbuf = c->get<unsigned long long>("ivf_trace", IVF_TRACE_N);
+            ck(cudaMemsetAsync(tbuf, 0, IVF_TRACE_N * 8, st), "trace");
+        }
+        const int R0 = std::min(Sout, std::min(64, std::max(2 * k, k + 1)));
+        for (int pass = 0; pass < 2; ++pass) {
+            const uint32_t nj = uint32_t(jb[pass].size());
+            if (nj == 0) continue;
+            uint32_t* djb = c->get<uint32_t>(pass ? "job_b1" : "job_b0", nj);
+            uint32_t* djq = c->get<uint32_t>(pass ? "job_q1" : "job_q0", nj);
+            uint32_t* dje = c->get<uint32_t>(pass ? "job_e1" : "job_e0", nj);
+            ck(cudaMemcpyAsync(djb, jb[pass].data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+            ck(cudaMemcpyAsync(djq, jq[pass].data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+            ck(cudaMemcpyAsync(dje, je[pass].data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+            IvfTileArgs a{};
+            a.job_bucket = djb;
+            a.job_qstart = djq;
+            a.job_qend = dje;
+            a.njobs = nj;
+            a.c_off = c_off;
+            a.qnorm = qbn;
+            a.qthr = pass ? qthr : nullptr;
+            a.qself = qself;
+            a.S = Ssh;
+            a.out_d = sd;
+            a.out_i = si;
+            a.err = c->d_err;
+            a.trace = tbuf;
+            {
+                KGScope kg(c, PQ_KG_JOIN_COUNT);
+                ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "ivf tiles");
+            }
+            if (pass == 0) {  // seed the other probes with the primary shortlist's R-th best
+                k_seed_thresholds<<<blocks(n, 256), 256, 0, st>>>(entry_of, n, P, sd, Ssh, R0, qthr);
+                count_launch();
+            }
+            ck(cudaStreamSynchronize(st), "jobs");  // the host job arrays are reused
+            if (trace) {
+                unsigned long long h[IVF_TRACE_N];
+                ck(cudaMemcpy(h, tbuf, sizeof(h), cudaMemcpyDeviceToHost), "trace");
+                std::fprintf(stderr,
+                             "[chosen] pass %d tiles block 0: jobs %llu tiles %llu drains %llu | "
+                             "cycles epi-wait %llu epi-work %llu epi-end %llu mma-wait-c %llu "
+                             "mma-wait-t %llu tma-wait %llu total %llu\n",
+                             pass, h[IVF_T_JOBS], h[IVF_T_TILES], h[IVF_T_DRAINS],
+                             h[IVF_T_EPI_WAIT], h[IVF_T_EPI_WORK], h[IVF_T_EPI_END],
+                             h[IVF_T_MMA_WAIT_C], h[IVF_T_MMA_WAIT_T], h[IVF_T_TMA_WAIT],
+                             h[IVF_T_TOTAL]);
+            }
+        }
+    }
+    int herr = 0;
+    ck(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, st), "err");
+    ck(cudaStreamSynchronize(st), "ivf tiles");
+    if (herr) throw DeviceError{"tensor-core tiles: a bounded wait gave up"};
+    S_.ms_rounds = tm.stop();
+
+    // ── 4. re-rank ──
+    tm.start();
+    uint32_t* ridx = c->get<uint32_t>("list_idx", size_t(n) * k);
+    float* rdist = c->get<float>("list_dist", size_t(n) * k);
+    // the exact re-rank list: 2k candidates ("2k-4k shortlist"), at most 64
+    const int R = std::min(P * Sout, std::min(64, std::max(2 * k, k + 1)));
+    if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
+    ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
+    {
+        KGScope kg(c, PQ_KG_REPLAY);
+        if (d == 50)
+            k_rerank<50><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
+                                                       si, perm, ridx, rdist, c->d_acc);
+        else
+            k_rerank<0><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
+                                                      si, perm, ridx, rdist, c->d_acc);
+        count_launch();
+    }
+    unsigned long long fixes = 0;
+    ck(cudaMemcpyAsync(&fixes, c->d_acc, 8, cudaMemcpyDeviceToHost, st), "fixes");
+    // ── 5. NN-Descent rounds from the shortlist lists, then the extract ──
+    uint32_t* hidx = c->get<uint32_t>("hidx", size_t(n) * k);
+    float* hdist = c->get<float>("hdist", size_t(n) * k);
+    uint8_t* hflag = c->get<uint8_t>("hflag", size_t(n) * k);
+    k_list_to_heap<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(ridx, rdist, n, k, hidx, hdist,
+                                                                hflag); count_launch();
+    const Resolved RR = resolve(n64, o);
+    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : 2;
+    int rounds = 0;
+    if (n > 1 && polish > 0)
+        rounds = run_rounds(c, X, d, dp, n, k, int(RR.max_cand), o.seed, polish, RR.stop_at, hidx,
+                            hdist, hflag, perm, 3, nullptr);
+    uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
+    uint32_t* eoff = c->get<uint32_t>("eoff", n);
+    launch_extract_count(hidx, n, k, ecnt, st);
+    ck(scan_exclusive_u32(ecnt, eoff, n, stemp, c->d_u64, st), "scan extract");
+    launch_extract(hidx, hdist, n, k, eoff, d_indptr, d_indices, d_dists, st);
+    uint64_t nnz = 0;
+    ck(cudaMemcpyAsync(&nnz, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "nnz");
+    ck(cudaStreamSynchronize(st), "extract");
+    S_.ms_extract = tm.stop();
+    S_.ms_total = tot.stop();
+    S_.changed[0] = fixes;  // FP64 boundary resolutions of the shortlist re-rank
+    S_.rounds_run = 3 + rounds;  // slots 0..2: shortlist stats; then one per NN-Descent round
+    S_.n_trees = int32_t(C);
+    S_.max_candidates = uint64_t(P) << 32 | uint64_t(Ssh);
+    S_.launches = g_launches - launches0;
+    kg_collect(c);
+    return nnz;
+}
+
+}  // namespace pqh

@@ -704,20 +704,20 @@ __global__ void k_leaf_scatter(const uint8_t* f, const uint32_t* pre, uint32_t n
 // rejected unchanged (nndescent.rs:176), so the heap row in HBM is touched
 // only when a mate beats the root.  Tiles whose span exceeds LCAP or whose
 // leaves exceed LMAX members take the direct path.
-constexpr int LPB = 16;     // leaves per CTA
-constexpr int LCAP = 256;   // staged positions per CTA (= threads)
-constexpr int LMAX = 32;    // largest leaf of the staged path
+constexpr int LPB = 8;      // leaves per CTA
+constexpr int LCAP = 128;   // staged positions per CTA (= threads)
+constexpr int LMAXC = 32;   // largest leaf of the staged path
 
 template <int D>
 __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
     const float* __restrict__ X, int d, int dp, const uint32_t* __restrict__ ids,
     const uint32_t* __restrict__ leaf_start, uint32_t nleaves, uint32_t n, int k, uint32_t* hidx,
-    float* hdist, uint8_t* hflag) {
+    float* hdist, uint8_t* hflag, int LMAX) {
     extern __shared__ __align__(16) float lsm[];
     __shared__ uint32_t sls[LPB + 1];
     __shared__ int staged;
     float* R = lsm;                               // LCAP * dp
-    float* Dt = lsm + size_t(LCAP) * dp;          // LCAP * LMAX
+    float* Dt = lsm + size_t(LCAP) * dp;          // LCAP * LMAX (LMAX: 16 or 32)
     __shared__ uint32_t sid[LCAP];
     __shared__ float sroot[LCAP];
     __shared__ uint16_t sl0[LCAP], sl1[LCAP];     // leaf bounds of each staged position
@@ -872,22 +872,26 @@ void launch_leaf_compact(const uint8_t* leafflag_t, uint32_t n, uint32_t* leaf_s
 }
 void launch_leaf_pairs(const float* X, int d, int dp, const uint32_t* ids_t,
                        const uint32_t* leaf_start, uint32_t nleaves, uint32_t n, int k,
-                       uint32_t* hidx, float* hdist, uint8_t* hflag, cudaStream_t st) {
+                       uint32_t leaf_cap, uint32_t* hidx, float* hdist, uint8_t* hflag,
+                       cudaStream_t st) {
     if (nleaves == 0) return;
-    const size_t sm = (size_t(LCAP) * dp + size_t(LCAP) * LMAX) * sizeof(float);
+    // leaves never exceed leaf_size (or come from depth > 100); a 16-wide mate
+    // table covers the default leaf size 15 and keeps more CTAs resident
+    const int lmax = leaf_cap <= 16 ? 16 : LMAXC;
+    const size_t sm = (size_t(LCAP) * dp + size_t(LCAP) * lmax) * sizeof(float);
     const unsigned grid = (nleaves + LPB - 1) / LPB;
     if (d == 50) {
         if (sm > 40 * 1024)
             cudaFuncSetAttribute(k_leaf_pairs<50>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sm));
         k_leaf_pairs<50><<<grid, LCAP, sm, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
-                                                 hidx, hdist, hflag); count_launch();
+                                                 hidx, hdist, hflag, lmax); count_launch();
     } else {
         if (sm > 40 * 1024)
             cudaFuncSetAttribute(k_leaf_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sm));
         k_leaf_pairs<0><<<grid, LCAP, sm, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
-                                                hidx, hdist, hflag); count_launch();
+                                                hidx, hdist, hflag, lmax); count_launch();
     }
 }
 void launch_random_fill(const float* X, int d, int dp, uint32_t n, int k, uint64_t seed,

@@ -1,0 +1,517 @@
+// Chosen form, stage 1: bucketed distance tiles on tcgen05 tensor cores.
+//
+// The cells are split into buckets (k-means centroids); every cell is a
+// candidate of exactly one bucket (its primary) and probes P buckets as a
+// query.  Within a bucket, coordinates are centred on the bucket's centroid
+// before rounding to BF16 (squared distances are shift invariant, and centring
+// keeps BF16's 8-bit mantissa accurate at the scale of neighbour distances).
+//
+// Rows are augmented so that one product gives the ranking quantity: a query
+// row is [q~, -1/2, -1/2, 0...] and a candidate row [x~, hi, lo, 0...] with
+// hi + lo = |x~|^2 (hi = BF16(|x~|^2), lo = BF16 of the remainder, 2^-17
+// relative), so the accumulator holds a = q~.x~ - |x~|^2 / 2 and the
+// approximate squared distance is |q~|^2 - 2a.  An entry with admission bound
+// thr keeps a candidate only if a > (|q~|^2 - thr) / 2: the hot loop is one
+// three-input max per two accumulators and a warp vote per 32 columns; only
+// the columns some row of the warp admits are visited after that.
+//
+// One CTA per SM runs a persistent job loop (job = 128 query entries of one
+// bucket against all of the bucket's candidates, 256 per tile) with
+// warp-specialised roles and mbarrier hand-offs, no CTA-wide barrier inside
+// the loop:
+//   warp 8 (one lane)  TMA loads: the job's Q tile (2 stages) and candidate
+//                      tiles (2-3 stages, 128-byte swizzled, K-major);
+//   warp 9 (one lane)  tcgen05.mma M=128 N=256 K=16 x4 into one of two TMEM
+//                      accumulator buffers (256 columns each); commits free
+//                      the candidate stage and fill the TMEM buffer;
+//   warps 0-7          epilogue: warp w reads TMEM lanes 32(w%4).. (its query
+//                      rows) for column half w/4 (tcgen05.ld 32x32b) and
+//                      filters; the few flagged chunks are re-read by one
+//                      compact (not unrolled) admission loop, so the rarely
+//                      run code stays small in the instruction cache; then the
+//                      TMEM buffer is freed.  Admitted entries go to a
+//                      per-thread append buffer drained into a shared-memory
+//                      max-heap of S (one heap per row and column half).
+// At job end each thread sorts its heap in registers and writes one ascending
+// run of S: the output row of an entry is NG runs of S.
+//
+// Every wait is bounded: a wait that gives up raises the CTA's abort flag,
+// every role leaves its loop, in-flight copies and MMAs are waited for (again
+// bounded), TMEM is freed and the kernel reports error 2.
+#include <cuda.h>
+
+#include "common.cuh"
+#include "ivf.cuh"
+#include "tc.cuh"
+
+namespace pq {
+namespace {
+
+constexpr int TQ = 128;   // query rows per tile (TMEM lanes)
+constexpr int TCN = 256;  // candidate rows per tile (TMEM columns per buffer)
+constexpr int ROWB = 128; // bytes per BF16 row (64 dims)
+constexpr int NG = 2;     // epilogue warpgroups: each owns half of a tile's columns
+constexpr int NEPI = TQ * NG;   // epilogue threads
+constexpr int NT = NEPI + 64;   // + TMA warp + MMA warp
+constexpr int CPG = TCN / NG;   // columns per warpgroup
+constexpr int BUF = 32;         // append buffer entries per (row, warpgroup)
+constexpr int QST = 2;          // Q tile stages
+constexpr int MAXCS = 3;        // candidate tile stages (at most)
+constexpr uint32_t WAIT_LIMIT = 1u << 24;
+constexpr uint32_t FULL = 0xFFFFFFFFu;
+
+struct __align__(8) IvfBars {
+    uint64_t q_full[QST], q_empty[QST];
+    uint64_t c_full[MAXCS], c_empty[MAXCS];
+    uint64_t t_full[2], t_empty[2];
+    uint64_t done;
+    uint32_t tmem;
+    int abort;
+};
+
+__device__ __forceinline__ float max3f(float a, float b, float c) {
+    float d;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(d) : "f"(a), "f"(b), "f"(c));
+    return d;
+}
+// Maximum of 32 values as a tree of three-input maxes.
+__device__ __forceinline__ float max32(const float (&v)[32]) {
+    float m[11];
+#pragma unroll
+    for (int i = 0; i < 10; ++i) m[i] = max3f(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+    m[10] = fmaxf(v[30], v[31]);
+    const float a = max3f(m[0], m[1], m[2]), b = max3f(m[3], m[4], m[5]),
+                c = max3f(m[6], m[7], m[8]), d = fmaxf(m[9], m[10]);
+    return fmaxf(max3f(a, b, c), d);
+}
+
+// Replace the root of a max-heap of S shortlist entries (one thread's column of
+// a transposed shared-memory tile, entries TQ apart) and sift down; returns
+// the new root (the shortlist's current worst).
+__device__ __forceinline__ float shortlist_insert(float* hd, uint32_t* hi, int S, float d,
+                                                  uint32_t id) {
+    int p = 0;
+    for (;;) {
+        const int l = 2 * p + 1;
+        if (l >= S) break;
+        int c = l;
+        float vc = hd[l * TQ];
+        if (l + 1 < S) {
+            const float vr = hd[(l + 1) * TQ];
+            if (vr > vc) {
+                c = l + 1;
+                vc = vr;
+            }
+        }
+        if (!(vc > d)) break;
+        hd[p * TQ] = vc;
+        hi[p * TQ] = hi[c * TQ];
+        p = c;
+    }
+    hd[p * TQ] = d;
+    hi[p * TQ] = id;
+    return hd[0];
+}
+
+// Ascending bitonic sort of S register pairs by (value, id).
+template <int S>
+__device__ __forceinline__ void sort_pairs(float (&v)[S], uint32_t (&id)[S]) {
+#pragma unroll
+    for (int size = 2; size <= S; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1)
+#pragma unroll
+            for (int i = 0; i < S; ++i) {
+                const int j = i ^ stride;
+                if (j > i) {
+                    const bool up = (i & size) == 0;
+                    const bool gt = v[i] > v[j] || (v[i] == v[j] && id[i] > id[j]);
+                    if (gt == up) {
+                        const float tv = v[i];
+                        v[i] = v[j];
+                        v[j] = tv;
+                        const uint32_t ti = id[i];
+                        id[i] = id[j];
+                        id[j] = ti;
+                    }
+                }
+            }
+}
+
+__host__ __device__ constexpr int cand_stages(int S) { return S <= 16 ? 3 : 2; }
+
+template <int S>
+__global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUtensorMap tmQ,
+                                                     const __grid_constant__ CUtensorMap tmC,
+                                                     IvfTileArgs a) {
+    constexpr int NCS = cand_stages(S);
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    // 1024-align the dynamic region (the swizzle pattern follows address bits)
+    uint8_t* smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint8_t* sQ = smem;                                          // QST x 16 KB
+    uint8_t* sC = sQ + QST * TQ * ROWB;                          // NCS x 32 KB
+    float* hdall = reinterpret_cast<float*>(sC + NCS * TCN * ROWB);         // NG x S x TQ
+    uint32_t* hiall = reinterpret_cast<uint32_t*>(hdall + NG * S * TQ);     // NG x S x TQ
+    float* bdall = reinterpret_cast<float*>(hiall + NG * S * TQ);           // NG x BUF x TQ
+    uint32_t* biall = reinterpret_cast<uint32_t*>(bdall + NG * BUF * TQ);   // NG x BUF x TQ
+    __shared__ IvfBars B;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    volatile int* abort_flag = &B.abort;
+
+    if (w == 0) {
+        tc::tmem_alloc(&B.tmem, 512);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < QST; ++s) {
+            tc::mbar_init(&B.q_full[s], 1);
+            tc::mbar_init(&B.q_empty[s], 1);
+        }
+        for (int s = 0; s < MAXCS; ++s) {
+            tc::mbar_init(&B.c_full[s], 1);
+            tc::mbar_init(&B.c_empty[s], 1);
+        }
+        for (int s = 0; s < 2; ++s) {
+            tc::mbar_init(&B.t_full[s], 1);
+            tc::mbar_init(&B.t_empty[s], NEPI / 32);
+        }
+        tc::mbar_init(&B.done, 1);
+        tc::fence_barrier_init();
+        B.abort = 0;
+    }
+    if (tid == NEPI) {
+        tc::prefetch_tmap(&tmQ);
+        tc::prefetch_tmap(&tmC);
+    }
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t taddr = B.tmem;
+    const bool tracing = a.trace && blockIdx.x == 0;
+    const long long c_start = clock64();
+
+    if (w == NEPI / 32) {
+        // ── TMA producer ──
+        if (lane == 0) {
+            uint32_t qi = 0, ci = 0;
+            long long c_wait = 0;
+            for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
+                const uint32_t b = a.job_bucket[job], qs = a.job_qstart[job];
+                const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
+                const uint32_t nct = (ce - cs + TCN - 1) / TCN;
+                if (nct == 0) continue;
+                const int qsd = int(qi % QST);
+                long long c0 = clock64();
+                if (!tc::mbar_wait(&B.q_empty[qsd], ((qi / QST) & 1) ^ 1, WAIT_LIMIT)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                c_wait += clock64() - c0;
+                tc::mbar_expect_tx(&B.q_full[qsd], TQ * ROWB);
+                tc::tma_load_2d(sQ + qsd * TQ * ROWB, &tmQ, &B.q_full[qsd], 0, int(qs));
+                ++qi;
+                for (uint32_t t = 0; t < nct; ++t) {
+                    const int s = int(ci % NCS);
+                    c0 = clock64();
+                    if (!tc::mbar_wait(&B.c_empty[s], ((ci / NCS) & 1) ^ 1, WAIT_LIMIT)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    c_wait += clock64() - c0;
+                    tc::mbar_expect_tx(&B.c_full[s], TCN * ROWB);
+                    tc::tma_load_2d(sC + s * TCN * ROWB, &tmC, &B.c_full[s], 0, int(cs + t * TCN));
+                    ++ci;
+                }
+            }
+            // every issued copy has landed before the CTA may exit
+            for (int s = 0; s < NCS; ++s) {
+                const uint32_t uses = ci / NCS + (uint32_t(s) < ci % NCS ? 1u : 0u);
+                if (uses > 0 && !tc::mbar_wait(&B.c_full[s], (uses - 1) & 1, WAIT_LIMIT))
+                    *abort_flag = 1;
+            }
+            for (int s = 0; s < QST; ++s) {
+                const uint32_t uses = qi / QST + (uint32_t(s) < qi % QST ? 1u : 0u);
+                if (uses > 0 && !tc::mbar_wait(&B.q_full[s], (uses - 1) & 1, WAIT_LIMIT))
+                    *abort_flag = 1;
+            }
+            if (tracing) a.trace[IVF_T_TMA_WAIT] = (unsigned long long)c_wait;
+        }
+        __syncwarp();
+    } else if (w == NEPI / 32 + 1) {
+        // ── MMA issuer ──
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16_f32(TQ, TCN);
+            uint32_t qi = 0, ci = 0, ti = 0;
+            long long c_wait_c = 0, c_wait_t = 0;
+            for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
+                const uint32_t b = a.job_bucket[job];
+                const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
+                const uint32_t nct = (ce - cs + TCN - 1) / TCN;
+                if (nct == 0) continue;
+                const int qsd = int(qi % QST);
+                if (!tc::mbar_wait(&B.q_full[qsd], (qi / QST) & 1, WAIT_LIMIT)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                const uint64_t dQ = tc::desc_k_sw128(tc::smem_u32(sQ + qsd * TQ * ROWB));
+                bool ok = true;
+                for (uint32_t t = 0; t < nct && ok; ++t) {
+                    const int s = int(ci % NCS), tb = int(ti & 1);
+                    long long c0 = clock64();
+                    ok = tc::mbar_wait(&B.c_full[s], (ci / NCS) & 1, WAIT_LIMIT);
+                    long long c1 = clock64();
+                    ok = ok && tc::mbar_wait(&B.t_empty[tb], ((ti >> 1) & 1) ^ 1, WAIT_LIMIT);
+                    c_wait_c += c1 - c0;
+                    c_wait_t += clock64() - c1;
+                    if (!ok) break;
+                    tc::tc_fence_after();
+                    const uint64_t dC = tc::desc_k_sw128(tc::smem_u32(sC + s * TCN * ROWB));
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)  // K = 64 as four K = 16 steps (32 B each)
+                        tc::umma_f16(taddr + uint32_t(tb * TCN), dQ + uint64_t(2 * kk),
+                                     dC + uint64_t(2 * kk), idesc, kk > 0 ? 1u : 0u);
+                    tc::umma_commit(&B.c_empty[s]);
+                    tc::umma_commit(&B.t_full[tb]);
+                    ++ci;
+                    ++ti;
+                }
+                tc::umma_commit(&B.q_empty[qsd]);
+                ++qi;
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+            }
+            // every issued MMA has completed before TMEM is freed
+            tc::umma_commit(&B.done);
+            if (!tc::mbar_wait(&B.done, 0, WAIT_LIMIT)) *abort_flag = 1;
+            if (tracing) {
+                a.trace[IVF_T_MMA_WAIT_C] = (unsigned long long)c_wait_c;
+                a.trace[IVF_T_MMA_WAIT_T] = (unsigned long long)c_wait_t;
+                a.trace[IVF_T_TILES] = ti;
+            }
+        }
+        __syncwarp();
+    } else {
+        // ── epilogue ──
+        const int g = w >> 2;
+        const int row = (w & 3) * 32 + lane;
+        const uint32_t lane_base = uint32_t((w & 3) * 32) << 16;
+        float* hd = hdall + size_t(g) * S * TQ + row;
+        uint32_t* hi = hiall + size_t(g) * S * TQ + row;
+        float* bd = bdall + size_t(g) * BUF * TQ + row;
+        uint32_t* bi = biall + size_t(g) * BUF * TQ + row;
+        const bool t0 = tracing && tid == 0;
+        long long c_wait = 0, c_work = 0, c_end = 0;
+        unsigned long long drains = 0, jobs = 0;
+        uint32_t ti = 0;
+        for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
+            const uint32_t b = a.job_bucket[job];
+            const uint32_t qs = a.job_qstart[job], qe = a.job_qend[job];
+            const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
+            const uint32_t nct = (ce - cs + TCN - 1) / TCN;
+            const uint32_t entry = qs + row;
+            const bool valid = entry < qe;
+            // an invalid row's infinite |q|^2 makes its bound +inf or NaN: it
+            // admits nothing
+            const float qn = valid ? a.qnorm[entry] : __int_as_float(0x7f800000);
+            const uint32_t qself = valid ? a.qself[entry] : 0xFFFFFFFFu;
+            const float thr0 = (valid && a.qthr) ? a.qthr[entry] : __int_as_float(0x7f800000);
+            float thr = thr0;
+            float ath = (qn - thr) * 0.5f;
+            int cnt = 0;
+#pragma unroll 4
+            for (int j = 0; j < S; ++j) {
+                hd[j * TQ] = __int_as_float(0x7f800000);
+                hi[j * TQ] = 0xFFFFFFFFu;
+            }
+            // drain this lane's append buffer into its heap
+            auto drain = [&]() {
+                for (int t = 0; t < cnt; ++t) {
+                    const float v = bd[t * TQ];
+                    if (v < thr) thr = fminf(thr0, shortlist_insert(hd, hi, S, v, bi[t * TQ]));
+                }
+                cnt = 0;
+                ath = (qn - thr) * 0.5f;
+            };
+            bool ok = true;
+            for (uint32_t t = 0; t < nct; ++t) {
+                const int tb = int(ti & 1);
+                long long c0 = t0 ? clock64() : 0;
+                ok = tc::mbar_wait(&B.t_full[tb], (ti >> 1) & 1, WAIT_LIMIT);
+                ok = __all_sync(FULL, ok);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const uint32_t tcol = taddr + lane_base + uint32_t(tb * TCN + g * CPG);
+                // columns of this slice that belong to the bucket
+                const int lim = int(ce) - int(cs + t * TCN + g * CPG);
+                const uint32_t cbase = cs + t * TCN + g * CPG;
+                // fast filter: the slice's four 32-column chunks from registers,
+                // one max and one vote each; flags the chunks some row admits
+                uint32_t slowq = 0;
+                {
+                    uint32_t r[CPG / 32][32];
+#pragma unroll
+                    for (int q = 0; q < CPG / 32; ++q) tc::tmem_ld32(tcol + uint32_t(q * 32), r[q]);
+                    tc::tmem_ld_wait();
+#pragma unroll
+                    for (int q = 0; q < CPG / 32; ++q) {
+                        float v[32];
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[q][j]);
+                        if (lim < (q + 1) * 32) {
+#pragma unroll
+                            for (int j = 0; j < 32; ++j)
+                                if (q * 32 + j >= lim) v[j] = __int_as_float(0xff800000);
+                        }
+                        if (__any_sync(FULL, max32(v) > ath)) slowq |= 1u << q;
+                    }
+                }
+                long long c1 = t0 ? clock64() : 0;
+                // rare: one compact copy of the admission code, the flagged
+                // chunks re-read from TMEM (the buffer is released after this)
+#pragma unroll 1
+                while (slowq) {
+                    const int q = __ffs(slowq) - 1;
+                    slowq &= slowq - 1;
+                    uint32_t x[32];
+                    tc::tmem_ld32(tcol + uint32_t(q * 32), x);
+                    tc::tmem_ld_wait();
+                    uint32_t lm = 0;  // this lane's admitted columns
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        if (q * 32 + j < lim && __uint_as_float(x[j]) > ath) lm |= 1u << j;
+                    if (__reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > uint32_t(BUF)) {
+                        ++drains;
+                        drain();  // cnt = 0, and at most 32 admissions follow
+                    }
+                    const uint32_t wm = __reduce_or_sync(FULL, lm);  // the warp's union
+                    const uint32_t cb0 = cbase + q * 32;
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        if (wm & (1u << j)) {
+                            if (((lm >> j) & 1u) && cb0 + j != qself) {
+                                bd[cnt * TQ] = fmaf(-2.0f, __uint_as_float(x[j]), qn);
+                                bi[cnt * TQ] = cb0 + j;
+                                ++cnt;
+                            }
+                        }
+                    }
+                }
+                tc::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&B.t_empty[tb]);
+                ++ti;
+                if (t0) {  // epi-wait: wait + fast filter; epi-work: admissions
+                    const long long c2 = clock64();
+                    c_wait += c1 - c0;
+                    c_work += c2 - c1;
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                break;
+            }
+            // job end: drain, sort the heap in registers, write one run of S
+            long long c3 = t0 ? clock64() : 0;
+            drain();
+            if (valid) {
+                float kv[S];
+                uint32_t ki[S];
+#pragma unroll
+                for (int j = 0; j < S; ++j) {
+                    kv[j] = hd[j * TQ];
+                    ki[j] = hi[j * TQ];
+                }
+                sort_pairs<S>(kv, ki);
+                float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
+                uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
+#pragma unroll
+                for (int j = 0; j < S / 4; ++j) {
+                    od[j] = make_float4(kv[4 * j], kv[4 * j + 1], kv[4 * j + 2], kv[4 * j + 3]);
+                    oi[j] = make_uint4(ki[4 * j], ki[4 * j + 1], ki[4 * j + 2], ki[4 * j + 3]);
+                }
+            }
+            ++jobs;
+            if (t0) c_end += clock64() - c3;
+        }
+        if (t0) {
+            a.trace[IVF_T_EPI_WAIT] = (unsigned long long)c_wait;
+            a.trace[IVF_T_EPI_WORK] = (unsigned long long)c_work;
+            a.trace[IVF_T_EPI_END] = (unsigned long long)c_end;
+            a.trace[IVF_T_DRAINS] = drains;
+            a.trace[IVF_T_JOBS] = jobs;
+        }
+    }
+    __syncthreads();
+    if (tracing && tid == 0) a.trace[IVF_T_TOTAL] = (unsigned long long)(clock64() - c_start);
+    if (*abort_flag && tid == 0) atomicExch(a.err, 2);
+    tc::tc_fence_after();
+    if (w == 0) tc::tmem_dealloc(taddr, 512);
+}
+
+// ── host: tensor maps ────────────────────────────────────────────────────
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                  const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                  const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                  CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn() {
+    static EncodeTiledFn fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void* p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) ==
+                cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiledFn>(p);
+    }
+    return fn;
+}
+
+template <int S>
+size_t tiles_smem() {
+    return 1024 + size_t(QST) * TQ * ROWB + size_t(cand_stages(S)) * TCN * ROWB +
+           size_t(NG) * S * TQ * 8 + size_t(NG) * BUF * TQ * 8;
+}
+
+template <int S>
+cudaError_t launch_s(const CUtensorMap& tmQ, const CUtensorMap& tmC, const IvfTileArgs& a,
+                     int grid, cudaStream_t st) {
+    const size_t sm = tiles_smem<S>();
+    cudaError_t e = cudaFuncSetAttribute(k_ivf_tiles<S>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
+    if (e != cudaSuccess) return e;
+    k_ivf_tiles<S><<<grid, NT, sm, st>>>(tmQ, tmC, a); count_launch();
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+// A [rows x 64] BF16 row-major matrix (128-byte rows) as 128-byte-swizzled
+// boxes of box_rows x 64.
+bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {64, rows};
+    cuuint64_t strides[1] = {ROWB};
+    cuuint32_t box[2] = {64, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
+int ivf_groups() { return NG; }
+
+int ivf_shortlist(int want) { return want <= 16 ? 16 : (want <= 32 ? 32 : 0); }
+
+cudaError_t launch_ivf_tiles(const CUtensorMap& tmQ, const CUtensorMap& tmC,
+                             const IvfTileArgs& a, int grid, cudaStream_t st) {
+    if (a.njobs == 0) return cudaSuccess;
+    if (a.S == 16) return launch_s<16>(tmQ, tmC, a, grid, st);
+    if (a.S == 32) return launch_s<32>(tmQ, tmC, a, grid, st);
+    return cudaErrorInvalidValue;
+}
+
+}  // namespace pq

@@ -1,0 +1,43 @@
+// Chosen form (tensor-core shortlist) interfaces.
+#pragma once
+
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace pq {
+
+// One tensor-core tile job list: job j covers query entries
+// [job_qstart[j], job_qend[j]) (at most 128) against the candidates
+// [c_off[b], c_off[b + 1]) of bucket b = job_bucket[j].  Query rows are
+// [q~, -1/2, -1/2, 0...] and candidate rows [x~, hi, lo, 0...] (BF16, 64
+// columns) with hi + lo = |x~|^2.
+struct IvfTileArgs {
+    const uint32_t* job_bucket;  // the job's candidate bucket
+    const uint32_t* job_qstart;  // the job's query entries [qstart, qend)
+    const uint32_t* job_qend;
+    uint32_t njobs;
+    const uint32_t* c_off;   // buckets + 1
+    const float* qnorm;      // per query entry: |q~|^2 of its BF16 row
+    const float* qthr;       // optional per query entry: initial admission bound
+    const uint32_t* qself;   // per query entry: its own candidate position, or ~0
+    int S;                   // shortlist length per entry and column half: 16 or 32
+    float* out_d;            // entries x (ivf_groups() x S): ascending runs of S
+    uint32_t* out_i;         // the candidate positions (~0 = none)
+    int* err;
+    unsigned long long* trace;  // optional: block 0 cycle counters (IVF_T_*)
+};
+
+enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT_C = 3,
+       IVF_T_MMA_WAIT_T = 4, IVF_T_TMA_WAIT = 5, IVF_T_TILES = 6, IVF_T_DRAINS = 7,
+       IVF_T_TOTAL = 8, IVF_T_JOBS = 9, IVF_TRACE_N = 10 };
+
+bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
+// Runs of one entry's output row.
+int ivf_groups();
+// The shortlist length the kernel supports for `want` entries (0 = too many).
+int ivf_shortlist(int want);
+cudaError_t launch_ivf_tiles(const CUtensorMap& tmQ, const CUtensorMap& tmC,
+                             const IvfTileArgs& a, int grid, cudaStream_t st);
+
+}  // namespace pq

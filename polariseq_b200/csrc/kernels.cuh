@@ -74,9 +74,11 @@ void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, ui
                      cudaStream_t st, cudaStream_t st_big);
 
 // Leaf all-pairs of one tree into the heaps (nndescent.rs:785-815).
+// leaf_cap: the largest leaf the forest can produce below depth 101 (leaf_size).
 void launch_leaf_pairs(const float* X, int d, int dp, const uint32_t* ids_t,
                        const uint32_t* leaf_start, uint32_t nleaves, uint32_t n, int k,
-                       uint32_t* hidx, float* hdist, uint8_t* hflag, cudaStream_t st);
+                       uint32_t leaf_cap, uint32_t* hidx, float* hdist, uint8_t* hflag,
+                       cudaStream_t st);
 void launch_leaf_compact(const uint8_t* leafflag_t, uint32_t n, uint32_t* leaf_start,
                          uint32_t* scan_buf, void* scan_temp, uint64_t* count_dev,
                          cudaStream_t st);

@@ -1,0 +1,75 @@
+"""The tensor-core shortlist form (mode='bf16') on the GPU: graph structure,
+determinism and recall@k against the FP64 exact oracle.
+
+Its graph is not the reference's (a different search), so it is judged by
+recall@k >= 0.99 against FP64 brute force with (distance, index) order and by
+its distances: every returned distance is the exact FP32 distance of its pair
+in the reference's summation order."""
+
+import numpy as np
+import pytest
+
+import oracle
+import polariseq_b200 as pq
+from polariseq_b200 import synth
+
+pytestmark = pytest.mark.gpu
+
+
+def recall(g, data, k, queries):
+    ex, _ = oracle.exact_knn_f64(data, queries, k)
+    a = g["indices"].reshape(-1, k)[queries]
+    return np.mean([len(set(a[i]) & set(ex[i])) / k for i in range(len(queries))])
+
+
+def check_structure(g, n, k):
+    ip, ix, dx = g["indptr"], g["indices"], g["data"]
+    assert np.all(np.diff(ip) == k)
+    rows = ix.reshape(n, k)
+    assert not (rows == np.arange(n)[:, None]).any(), "self-loop"
+    assert all(len(set(r)) == k for r in rows[:: max(1, n // 2000)]), "duplicate neighbour"
+    assert (np.diff(dx.reshape(n, k), axis=1) >= 0).all(), "not sorted"
+
+
+@pytest.mark.parametrize("n,comps", [(20_000, 20), (120_000, 40)])
+def test_bf16_form_recall_and_structure(n, comps):
+    x = synth.mixture_lognormal(n, 50, comps, seed=5)
+    g = pq.nndescent_dense(x, 15, mode="bf16")
+    check_structure(g, n, 15)
+    q = np.random.default_rng(1).choice(n, 2000, replace=False).astype(np.uint32)
+    assert recall(g, x, 15, q) >= 0.99
+
+
+def test_bf16_form_distances_are_exact_fp32():
+    x = synth.mixture_dirichlet(20_000, 50, 20, 0)
+    g = pq.nndescent_dense(x, 15, mode="bf16")
+    ix = g["indices"].reshape(-1, 15)
+    dx = g["data"].reshape(-1, 15)
+    for i in range(0, 20_000, 997):
+        for t in range(15):
+            want = np.sqrt(oracle.sq_dist(x[i], x[ix[i, t]]))
+            assert dx[i, t] == np.float32(want)
+
+
+def test_bf16_form_is_deterministic():
+    x = synth.mixture_lognormal(50_000, 50, 30, seed=2)
+    a = pq.nndescent_dense(x, 15, mode="bf16")
+    b = pq.nndescent_dense(x, 15, mode="bf16")
+    np.testing.assert_array_equal(a["indices"], b["indices"])
+    assert a["data"].tobytes() == b["data"].tobytes()
+
+
+def test_bf16_form_k30_and_30_pcs():
+    x = synth.mixture_lognormal(40_000, 30, 10, seed=3)
+    g = pq.nndescent_dense(x, 30, mode="bf16")
+    check_structure(g, 40_000, 30)
+    q = np.random.default_rng(2).choice(40_000, 1000, replace=False).astype(np.uint32)
+    assert recall(g, x, 30, q) >= 0.99
+
+
+def test_bf16_form_small_inputs_are_exact():
+    # one bucket: the shortlist covers every cell, so the graph is the exact kNN
+    x = synth.blobs_rust_tests(3000, 8, 4, 1)
+    g = pq.nndescent_dense(x, 10, mode="bf16")
+    q = np.arange(0, 3000, 7, dtype=np.uint32)
+    assert recall(g, x, 10, q) >= 0.999
