@@ -35,6 +35,9 @@ typedef enum pq_status {
     PQ_ENOTSUP = 5   /* option combination not supported by this build */
 } pq_status;
 
+/* Metric of the exact search (neighbors.rs:16-39). */
+enum { PQ_METRIC_EUCLIDEAN = 0, PQ_METRIC_COSINE = 1 };
+
 /* Search form.  PLAIN reproduces the reference graph bit for bit. */
 enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
 /* Initial neighbour lists: the reference's RP-tree forest, or learned buckets. */
@@ -136,6 +139,29 @@ int pq_nndescent_probe(pq_ctx* ctx, const float* data, uint64_t n_obs, uint64_t 
 int pq_debug_tree(pq_ctx* ctx, const float* data, uint64_t n_obs, uint64_t n_dim,
                   const pq_nnd_opts* opts, uint32_t tree, uint32_t* ids, uint32_t* leaves,
                   uint64_t leaves_cap, uint64_t* n_leaves);
+
+/* neighbors::neighbors (crates/polariseq-core/src/neighbors.rs:101-147), the
+ * exact brute-force kNN behind PyO3 neighbors_dense (crates/polariseq-python/
+ * src/lib.rs:474-501), bit for bit: each cell's k_with_self = min(n_neighbors,
+ * n_obs) nearest are searched including itself and the closest is dropped, so
+ * every row has k_with_self - 1 entries; distances are Euclidean (sqrt of the
+ * reference's squared distance) or cosine (1 - cos).  HOST buffers: indptr
+ * n_obs+1, indices/dists at least n_obs * (k_with_self - 1).  Errors follow
+ * NeighborsError (neighbors.rs:62-84): PQ_EINVAL for empty input, zero
+ * neighbours or an unknown metric; PQ_ENOTSUP above n_dim 512 or
+ * k_with_self 256. */
+int pq_neighbors_into(pq_ctx* ctx, const float* data, uint64_t n_obs, uint64_t n_dim,
+                      uint64_t n_neighbors, int32_t metric, uint32_t* indptr,
+                      uint64_t indptr_len, uint32_t* indices, uint64_t indices_len,
+                      float* dists, uint64_t dists_len, uint64_t* nnz_out);
+
+/* The same with DEVICE buffers (data n_obs x n_dim row-major f32, any
+ * alignment); `stream` (a cudaStream_t, may be null) is ordered before and
+ * after the search.  The context's workspace holds the cosine row norms. */
+int pq_neighbors_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_obs, uint64_t n_dim,
+                             uint64_t n_neighbors, int32_t metric, uint32_t* d_indptr,
+                             uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
+                             void* stream);
 
 #ifdef __cplusplus
 }

@@ -29,6 +29,7 @@ from . import _lib
 
 __all__ = [
     "PanicException", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
+    "neighbors_dense",
 ]
 
 
@@ -143,6 +144,39 @@ class Context:
             self._check(rc, "nndescent_device")
         return int(nnz.value)
 
+    # -- exact kNN (neighbors::neighbors) -----------------------------------
+    def _check_neighbors(self, rc: int) -> None:
+        if rc == _lib.PQ_EINVAL:  # NeighborsError -> RuntimeError (lib.rs:493-495)
+            msg = _lib.load().pq_ctx_last_error(self._h).decode(errors="replace")
+            raise RuntimeError(f"neighbors failed: {msg}")
+        self._check(rc, "neighbors")
+
+    def neighbors_into(self, data: np.ndarray, n_neighbors: int, metric: int,
+                       indptr: np.ndarray, indices: np.ndarray, dists: np.ndarray) -> int:
+        n, d = data.shape
+        nnz = C.c_uint64(0)
+        with self._lock:
+            rc = _lib.load().pq_neighbors_into(
+                self._h, data.ctypes.data, n, d, int(n_neighbors), int(metric),
+                indptr.ctypes.data, indptr.size, indices.ctypes.data, indices.size,
+                dists.ctypes.data, dists.size, C.byref(nnz))
+            self._check_neighbors(rc)
+        return int(nnz.value)
+
+    def neighbors_device(self, data, n_neighbors: int, metric: int, indptr, indices, dists,
+                         stream=None) -> int:
+        """`data` float32 [n, d], `indptr` [n+1], `indices`/`dists` [>= n*(k-1)]:
+        contiguous CUDA tensors."""
+        n, d = int(data.shape[0]), int(data.shape[1])
+        nnz = C.c_uint64(0)
+        sp = None if stream is None else C.c_void_p(int(stream))
+        with self._lock:
+            rc = _lib.load().pq_neighbors_into_device(
+                self._h, data.data_ptr(), n, d, int(n_neighbors), int(metric),
+                indptr.data_ptr(), indices.data_ptr(), dists.data_ptr(), C.byref(nnz), sp)
+            self._check_neighbors(rc)
+        return int(nnz.value)
+
     # -- parity probes (test hooks) ----------------------------------------
     def probe(self, data: np.ndarray, opts: _lib.NndOpts, stop_after: int) -> dict:
         data = np.ascontiguousarray(data, np.float32)
@@ -249,6 +283,36 @@ def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_
     ix = np.zeros(cap, np.uint32)
     dx = np.zeros(cap, np.float32)
     nnz = ctx.nndescent_into(emb, opts, ip, ix, dx)
+    return {"indptr": ip, "indices": ix[:nnz], "data": dx[:nnz], "n_obs": n_obs}
+
+
+METRICS = {"euclidean": _lib.PQ_METRIC_EUCLIDEAN, "cosine": _lib.PQ_METRIC_COSINE}
+
+
+def neighbors_dense(embedding, n_neighbors, metric, *, device: int = 0) -> dict:
+    """Exact kNN graph, bit-exact with the reference's ``neighbors_dense``
+    (crates/polariseq-python/src/lib.rs:474-501, neighbors.rs:101-241).
+
+    Every cell searches its ``min(n_neighbors, n_obs)`` nearest including
+    itself; the closest is dropped, so each row holds ``min(n_neighbors,
+    n_obs) - 1`` entries, ascending.  ``metric`` is ``"euclidean"`` (distances
+    are sqrt of the squared distance) or ``"cosine"`` (1 - cosine similarity),
+    case-insensitive.  Returns ``{"indptr", "indices", "data", "n_obs"}``."""
+    if not isinstance(embedding, np.ndarray) or embedding.ndim != 2:
+        raise TypeError("argument 'embedding': expected a 2-D numpy.ndarray of float32")
+    if embedding.dtype != np.float32:
+        raise TypeError(f"argument 'embedding': expected float32, got {embedding.dtype}")
+    m = METRICS.get(str(metric).lower())
+    if m is None:
+        raise RuntimeError(f"unknown metric: {metric}")
+    emb = np.ascontiguousarray(embedding)  # the binding copies the array (lib.rs:484)
+    n_obs = emb.shape[0]
+    kws = min(int(n_neighbors), n_obs)
+    nnz_cap = max(n_obs * max(kws - 1, 0), 1)
+    ip = np.zeros(n_obs + 1, np.uint32)
+    ix = np.zeros(nnz_cap, np.uint32)
+    dx = np.zeros(nnz_cap, np.float32)
+    nnz = default_context(device).neighbors_into(emb, int(n_neighbors), m, ip, ix, dx)
     return {"indptr": ip, "indices": ix[:nnz], "data": dx[:nnz], "n_obs": n_obs}
 
 

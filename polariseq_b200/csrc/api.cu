@@ -8,6 +8,7 @@
 #include <functional>
 
 #include "ctx.cuh"
+#include "exact.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
@@ -470,6 +471,29 @@ int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
     return PQ_OK;
 }
 
+// neighbors::neighbors argument rules (neighbors.rs:106-117) and the limits of
+// the exact kernel.
+int check_neighbors(pq_ctx* c, uint64_t n, uint64_t d, uint64_t nn, int32_t metric) {
+    if (!c) return PQ_EINVAL;
+    if (n == 0 || d == 0)
+        return fail(c, PQ_EINVAL, "embedding has zero rows (" + std::to_string(n) + ") or dims (" +
+                                      std::to_string(d) + ")");
+    if (nn == 0) return fail(c, PQ_EINVAL, "n_neighbors must be >= 1, got 0");
+    if (metric != PQ_METRIC_EUCLIDEAN && metric != PQ_METRIC_COSINE)
+        return fail(c, PQ_EINVAL, "unknown metric");
+    if (n >= 0xFFFFFFFEull) return fail(c, PQ_EINVAL, "n_obs must be below 2^32 - 1");
+    const uint64_t kws = std::min(nn, n);
+    if (kws > uint64_t(pq::EXACT_MAX_K))
+        return fail(c, PQ_ENOTSUP, "the exact search supports n_neighbors <= " +
+                                       std::to_string(pq::EXACT_MAX_K));
+    if (d > uint64_t(pq::EXACT_MAX_DIM))
+        return fail(c, PQ_ENOTSUP, "the exact search supports n_dim <= " +
+                                       std::to_string(pq::EXACT_MAX_DIM));
+    if (n * (kws - 1) >= 0xFFFFFFFFull)
+        return fail(c, PQ_EINVAL, "n_obs * (n_neighbors - 1) must be below 2^32");
+    return PQ_OK;
+}
+
 template <class F>
 int guarded(pq_ctx* c, F&& f) {
     try {
@@ -652,6 +676,69 @@ int pq_debug_tree(pq_ctx* c, const float* data, uint64_t n, uint64_t d, const pq
         p.leaves_cap = leaves_cap;
         p.n_leaves = n_leaves;
         build_plain(c, data, true, n, d, *o, nullptr, nullptr, nullptr, &p);
+        return PQ_OK;
+    });
+}
+
+int pq_neighbors_into(pq_ctx* c, const float* data, uint64_t n, uint64_t d,
+                      uint64_t n_neighbors, int32_t metric, uint32_t* indptr,
+                      uint64_t indptr_len, uint32_t* indices, uint64_t indices_len,
+                      float* dists, uint64_t dists_len, uint64_t* nnz_out) {
+    int rc = check_neighbors(c, n, d, n_neighbors, metric);
+    if (rc != PQ_OK) return rc;
+    if (!data || !indptr || !indices || !dists || !nnz_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    const uint64_t kws = std::min(n_neighbors, n), nnz = n * (kws - 1);
+    if (indptr_len != n + 1) return fail(c, PQ_EINVAL, "indptr must have n_obs + 1 entries");
+    if (indices_len < nnz || dists_len < nnz)
+        return fail(c, PQ_EINVAL, "the graph arrays are too short");
+    return guarded(c, [&]() -> int {
+        cudaStream_t st = c->stream;
+        float* X = c->get<float>("ex_X", n * d);
+        float* norms = c->get<float>("ex_norms", n);
+        uint32_t* dip = c->get<uint32_t>("out_indptr", n + 1);
+        uint32_t* dix = c->get<uint32_t>("out_indices", std::max<uint64_t>(nnz, 1));
+        float* ddx = c->get<float>("out_dists", std::max<uint64_t>(nnz, 1));
+        ck(cudaMemcpyAsync(X, data, n * d * 4, cudaMemcpyHostToDevice, st), "h2d");
+        ck(pq::exact_knn_prepare(), "exact kNN set-up");
+        ck(pq::launch_exact_knn(X, n, int(d), int(kws), metric == PQ_METRIC_COSINE, norms, dip, dix,
+                            ddx, st),
+           "exact kNN");
+        ck(cudaMemcpyAsync(indptr, dip, (n + 1) * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        if (nnz) {
+            ck(cudaMemcpyAsync(indices, dix, nnz * 4, cudaMemcpyDeviceToHost, st), "d2h");
+            ck(cudaMemcpyAsync(dists, ddx, nnz * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        }
+        ck(cudaStreamSynchronize(st), "d2h");
+        *nnz_out = nnz;
+        return PQ_OK;
+    });
+}
+
+int pq_neighbors_into_device(pq_ctx* c, const float* d_data, uint64_t n, uint64_t d,
+                             uint64_t n_neighbors, int32_t metric, uint32_t* d_indptr,
+                             uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
+                             void* stream) {
+    int rc = check_neighbors(c, n, d, n_neighbors, metric);
+    if (rc != PQ_OK) return rc;
+    if (!d_data || !d_indptr || !d_indices || !d_dists || !nnz_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    const uint64_t kws = std::min(n_neighbors, n);
+    return guarded(c, [&]() -> int {
+        cudaStream_t user = static_cast<cudaStream_t>(stream);
+        float* norms = c->get<float>("ex_norms", n);
+        cudaEvent_t ev;
+        ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        ck(cudaEventRecord(ev, user), "event");
+        ck(cudaStreamWaitEvent(c->stream, ev, 0), "event");
+        ck(pq::exact_knn_prepare(), "exact kNN set-up");
+        ck(pq::launch_exact_knn(d_data, n, int(d), int(kws), metric == PQ_METRIC_COSINE, norms,
+                            d_indptr, d_indices, d_dists, c->stream),
+           "exact kNN");
+        ck(cudaEventRecord(ev, c->stream), "event");
+        ck(cudaStreamWaitEvent(user, ev, 0), "event");
+        cudaEventDestroy(ev);
+        *nnz_out = n * (kws - 1);
         return PQ_OK;
     });
 }
