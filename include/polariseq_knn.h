@@ -32,7 +32,8 @@ typedef enum pq_status {
     PQ_ENOMEM = 2,   /* device allocation failed */
     PQ_EDEVICE = 3,  /* CUDA error, no device, or a kernel reported an error flag */
     PQ_ETIMEOUT = 4, /* a bounded device-side wait gave up */
-    PQ_ENOTSUP = 5   /* option combination not supported by this build */
+    PQ_ENOTSUP = 5,  /* option combination not supported by this build */
+    PQ_ETOOBIG = 6   /* input beyond the fixed capacity of an allocation-free entry point */
 } pq_status;
 
 /* Metric of the exact search (neighbors.rs:16-39). */
@@ -162,6 +163,31 @@ int pq_neighbors_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_obs, u
                              uint64_t n_neighbors, int32_t metric, uint32_t* d_indptr,
                              uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
                              void* stream);
+
+/* Allocation-free exact kNN.  No counterpart in the reference: it is an
+ * addition of this library for callers that must not allocate device memory,
+ * such as a host framework that owns the whole device budget through its own
+ * pool (a cudaMalloc outside it can push the framework out of memory), or a
+ * serving loop where cudaMalloc / cudaFree would synchronise the device and
+ * stall the work of other streams.  It computes exactly what
+ * pq_neighbors_into_device computes, with DEVICE buffers the caller passes,
+ * enqueued on `stream` (a cudaStream_t, may be null) of the current device; it
+ * needs no context, calls no allocator and does not wait for the GPU.
+ *
+ * Limit: n_obs <= 262144 (PQ_ETOOBIG beyond), n_dim <= 512 and
+ * min(n_neighbors, n_obs) <= 256 (PQ_ENOTSUP beyond).  The cosine metric keeps
+ * per-row norms in one fixed 1 MiB device array inside the library, shared by
+ * every call on that device: nothing in it needs to start at zero (each call
+ * writes the norms it reads before reading them), but calls whose work
+ * overlaps on the GPU (other streams, other host threads) race on it, so
+ * order them.  The first call on each device does a one-time set-up (looks up
+ * that array's device address and loads the kernels): make it before any
+ * stream capture.  Errors: PQ_EINVAL (null buffer, empty data, zero
+ * neighbours, unknown metric), PQ_ETOOBIG, PQ_ENOTSUP, PQ_EDEVICE. */
+int pq_neighbors_into_device_noalloc(const float* d_data, uint64_t n_obs, uint64_t n_dim,
+                                     uint64_t n_neighbors, int32_t metric, uint32_t* d_indptr,
+                                     uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
+                                     void* stream);
 
 #ifdef __cplusplus
 }

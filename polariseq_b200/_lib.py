@@ -12,7 +12,7 @@ import threading
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "_build", "libpq_knn.so")
 
-PQ_OK, PQ_EINVAL, PQ_ENOMEM, PQ_EDEVICE, PQ_ETIMEOUT, PQ_ENOTSUP = range(6)
+PQ_OK, PQ_EINVAL, PQ_ENOMEM, PQ_EDEVICE, PQ_ETIMEOUT, PQ_ENOTSUP, PQ_ETOOBIG = range(7)
 PQ_MODE_PLAIN, PQ_MODE_BF16, PQ_MODE_FP8 = 0, 1, 2
 PQ_INIT_RP, PQ_INIT_LEARNED = 0, 1
 PQ_METRIC_EUCLIDEAN, PQ_METRIC_COSINE = 0, 1
@@ -22,7 +22,7 @@ EXPORTS = (
     "pq_nnd_opts_default", "pq_effective_k", "pq_ctx_create", "pq_ctx_destroy",
     "pq_ctx_last_error", "pq_ctx_stats", "pq_nndescent_into", "pq_nndescent_into_device",
     "pq_nndescent_probe", "pq_debug_tree", "pq_ctx_set_profiling", "pq_neighbors_into",
-    "pq_neighbors_into_device",
+    "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc",
 )
 
 
@@ -126,5 +126,8 @@ def load(build_if_missing: bool = False):
         L.pq_neighbors_into_device.argtypes = [P, P, U64, U64, U64, C.c_int32, P, P, P,
                                                 C.POINTER(U64), P]
         L.pq_neighbors_into_device.restype = C.c_int
+        L.pq_neighbors_into_device_noalloc.argtypes = [P, U64, U64, U64, C.c_int32, P, P, P,
+                                                        C.POINTER(U64), P]
+        L.pq_neighbors_into_device_noalloc.restype = C.c_int
         _lib = L
         return L

@@ -21,8 +21,11 @@
 // dot(b, b)).
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "common.cuh"
 #include "exact.cuh"
+#include "polariseq_knn.h"
 
 namespace pq {
 namespace {
@@ -242,3 +245,71 @@ cudaError_t launch_exact_knn(const float* X, uint64_t n, int d, int kws, int cos
 }
 
 }  // namespace pq
+
+// ── allocation-free variant ─────────────────────────────────────────────────
+// Scratch of pq_neighbors_into_device_noalloc: the cosine metric's per-row
+// |x|^2, for at most EXACT_NOALLOC_MAX_ROWS rows (1 MiB).  It lives in every
+// device that loads the library, from load until process exit.  In host code
+// the name below stands for a host-side shadow, not the device array: the
+// device address comes from cudaGetSymbolAddress at set-up.
+namespace pq {
+namespace {
+
+constexpr uint64_t EXACT_NOALLOC_MAX_ROWS = uint64_t(1) << 18;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) float g_noalloc_norms[EXACT_NOALLOC_MAX_ROWS];
+
+std::mutex g_noalloc_mu;
+float* g_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};
+
+// Once per device, with that device current: the scratch array's device
+// address, and the kernels loaded with their shared-memory limit raised.
+cudaError_t noalloc_setup(int dev, float** out) {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        float* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_noalloc_norms);
+        if (e != cudaSuccess) return e;
+        if ((e = exact_knn_prepare()) != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
+}  // namespace
+}  // namespace pq
+
+extern "C" int pq_neighbors_into_device_noalloc(const float* d_data, uint64_t n_obs,
+                                                uint64_t n_dim, uint64_t n_neighbors,
+                                                int32_t metric, uint32_t* d_indptr,
+                                                uint32_t* d_indices, float* d_dists,
+                                                uint64_t* nnz_out, void* stream) {
+    using namespace pq;
+    if (!d_data || !d_indptr || !d_indices || !d_dists || !nnz_out) return PQ_EINVAL;
+    if (n_obs == 0 || n_dim == 0 || n_neighbors == 0) return PQ_EINVAL;
+    if (metric != PQ_METRIC_EUCLIDEAN && metric != PQ_METRIC_COSINE) return PQ_EINVAL;
+    if (n_obs > EXACT_NOALLOC_MAX_ROWS) return PQ_ETOOBIG;
+    const uint64_t kws = n_neighbors < n_obs ? n_neighbors : n_obs;
+    if (kws > uint64_t(EXACT_MAX_K) || n_dim > uint64_t(EXACT_MAX_DIM)) return PQ_ENOTSUP;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+        cudaGetLastError();
+        return PQ_EDEVICE;
+    }
+    float* norms = nullptr;
+    if (noalloc_setup(dev, &norms) != cudaSuccess) {
+        cudaGetLastError();
+        return PQ_EDEVICE;
+    }
+    // every norm the search reads is written first, on the same stream
+    if (launch_exact_knn(d_data, n_obs, int(n_dim), int(kws), metric == PQ_METRIC_COSINE, norms,
+                         d_indptr, d_indices, d_dists,
+                         static_cast<cudaStream_t>(stream)) != cudaSuccess) {
+        cudaGetLastError();
+        return PQ_EDEVICE;
+    }
+    *nnz_out = n_obs * (kws - 1);
+    return PQ_OK;
+}
