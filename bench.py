@@ -54,7 +54,9 @@ def parse():
     ap.add_argument("--queries", type=int, default=20_000)
     ap.add_argument("--cpu-sample", type=int, default=262_144)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--form", default="plain", choices=["plain", "bf16"])
+    ap.add_argument("--form", default="bf16", choices=["plain", "bf16"],
+                    help="the headline form (the other is measured too unless --skip-other)")
+    ap.add_argument("--skip-other", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="run W warm-up and K device-resident builds, print nothing else "
                          "(for ncu launch lists)")
@@ -72,7 +74,7 @@ def config(args):
                         f"{args.comps}-component log-normal Gaussian mixture, 5% doublets",
             "n_cells": args.n, "n_pcs": args.d, "k": args.k,
             "form": "plain (bit-exact)" if args.form == "plain" else
-                    "bf16 tensor-core shortlist + FP32 re-rank + FP64 boundary",
+                    "chosen: bf16 tensor-core shortlist + FP32 re-rank + FP64 boundary",
             "l2": "inputs larger than L2 (embedding 800 MB, graph 480 MB)"}
 
 
@@ -194,19 +196,110 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# Algorithmic bytes of one launch of the dominant kernel group, per unit.
-def algorithmic_bytes(group, st, args):
-    n, d, k = args.n, args.d, args.k
-    row = 4 * d
-    if group == "join_count":
-        # every non-empty candidate row of every source row read once, the
-        # candidate ids and thresholds, and the emit bits written
-        m = st["max_candidates"]
-        return n * (2 * m * row + 2 * m * 8 + (4 * m * m) // 8 + 4)
-    if group == "seqtree":
-        # each point's row read once per level it passes below the top levels
+# DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel,
+# from an ncu capture of the same kernel (profiles/k_ivf_tiles_*.md); the
+# traffic of a launch scales with the tile pairs it processes.
+TILE_DRAM_BYTES_PER_PAIR = None
+
+
+def tiles_roofline(per, st, args, peaks):
+    """The shortlist tile kernel against the tensor pipe: algorithmic flops are
+    2 * (query entry, candidate) pairs * d (unpadded), per launch, over the
+    launch's CUDA-event time."""
+    g = per.get("tiles")
+    if not g or g["launches_per_build"] == 0:
         return None
-    return None
+    cells = st["shortlist"][3]
+    tile_pairs = st["shortlist"][0]
+    L = g["launches_per_build"]
+    sec = g["ms_per_build"] / L / 1000.0
+    flops = 2.0 * cells * args.d / L
+    achieved = flops / sec / 1e12
+    peak = peaks.get("bf16_tflops_sustained") or 1400.0
+    padded = 2.0 * tile_pairs * 128 * 256 * 64 / L / sec / 1e12
+    traffic = (TILE_DRAM_BYTES_PER_PAIR * tile_pairs / L
+               if TILE_DRAM_BYTES_PER_PAIR is not None else None)
+    return {"bound": "tensor", "kernel": "k_ivf_tiles", "achieved": achieved, "peak": peak,
+            "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
+            "padded_tflops": padded, "launches_per_build": L,
+            "peak_source": ("measured sustained bf16" if "bf16_tflops_sustained" in peaks
+                            else "fallback")}
+
+
+def join_roofline(per, st, args, peaks):
+    """The plain form's join pass 1 against HBM: every non-empty candidate row
+    of every source row read once, the candidate ids and thresholds, and the
+    emit bits written, per launch over the launch's CUDA-event time."""
+    g = per.get("join_count")
+    if not g or g["launches_per_build"] == 0:
+        return None
+    n, d = args.n, args.d
+    m = st["max_candidates"]
+    ab = n * (2 * m * 4 * d + 2 * m * 8 + (4 * m * m) // 8 + 4) * g["launches_per_build"]
+    L = g["launches_per_build"]
+    sec = g["ms_per_build"] / L / 1000.0
+    achieved = ab / L / sec / 1e9
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    return {"bound": "hbm", "kernel": "k_join_count", "achieved": achieved, "peak": hbm,
+            "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+
+
+def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, world):
+    """W warm-up then K device-resident builds of one form, timed with CUDA
+    events on the launching stream (max over ranks), with per-group events."""
+    n, k = xd.shape[0], args.k
+    cap = n * pq.effective_k(n, k)
+    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[form])
+    ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    ix = torch.empty(cap, dtype=torch.int32, device=dev)
+    dx = torch.empty(cap, dtype=torch.float32, device=dev)
+
+    def step():
+        return ctx.nndescent_device(xd, opts, ip, ix, dx, stream=stream.cuda_stream)
+
+    for _ in range(max(3, args.warmup)):
+        step()
+    torch.cuda.synchronize(dev)
+    _lib.load().pq_ctx_set_profiling(ctx._h, 1)
+    kg_ms = np.zeros(16)
+    kg_l = np.zeros(16, np.int64)
+    launches = 0
+    stats = []
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        nnz = step()
+        stats.append(ctx.stats())
+        s = _lib.NndStats()
+        _lib.load().pq_ctx_stats(ctx._h, s)
+        kg_ms += np.array(s.kg_ms[:16])
+        kg_l += np.array(s.kg_launches[:16], np.int64)
+        launches += s.launches
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    barrier()
+    _lib.load().pq_ctx_set_profiling(ctx._h, 0)
+    ms = e0.elapsed_time(e1) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    names = _lib.KERNEL_GROUPS
+    per = {names[g]: {"ms_per_build": float(kg_ms[g] / args.steps),
+                      "launches_per_build": int(kg_l[g] // args.steps)}
+           for g in range(len(names)) if kg_l[g] > 0}
+    rec, max_rel = recall_fp64(torch, xd, ix[:nnz].cpu().numpy().view(np.uint32),
+                               dx[:nnz].cpu().numpy(), k, args.queries)
+    st = stats[-1]
+    return {"ms": ms, "value": world * n / (ms / 1000.0), "launches": launches // args.steps,
+            "launches_timed": int(launches), "groups": per, "stats": st,
+            "recall_at_k": rec, "max_rel_dist_err": max_rel, "rounds_run": st["rounds_run"]}
 
 
 def main():
@@ -234,76 +327,50 @@ def main():
     n, d, k = x.shape[0], x.shape[1], args.k
     cap = n * pq.effective_k(n, k)
     ctx = pq.Context(local)
-    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[args.form])
     stream = torch.cuda.current_stream(dev)
     xd = torch.from_numpy(x).to(dev)
-    ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
-    ix = torch.empty(cap, dtype=torch.int32, device=dev)
-    dx = torch.empty(cap, dtype=torch.float32, device=dev)
-
-    def step():
-        return ctx.nndescent_device(xd, opts, ip, ix, dx, stream=stream.cuda_stream)
-
-    if args.profile_only:
-        for _ in range(args.warmup + args.steps):
-            step()
-        torch.cuda.synchronize(dev)
-        st = ctx.stats()
-        print(json.dumps({"profile_only": True, "n": n, "launches_per_build": None,
-                          "ms_total": st["ms_total"]}), flush=True)
-        return
-
-    for _ in range(max(3, args.warmup)):
-        step()
-    torch.cuda.synchronize(dev)
 
     def barrier():
         if world > 1:
             dist.barrier()
 
-    # ── device-resident timed region (with kernel-group events) ──
-    _lib.load().pq_ctx_set_profiling(ctx._h, 1)
+    if args.profile_only:
+        opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[args.form])
+        ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
+        ix = torch.empty(cap, dtype=torch.int32, device=dev)
+        dx = torch.empty(cap, dtype=torch.float32, device=dev)
+        for _ in range(args.warmup + args.steps):
+            ctx.nndescent_device(xd, opts, ip, ix, dx, stream=stream.cuda_stream)
+        torch.cuda.synchronize(dev)
+        print(json.dumps({"profile_only": True, "n": n, "form": args.form,
+                          "ms_total": ctx.stats()["ms_total"]}), flush=True)
+        return
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except OSError:
+        pass
+
+    # ── device-resident timed region of the headline form (clocks sampled) ──
     clocks = Clocks(local)
     clocks.start()
-    kg_ms = np.zeros(16)
-    kg_l = np.zeros(16, np.int64)
-    launches = 0
-    barrier()
-    torch.cuda.synchronize(dev)
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    stats = []
-    for _ in range(args.steps):
-        nnz = step()
-        st = ctx.stats()
-        stats.append(st)
-        s = _lib.NndStats()
-        _lib.load().pq_ctx_stats(ctx._h, s)
-        kg_ms += np.array(s.kg_ms[:16])
-        kg_l += np.array(s.kg_launches[:16], np.int64)
-        launches += s.launches
-    e1.record(stream)
-    torch.cuda.synchronize(dev)
-    barrier()
-    ms = e0.elapsed_time(e1) / args.steps
+    head = measure_form(torch, pq, _lib, ctx, args.form, xd, dev, stream, args, barrier, world)
     ck = clocks.stop()
-    _lib.load().pq_ctx_set_profiling(ctx._h, 0)
-    if world > 1:
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = world * n / (ms / 1000.0)
+    forms = {args.form: head}
+    if not args.skip_other:
+        other = "plain" if args.form != "plain" else "bf16"
+        forms[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, args, barrier,
+                                    world)
 
-    # ── end to end through the C ABI with pinned host buffers ──
+    # ── end to end through the public API with pinned host buffers ──
     hx = torch.from_numpy(x).pin_memory()
     hip = torch.empty(n + 1, dtype=torch.int32).pin_memory()
     hix = torch.empty(cap, dtype=torch.int32).pin_memory()
     hdx = torch.empty(cap, dtype=torch.float32).pin_memory()
     hxn, hipn = hx.numpy(), hip.numpy().view(np.uint32)
     hixn, hdxn = hix.numpy().view(np.uint32), hdx.numpy()
-    pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local,
-                       mode=args.form)  # warm the host path
+    r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
     barrier()
     t0 = time.perf_counter()
     e2e_steps = max(1, min(args.steps, 3))
@@ -316,32 +383,10 @@ def main():
         e2e_ms = float(t.item())
     e2e = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(x.nbytes),
-           "d2h_bytes_per_step": int(4 * (n + 1) + 8 * r["nnz"])}
+           "d2h_bytes_per_step": int(4 * (n + 1) + 8 * r["nnz"]), "steps": e2e_steps}
 
-    # ── quality: recall@k and max relative distance error vs FP64 exact ──
-    rec, max_rel = recall_fp64(torch, xd, hixn[:r["nnz"]], hdxn[:r["nnz"]], k, args.queries)
-
-    # ── roofline of the dominant kernel group ──
-    names = _lib.KERNEL_GROUPS
-    per = {names[g]: {"ms_per_build": kg_ms[g] / args.steps,
-                      "launches_per_build": int(kg_l[g] // args.steps)}
-           for g in range(len(names))}
-    dom = max(per, key=lambda g: per[g]["ms_per_build"])
-    peaks = {}
-    try:
-        peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
-    except OSError:
-        pass
-    hbm = peaks.get("hbm_gbs", 6650.0)
-    roof = None
-    ab = algorithmic_bytes(dom, stats[-1], args)
-    if ab is not None and per[dom]["launches_per_build"] > 0:
-        per_launch_ms = per[dom]["ms_per_build"] / per[dom]["launches_per_build"]
-        bytes_per_launch = ab / per[dom]["launches_per_build"]
-        achieved = bytes_per_launch / (per_launch_ms / 1000.0) / 1e9
-        roof = {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": hbm, "unit": "GB/s",
-                "frac": achieved / hbm, "traffic": None,
-                "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
+    roof = (tiles_roofline(head["groups"], head["stats"], args, peaks) if args.form != "plain"
+            else join_roofline(head["groups"], head["stats"], args, peaks))
 
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -350,17 +395,30 @@ def main():
         except Exception as e:  # pragma: no cover
             cpu = {"error": str(e)}
 
-    st = stats[-1]
-    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-            "warmup": max(3, args.warmup), "ms_per_step": ms, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": config(args), "e2e": e2e, "gpu_launches": int(launches),
+    def summary(f):
+        st = f["stats"]
+        out = {"cells_per_s": f["value"], "ms_per_build": f["ms"],
+               "recall_at_k": f["recall_at_k"], "max_rel_dist_err": f["max_rel_dist_err"],
+               "rounds_run": f["rounds_run"], "launches_per_build": f["launches"],
+               "phases_ms": {"init": st["ms_forest"], "layout_or_leaves": st["ms_leaves"],
+                             "search_or_rounds": st["ms_rounds"], "finish": st["ms_extract"]},
+               "kernel_groups": f["groups"]}
+        return out
+
+    forms_out = {f: summary(v) for f, v in forms.items()}
+    if "plain" in forms:
+        forms_out["plain"]["roofline"] = join_roofline(forms["plain"]["groups"],
+                                                       forms["plain"]["stats"], args, peaks)
+    line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
+            "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": head["ms"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "bf16" if args.form != "plain" else "f32", "data": "synthetic",
+            "config": config(args), "e2e": e2e, "gpu_launches": head["launches_timed"],
             "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
-            "quality": {"recall_at_k": rec, "max_rel_dist_err": max_rel,
+            "quality": {"recall_at_k": head["recall_at_k"],
+                        "max_rel_dist_err": head["max_rel_dist_err"],
                         "queries": min(args.queries, n), "oracle": "FP64 brute force"},
-            "phases_ms": {"forest": st["ms_forest"], "leaf_pairs": st["ms_leaves"],
-                          "rounds": st["ms_rounds"], "extract": st["ms_extract"]},
-            "rounds_run": st["rounds_run"], "kernel_groups": per}
+            "forms": forms_out}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

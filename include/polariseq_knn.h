@@ -58,8 +58,8 @@ typedef struct pq_nnd_opts {
     int32_t mode;            /* PQ_MODE_* */
     int32_t init;            /* PQ_INIT_* */
     /* Tensor-core forms only (ignored by PQ_MODE_PLAIN): */
-    int32_t probes;          /* buckets each cell searches; 0 -> min(12, buckets) */
-    int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (2) */
+    int32_t probes;          /* buckets each cell searches (<= 16); 0 -> min(14, buckets) */
+    int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (0) */
 } pq_nnd_opts;
 
 /* Per-call statistics of the last build on a context. */
@@ -76,6 +76,10 @@ typedef struct pq_nnd_stats {
      * count per kernel group, indexed by PQ_KG_*. */
     double kg_ms[16];
     uint64_t kg_launches[16];
+    /* Tensor-core form: [0] 128x256 tile pairs, [1] largest bucket, [2] buckets,
+     * [3] (query entry, candidate) distances contracted, [4] / [5] tile pairs of
+     * the primary pass / the other probes, [6] FP64 boundary resolutions. */
+    uint64_t shortlist[8];
 } pq_nnd_stats;
 
 /* Kernel groups timed by the profiling mode. */
@@ -89,7 +93,11 @@ enum {
     PQ_KG_SORT = 6,        /* stable sort of join records by destination */
     PQ_KG_REPLAY = 7,      /* per-destination replay of join records */
     PQ_KG_EXTRACT = 8,     /* sorted CSR extract */
-    PQ_KG_COUNT = 9
+    PQ_KG_BUCKETS = 9,     /* tensor-core form: k-means buckets and every cell's probes */
+    PQ_KG_LAYOUT = 10,     /* tensor-core form: bucket-ordered BF16 rows and query entries */
+    PQ_KG_TILES = 11,      /* tensor-core form: the shortlist tile kernel (one launch per pass) */
+    PQ_KG_RERANK = 12,     /* tensor-core form: exact re-rank with the FP64 boundary step */
+    PQ_KG_COUNT = 13
 };
 
 typedef struct pq_ctx pq_ctx;

@@ -115,6 +115,7 @@ class Context:
             "changed": list(s.changed[:r]), "emitted": list(s.emitted[:r]),
             "pairs": list(s.pairs[:r]), "ms_forest": s.ms_forest, "ms_leaves": s.ms_leaves,
             "ms_rounds": s.ms_rounds, "ms_extract": s.ms_extract, "ms_total": s.ms_total,
+            "shortlist": list(s.shortlist),
         }
 
     # -- host-buffer build (the drop-in) ------------------------------------

@@ -65,11 +65,13 @@ class NndStats(C.Structure):
         ("launches", C.c_uint64),
         ("kg_ms", C.c_double * 16),
         ("kg_launches", C.c_uint64 * 16),
+        ("shortlist", C.c_uint64 * 8),
     ]
 
 
 KERNEL_GROUPS = ("forest_top", "seqtree", "leaf_pairs", "candidates", "join_count",
-                 "join_write", "sort", "replay", "extract")
+                 "join_write", "sort", "replay", "extract", "buckets", "layout", "tiles",
+                 "rerank")
 
 
 _lib = None

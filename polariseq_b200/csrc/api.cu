@@ -20,6 +20,16 @@ using namespace pqh;
 
 namespace {
 
+// Padded copy of row-major n x d rows: dst[i][j] = src[i][j] for j < d, 0 up to dp.
+__global__ void k_pad_rows(const float* __restrict__ src, size_t n, int d, int dp,
+                           float* __restrict__ dst) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= n * size_t(dp)) return;
+    const size_t i = t / dp;
+    const int j = int(t - i * dp);
+    dst[t] = j < d ? src[i * d + j] : 0.0f;
+}
+
 __global__ void k_fill_u32(uint32_t* p, size_t n, uint32_t v) {
     size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) p[i] = v;
@@ -58,6 +68,28 @@ struct Probe {
 }  // namespace
 
 namespace pqh {
+float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp) {
+    cudaStream_t st = c->stream;
+    float* X = c->get<float>("X", size_t(n) * dp);
+    const size_t bytes = size_t(n) * d * sizeof(float);
+    if (dp == d) {
+        ck(cudaMemcpyAsync(X, data, bytes,
+                           on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st),
+           "copy embedding");
+        return X;
+    }
+    const float* src = data;
+    if (on_host) {  // one contiguous transfer, then the padding on the device
+        float* stage = c->get<float>("X_stage", size_t(n) * d);
+        ck(cudaMemcpyAsync(stage, data, bytes, cudaMemcpyHostToDevice, st), "copy embedding");
+        src = stage;
+    }
+    k_pad_rows<<<blocks(size_t(n) * dp, 256), 256, 0, st>>>(src, n, d, dp, X);
+    pq::count_launch();
+    ck(cudaGetLastError(), "pad embedding");
+    return X;
+}
+
 int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m, uint64_t seed,
                uint64_t n_iters, uint64_t stop_at, uint32_t* hidx, float* hdist, uint8_t* hflag,
                const uint32_t* perm, int stats_offset,
@@ -178,12 +210,7 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
     const unsigned long long launches0 = g_launches;
 
     // padded rows
-    float* X = c->get<float>("X", size_t(n) * dp);
-    if (dp != d) ck(cudaMemsetAsync(X, 0, size_t(n) * dp * sizeof(float), st), "memset X");
-    ck(cudaMemcpy2DAsync(X, size_t(dp) * sizeof(float), data, size_t(d) * sizeof(float),
-                         size_t(d) * sizeof(float), n,
-                         data_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st),
-       "copy embedding");
+    float* X = load_embedding(c, data, data_on_host, n, d, dp);
 
     // heaps
     uint32_t* hidx = c->get<uint32_t>("hidx", size_t(n) * k);

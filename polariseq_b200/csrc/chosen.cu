@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <optional>
 
 #include "ctx.cuh"
 #include "ivf.cuh"
@@ -174,14 +175,23 @@ __global__ void k_merge_runs(const float* __restrict__ rd, const uint32_t* __res
 }
 
 __global__ void k_primary_keys(const uint32_t* __restrict__ probes, int P, uint32_t n,
-                               uint32_t* __restrict__ keys, uint64_t* __restrict__ vals,
-                               uint32_t* __restrict__ hist) {
+                               uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t b = probes[size_t(i) * P];
-    keys[i] = b;
+    keys[i] = probes[size_t(i) * P];
     vals[i] = i;
-    atomicAdd(&hist[b], 1u);
+}
+
+// Offsets of every key value in a sorted key array: off[v] = first position
+// with key >= v, for v in [0, nkeys]; each off entry is written exactly once
+// (by the position where the key steps past it, or by the last position).
+__global__ void k_key_bounds(const uint32_t* __restrict__ keys, size_t ne, uint32_t nkeys,
+                             uint32_t* __restrict__ off) {
+    const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e > ne) return;
+    const uint32_t lo = e == 0 ? 0u : keys[e - 1] + 1;
+    const uint32_t hi = e == ne ? nkeys : keys[e];
+    for (uint32_t v = lo; v <= hi; ++v) off[v] = uint32_t(e);
 }
 
 __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n,
@@ -199,7 +209,7 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
                                size_t ne, int P, uint32_t C, const uint32_t* __restrict__ probes,
                                const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpoint,
                                uint32_t* __restrict__ qbucket, uint32_t* __restrict__ qself,
-                               uint32_t* __restrict__ entry_of, uint32_t* __restrict__ qhist) {
+                               uint32_t* __restrict__ entry_of) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     const uint64_t v = vals[e];
@@ -210,7 +220,6 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
     qbucket[e] = b;
     qself[e] = b == probes[size_t(i) * P] ? pos_of[i] : 0xFFFFFFFFu;
     entry_of[v] = uint32_t(e);
-    atomicAdd(&qhist[key], 1u);
     (void)r;
 }
 
@@ -417,17 +426,14 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     tot.start();
     const unsigned long long launches0 = g_launches;
 
-    float* X = c->get<float>("X", size_t(n) * dp);
-    if (dp != d) ck(cudaMemsetAsync(X, 0, size_t(n) * dp * sizeof(float), st), "memset X");
-    ck(cudaMemcpy2DAsync(X, size_t(dp) * sizeof(float), data, size_t(d) * sizeof(float),
-                         size_t(d) * sizeof(float), n,
-                         data_on_host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, st),
-       "copy embedding");
+    float* X = load_embedding(c, data, data_on_host, n, d, dp);
 
     // ── 1. buckets ──
     tm.start();
+    std::optional<KGScope> kg_sec;
+    kg_sec.emplace(c, PQ_KG_BUCKETS);
     const uint32_t C = std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
-    const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : 12u, std::min(C, 16u)));
+    const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : 14u, std::min(C, 16u)));
     const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
     if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};
     int num_sms = 148;
@@ -519,23 +525,23 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* ekeys2 = c->get<uint32_t>("ekeys2", ne);
     uint64_t* evals2 = c->get<uint64_t>("evals2", ne);
     k_entry_keys<<<blocks(ne, 256), 256, 0, st>>>(probes, ne, P, C, ekeys, evals); count_launch();
+    kg_sec.reset();
     S_.ms_forest = tm.stop();
 
     // ── 2. layout ──
     tm.start();
+    kg_sec.emplace(c, PQ_KG_LAYOUT);
     void* stemp = c->get<uint8_t>("scan_temp_c", scan_temp_bytes(std::max<size_t>(ne, C + 1)));
     uint32_t* ckeys = c->get<uint32_t>("ckeys_c", n);
     uint64_t* cvals = c->get<uint64_t>("cvals_c", n);
     uint32_t* ckeys2 = c->get<uint32_t>("ckeys_c2", n);
     uint64_t* cvals2 = c->get<uint64_t>("cvals_c2", n);
-    uint32_t* chist = c->get<uint32_t>("chist", C + 1);
-    ck(cudaMemsetAsync(chist, 0, size_t(C + 1) * 4, st), "hist");
-    k_primary_keys<<<blocks(n, 256), 256, 0, st>>>(probes, P, n, ckeys, cvals, chist); count_launch();
+    k_primary_keys<<<blocks(n, 256), 256, 0, st>>>(probes, P, n, ckeys, cvals); count_launch();
     ck(radix_sort_pairs(ckeys, cvals, ckeys2, cvals2, n, key_bits(C),
                         c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
        "sort cand");
     uint32_t* c_off = c->get<uint32_t>("c_off", C + 1);
-    ck(scan_exclusive_u32(chist, c_off, C + 1, stemp, nullptr, st), "scan c");
+    k_key_bounds<<<blocks(size_t(n) + 1, 256), 256, 0, st>>>(ckeys, n, C, c_off); count_launch();
     uint32_t* perm = c->get<uint32_t>("cperm", n);
     uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
     uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
@@ -551,12 +557,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* qbucket = c->get<uint32_t>("qbucket", ne);
     uint32_t* qself = c->get<uint32_t>("qself", ne);
     uint32_t* entry_of = c->get<uint32_t>("entry_of", ne);
-    uint32_t* qhist = c->get<uint32_t>("qhist", 2 * C + 1);
-    ck(cudaMemsetAsync(qhist, 0, size_t(2 * C + 1) * 4, st), "hist");
     k_entry_layout<<<blocks(ne, 256), 256, 0, st>>>(evals, ekeys, ne, P, C, probes, pos_of,
-                                                     qpoint, qbucket, qself, entry_of, qhist); count_launch();
+                                                     qpoint, qbucket, qself, entry_of); count_launch();
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
-    ck(scan_exclusive_u32(qhist, q_off, 2 * C + 1, stemp, nullptr, st), "scan q");
+    k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, 2 * C, q_off); count_launch();
     __nv_bfloat16* qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
     float* qbn = c->get<float>("q_norm", ne);
     k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, 1, qb, qbn); count_launch();
@@ -568,7 +572,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     ck(cudaMemcpy(hc.data(), c_off, size_t(C + 1) * 4, cudaMemcpyDeviceToHost), "c_off");
     // jobs: pass 0 = primary entries (keys [0, C)), pass 1 = the others
     std::vector<uint32_t> jb[2], jq[2], je[2];
-    uint64_t tile_pairs = 0, maxb = 0;
+    uint64_t tile_pairs = 0, maxb = 0, cells = 0, pass_pairs[2] = {0, 0};
     for (int pass = 0; pass < 2; ++pass)
         for (uint32_t b = 0; b < C; ++b) {
             const uint32_t key = b + (pass ? C : 0);
@@ -579,15 +583,21 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                 jq[pass].push_back(q0);
                 je[pass].push_back(std::min(q0 + 128, hq[key + 1]));
                 tile_pairs += nct;
+                pass_pairs[pass] += nct;
+                cells += uint64_t(std::min(q0 + 128, hq[key + 1]) - q0) * (hc[b + 1] - hc[b]);
             }
         }
-    S_.pairs[0] = tile_pairs;  // 128 x 256 tensor-core tiles
-    S_.pairs[1] = maxb;        // largest bucket
-    S_.pairs[2] = C;
+    S_.shortlist[0] = tile_pairs;
+    S_.shortlist[1] = maxb;
+    S_.shortlist[2] = C;
+    S_.shortlist[3] = cells;
+    S_.shortlist[4] = pass_pairs[0];
+    S_.shortlist[5] = pass_pairs[1];
     if (std::getenv("POLARISEQ_TRACE"))
         std::fprintf(stderr, "[chosen] %u buckets, largest %llu, %zu + %zu query tiles, %llu tile pairs\n",
                      C, (unsigned long long)maxb, jb[0].size(), jb[1].size(),
                      (unsigned long long)tile_pairs);
+    kg_sec.reset();
     S_.ms_leaves = tm.stop();
 
     // ── 3. tensor-core shortlist ──
@@ -633,7 +643,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.err = c->d_err;
             a.trace = tbuf;
             {
-                KGScope kg(c, PQ_KG_JOIN_COUNT);
+                KGScope kg(c, PQ_KG_TILES);
                 ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "ivf tiles");
             }
             if (pass == 0) {  // seed the other probes with the primary shortlist's R-th best
@@ -670,7 +680,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
     ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
     {
-        KGScope kg(c, PQ_KG_REPLAY);
+        KGScope kg(c, PQ_KG_RERANK);
         if (d == 50)
             k_rerank<50><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
                                                        si, perm, ridx, rdist, c->d_acc);
@@ -688,11 +698,11 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     k_list_to_heap<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(ridx, rdist, n, k, hidx, hdist,
                                                                 hflag); count_launch();
     const Resolved RR = resolve(n64, o);
-    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : 2;
+    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : 0;
     int rounds = 0;
     if (n > 1 && polish > 0)
         rounds = run_rounds(c, X, d, dp, n, k, int(RR.max_cand), o.seed, polish, RR.stop_at, hidx,
-                            hdist, hflag, perm, 3, nullptr);
+                            hdist, hflag, perm, 0, nullptr);
     uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
     uint32_t* eoff = c->get<uint32_t>("eoff", n);
     launch_extract_count(hidx, n, k, ecnt, st);
@@ -703,8 +713,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     ck(cudaStreamSynchronize(st), "extract");
     S_.ms_extract = tm.stop();
     S_.ms_total = tot.stop();
-    S_.changed[0] = fixes;  // FP64 boundary resolutions of the shortlist re-rank
-    S_.rounds_run = 3 + rounds;  // slots 0..2: shortlist stats; then one per NN-Descent round
+    S_.shortlist[6] = fixes;
+    S_.rounds_run = rounds;  // polish rounds after the shortlist
     S_.n_trees = int32_t(C);
     S_.max_candidates = uint64_t(P) << 32 | uint64_t(Ssh);
     S_.launches = g_launches - launches0;

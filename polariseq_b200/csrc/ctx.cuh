@@ -174,6 +174,10 @@ inline void kg_collect(pq_ctx* c) {
     c->kg_pending.clear();
 }
 
+// The caller's row-major n x d f32 embedding (host or device) as padded rows
+// X[n][dp] in the context's workspace, 16-byte aligned and zero padded (api.cu).
+float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp);
+
 // NN-Descent rounds on heaps in place (api.cu).
 int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m, uint64_t seed,
                uint64_t n_iters, uint64_t stop_at, uint32_t* hidx, float* hdist, uint8_t* hflag,
