@@ -42,7 +42,7 @@ __global__ void k_sample_rows(const float* __restrict__ X, int dp, uint32_t n, u
     out[t] = X[i * dp + c];
 }
 
-// Column sums of the padded rows (for the global mean used as BF16 centre).
+// Column sums of padded rows (for the mean used as the centroid search's BF16 centre).
 __global__ void k_col_sum(const float* __restrict__ X, uint32_t n, int dp, float* sums) {
     const int j = threadIdx.x;
     if (j >= dp) return;
@@ -66,15 +66,40 @@ __global__ void k_kmeans_accumulate(const float* __restrict__ xs, uint32_t ns, i
     for (int j = 0; j < d; ++j) atomicAdd(&sums[size_t(b) * dp + j], xs[size_t(i) * dp + j]);
 }
 
-// Query-entry keys and values (cell * P + rank) from the probes: primary
-// entries (rank 0) sort first by bucket (key = bucket), the others after them
-// (key = C + bucket), so the primary probes can run as a first pass.
+// Query-entry keys and values (cell * P + rank) from the probes.  Primary
+// entries (rank 0) sort first, by (bucket, second-nearest centroid) exactly
+// as the candidates do, so that a primary job's own cells form its first
+// candidate tile; the others follow by (probe bucket, the cell's primary
+// bucket), so that a job's queries come from one neighbouring bucket and meet
+// the candidates on that side of the probe bucket first.
 __global__ void k_entry_keys(const uint32_t* __restrict__ probes, size_t ne, int P, uint32_t C,
                              uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= ne) return;
-    keys[e] = probes[e] + (e % P != 0 ? C : 0u);
+    const size_t i = e / P;
+    const uint32_t r = uint32_t(e - i * P);
+    const uint32_t a = probes[i * P];
+    if (r == 0)
+        keys[e] = a * C + (P > 1 ? probes[i * P + 1] : 0u);
+    else
+        keys[e] = (C + probes[e]) * C + a;
     vals[e] = e;
+}
+
+// First candidate tile of each job of the non-primary pass: where the probe
+// bucket's candidates whose second-nearest centroid is the job's primary
+// bucket begin (candidate key = bucket * C + second-nearest centroid).
+__global__ void k_job_tstart(const uint32_t* __restrict__ job_bucket,
+                             const uint32_t* __restrict__ job_qstart, uint32_t njobs,
+                             const uint32_t* __restrict__ ekeys, uint32_t C,
+                             const uint32_t* __restrict__ c_off,
+                             const uint32_t* __restrict__ pair_off,
+                             uint32_t* __restrict__ tstart) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= njobs) return;
+    const uint32_t b = job_bucket[j];
+    const uint32_t a = ekeys[job_qstart[j]] % C;
+    tstart[j] = (pair_off[size_t(b) * C + a] - c_off[b]) / 256u;
 }
 
 // Seed thresholds of the non-primary entries: the R-th best approximate
@@ -174,27 +199,29 @@ __global__ void k_merge_runs(const float* __restrict__ rd, const uint32_t* __res
     }
 }
 
-__global__ void k_primary_keys(const uint32_t* __restrict__ probes, int P, uint32_t n,
+// Candidate keys: (primary bucket, second-nearest centroid), so that cells of
+// a bucket lying towards the same neighbour sit together.
+__global__ void k_primary_keys(const uint32_t* __restrict__ probes, int P, uint32_t n, uint32_t C,
                                uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    keys[i] = probes[size_t(i) * P];
+    keys[i] = probes[size_t(i) * P] * C + (P > 1 ? probes[size_t(i) * P + 1] : 0u);
     vals[i] = i;
 }
 
-// Offsets of every key value in a sorted key array: off[v] = first position
-// with key >= v, for v in [0, nkeys]; each off entry is written exactly once
-// (by the position where the key steps past it, or by the last position).
-__global__ void k_key_bounds(const uint32_t* __restrict__ keys, size_t ne, uint32_t nkeys,
-                             uint32_t* __restrict__ off) {
+// Offsets of every value v = key / div in a sorted key array: off[v] = first
+// position with key / div >= v, for v in [0, nv]; each off entry is written
+// exactly once (by the position where the value steps past it, or the last).
+__global__ void k_key_bounds(const uint32_t* __restrict__ keys, size_t ne, uint32_t div,
+                             uint32_t nv, uint32_t* __restrict__ off) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e > ne) return;
-    const uint32_t lo = e == 0 ? 0u : keys[e - 1] + 1;
-    const uint32_t hi = e == ne ? nkeys : keys[e];
+    const uint32_t lo = e == 0 ? 0u : keys[e - 1] / div + 1;
+    const uint32_t hi = e == ne ? nv : keys[e] / div;
     for (uint32_t v = lo; v <= hi; ++v) off[v] = uint32_t(e);
 }
 
-__global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n,
+__global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n, uint32_t C,
                               const uint32_t* __restrict__ keys, uint32_t* __restrict__ perm,
                               uint32_t* __restrict__ pos_of, uint32_t* __restrict__ cbucket) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
@@ -202,7 +229,7 @@ __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n,
     const uint32_t i = uint32_t(vals[p]);
     perm[p] = i;
     pos_of[i] = p;
-    cbucket[p] = keys[p];
+    cbucket[p] = keys[p] / C;
 }
 
 __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t* __restrict__ keys,
@@ -214,8 +241,8 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
     if (e >= ne) return;
     const uint64_t v = vals[e];
     const uint32_t i = uint32_t(v / P), r = uint32_t(v % P);
-    const uint32_t key = keys[e];
-    const uint32_t b = key >= C ? key - C : key;
+    const uint32_t kb = keys[e] / C;
+    const uint32_t b = kb >= C ? kb - C : kb;
     qpoint[e] = i;
     qbucket[e] = b;
     qself[e] = b == probes[size_t(i) * P] ? pos_of[i] : 0xFFFFFFFFu;
@@ -436,6 +463,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : 14u, std::min(C, 16u)));
     const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
     if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};
+    if (uint64_t(C) * C * 2 >= 0xFFFFFFFFull)
+        throw DeviceError{"the tensor-core form supports n_obs below 190M"};
     int num_sms = 148;
     cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, c->device);
     float* xs = c->get<float>("km_sample", size_t(ns) * dp);
@@ -446,12 +475,12 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     ck(cudaMemsetAsync(zeros, 0, size_t(std::max<uint32_t>(C, n)) * 4, st), "zeros");
     uint32_t* noself = c->get<uint32_t>("noself", n);
     ck(cudaMemsetAsync(noself, 0xFF, size_t(n) * 4, st), "noself");
-    // global mean: the BF16 centre of the centroid search
+    k_sample_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, n, ns, xs); count_launch();
+    // the sample's mean: the BF16 centre of the centroid search
     float* mean = c->get<float>("mean", dp);
     ck(cudaMemsetAsync(mean, 0, dp * 4, st), "mean");
-    k_col_sum<<<512, 64 * ((dp + 63) / 64), 0, st>>>(X, n, dp, mean); count_launch();
-    k_scale<<<1, 128, 0, st>>>(mean, dp, 1.0f / float(n)); count_launch();
-    k_sample_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, n, ns, xs); count_launch();
+    k_col_sum<<<1024, 64 * ((dp + 63) / 64), 0, st>>>(xs, ns, dp, mean); count_launch();
+    k_scale<<<1, 128, 0, st>>>(mean, dp, 1.0f / float(ns)); count_launch();
     k_sample_rows<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(xs, dp, ns, C, cent); count_launch();
     __nv_bfloat16* xsb = c->get<__nv_bfloat16>("km_sample_bf16", size_t(ns) * 64);
     float* xsn = c->get<float>("km_sample_norm", ns);
@@ -490,12 +519,13 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         a.c_off = offs;
         a.qnorm = qnorm;
         a.qself = noself;
-        a.S = 16;
+        const int sr = s_out == 1 ? 1 : 16;  // per column half: the nearest, or up to 16
+        a.S = sr;
         a.out_d = c->get<float>("arun_d", size_t(nq) * 2 * 16);
         a.out_i = c->get<uint32_t>("arun_i", size_t(nq) * 2 * 16);
         a.err = c->d_err;
         ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "centroid tiles");
-        k_merge_runs<<<blocks(nq, 256), 256, 0, st>>>(a.out_d, a.out_i, nq, 16, s_out, od, oi); count_launch();
+        k_merge_runs<<<blocks(nq, 256), 256, 0, st>>>(a.out_d, a.out_i, nq, sr, s_out, od, oi); count_launch();
         ck(cudaStreamSynchronize(st), "centroid tiles");  // the host job arrays are reused
     };
     ck(cudaMemsetAsync(c->d_err, 0, 4, st), "err");
@@ -536,21 +566,24 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint64_t* cvals = c->get<uint64_t>("cvals_c", n);
     uint32_t* ckeys2 = c->get<uint32_t>("ckeys_c2", n);
     uint64_t* cvals2 = c->get<uint64_t>("cvals_c2", n);
-    k_primary_keys<<<blocks(n, 256), 256, 0, st>>>(probes, P, n, ckeys, cvals); count_launch();
-    ck(radix_sort_pairs(ckeys, cvals, ckeys2, cvals2, n, key_bits(C),
+    k_primary_keys<<<blocks(n, 256), 256, 0, st>>>(probes, P, n, C, ckeys, cvals); count_launch();
+    ck(radix_sort_pairs(ckeys, cvals, ckeys2, cvals2, n, key_bits(uint64_t(C) * C - 1),
                         c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
        "sort cand");
     uint32_t* c_off = c->get<uint32_t>("c_off", C + 1);
-    k_key_bounds<<<blocks(size_t(n) + 1, 256), 256, 0, st>>>(ckeys, n, C, c_off); count_launch();
+    k_key_bounds<<<blocks(size_t(n) + 1, 256), 256, 0, st>>>(ckeys, n, C, C, c_off); count_launch();
+    // where each (bucket, second-nearest centroid) group of candidates begins
+    uint32_t* pair_off = c->get<uint32_t>("pair_off", size_t(C) * C + 1);
+    k_key_bounds<<<blocks(size_t(n) + 1, 256), 256, 0, st>>>(ckeys, n, 1, C * C, pair_off); count_launch();
     uint32_t* perm = c->get<uint32_t>("cperm", n);
     uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
     uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
-    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, ckeys, perm, pos_of, cbucket); count_launch();
+    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, pos_of, cbucket); count_launch();
     __nv_bfloat16* xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
     float* xcn = c->get<float>("xc_norm", n);
     k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, 2, xc, xcn); count_launch();
     // query entries grouped by probe bucket (stable: cell order within a bucket)
-    ck(radix_sort_pairs(ekeys, evals, ekeys2, evals2, ne, key_bits(2 * C),
+    ck(radix_sort_pairs(ekeys, evals, ekeys2, evals2, ne, key_bits(2 * uint64_t(C) * C - 1),
                         c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
        "sort entries");
     uint32_t* qpoint = c->get<uint32_t>("qpoint", ne);
@@ -560,7 +593,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     k_entry_layout<<<blocks(ne, 256), 256, 0, st>>>(evals, ekeys, ne, P, C, probes, pos_of,
                                                      qpoint, qbucket, qself, entry_of); count_launch();
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
-    k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, 2 * C, q_off); count_launch();
+    k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, C, 2 * C, q_off); count_launch();
     __nv_bfloat16* qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
     float* qbn = c->get<float>("q_norm", ne);
     k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, 1, qb, qbn); count_launch();
@@ -571,7 +604,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     std::vector<uint32_t> hc(C + 1);
     ck(cudaMemcpy(hc.data(), c_off, size_t(C + 1) * 4, cudaMemcpyDeviceToHost), "c_off");
     // jobs: pass 0 = primary entries (keys [0, C)), pass 1 = the others
-    std::vector<uint32_t> jb[2], jq[2], je[2];
+    std::vector<uint32_t> jb[2], jq[2], je[2], jt0;
     uint64_t tile_pairs = 0, maxb = 0, cells = 0, pass_pairs[2] = {0, 0};
     for (int pass = 0; pass < 2; ++pass)
         for (uint32_t b = 0; b < C; ++b) {
@@ -582,6 +615,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                 jb[pass].push_back(b);
                 jq[pass].push_back(q0);
                 je[pass].push_back(std::min(q0 + 128, hq[key + 1]));
+                // a primary job's own cells are its candidates at the same offset
+                if (pass == 0) jt0.push_back((q0 - hq[key]) / 256);
                 tile_pairs += nct;
                 pass_pairs[pass] += nct;
                 cells += uint64_t(std::min(q0 + 128, hq[key + 1]) - q0) * (hc[b + 1] - hc[b]);
@@ -618,7 +653,14 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             tbuf = c->get<unsigned long long>("ivf_trace", IVF_TRACE_N);
             ck(cudaMemsetAsync(tbuf, 0, IVF_TRACE_N * 8, st), "trace");
         }
-        const int R0 = std::min(Sout, std::min(64, std::max(2 * k, k + 1)));
+        // the seed: the (k+2)-th best of the primary shortlist.  A candidate of
+        // another bucket can reach the cell's k best only by beating it; the two
+        // extra places absorb the BF16 ranking error (recall@15 at 4M matches the
+        // 2k-th seed to four digits, with 16% fewer tile-kernel cycles)
+        const int R0 = std::min(Sout, k + 2);
+        // the primary pass starts without a bound and admits often: drain at
+        // half a buffer so that its bound tightens sooner
+        const int drain_at0 = 16;
         for (int pass = 0; pass < 2; ++pass) {
             const uint32_t nj = uint32_t(jb[pass].size());
             if (nj == 0) continue;
@@ -628,16 +670,27 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             ck(cudaMemcpyAsync(djb, jb[pass].data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
             ck(cudaMemcpyAsync(djq, jq[pass].data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
             ck(cudaMemcpyAsync(dje, je[pass].data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
+            uint32_t* djt = c->get<uint32_t>(pass ? "job_t1" : "job_t0", nj);
+            if (pass == 0) {
+                ck(cudaMemcpyAsync(djt, jt0.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st),
+                   "jobs");
+            } else {
+                k_job_tstart<<<blocks(nj, 256), 256, 0, st>>>(djb, djq, nj, ekeys, C, c_off,
+                                                              pair_off, djt);
+                count_launch();
+            }
             IvfTileArgs a{};
             a.job_bucket = djb;
             a.job_qstart = djq;
             a.job_qend = dje;
+            a.job_tstart = djt;
             a.njobs = nj;
             a.c_off = c_off;
             a.qnorm = qbn;
             a.qthr = pass ? qthr : nullptr;
             a.qself = qself;
             a.S = Ssh;
+            a.drain_at = pass == 0 ? drain_at0 : 0;
             a.out_d = sd;
             a.out_i = si;
             a.err = c->d_err;
@@ -657,11 +710,13 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                 std::fprintf(stderr,
                              "[chosen] pass %d tiles block 0: jobs %llu tiles %llu drains %llu | "
                              "cycles epi-wait %llu epi-work %llu epi-end %llu mma-wait-c %llu "
-                             "mma-wait-t %llu tma-wait %llu total %llu\n",
+                             "mma-wait-t %llu tma-wait %llu total %llu | warp 0: slow chunks %llu "
+                             "admits %llu union bits %llu end-drain cycles %llu\n",
                              pass, h[IVF_T_JOBS], h[IVF_T_TILES], h[IVF_T_DRAINS],
                              h[IVF_T_EPI_WAIT], h[IVF_T_EPI_WORK], h[IVF_T_EPI_END],
                              h[IVF_T_MMA_WAIT_C], h[IVF_T_MMA_WAIT_T], h[IVF_T_TMA_WAIT],
-                             h[IVF_T_TOTAL]);
+                             h[IVF_T_TOTAL], h[IVF_T_SLOW], h[IVF_T_ADMITS], h[IVF_T_WMBITS],
+                             h[IVF_T_END_DRAIN]);
             }
         }
     }

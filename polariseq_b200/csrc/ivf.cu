@@ -198,6 +198,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 const uint32_t b = a.job_bucket[job], qs = a.job_qstart[job];
                 const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
                 const uint32_t nct = (ce - cs + TCN - 1) / TCN;
+                // tiles run from the job's start tile, wrapping around
+                const uint32_t t0 = (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
                 if (nct == 0) continue;
                 const int qsd = int(qi % QST);
                 long long c0 = clock64();
@@ -218,7 +220,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                     }
                     c_wait += clock64() - c0;
                     tc::mbar_expect_tx(&B.c_full[s], TCN * ROWB);
-                    tc::tma_load_2d(sC + s * TCN * ROWB, &tmC, &B.c_full[s], 0, int(cs + t * TCN));
+                    const uint32_t tt = t0 + t >= nct ? t0 + t - nct : t0 + t;
+                    tc::tma_load_2d(sC + s * TCN * ROWB, &tmC, &B.c_full[s], 0, int(cs + tt * TCN));
                     ++ci;
                 }
             }
@@ -301,14 +304,21 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
         float* bd = bdall + size_t(g) * BUF * TQ + row;
         uint32_t* bi = biall + size_t(g) * BUF * TQ + row;
         const bool t0 = tracing && tid == 0;
+        // drain once some lane's buffer would pass this fill: early drains
+        // tighten the admission bound sooner where admissions are frequent
+        const uint32_t drain_at = a.drain_at > 0 && a.drain_at < BUF ? uint32_t(a.drain_at)
+                                                                     : uint32_t(BUF);
         long long c_wait = 0, c_work = 0, c_end = 0;
-        unsigned long long drains = 0, jobs = 0;
+        unsigned long long drains = 0, jobs = 0, slow = 0, admits = 0, wmbits = 0;
+        long long c_end_drain = 0;
         uint32_t ti = 0;
         for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
             const uint32_t b = a.job_bucket[job];
             const uint32_t qs = a.job_qstart[job], qe = a.job_qend[job];
             const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
             const uint32_t nct = (ce - cs + TCN - 1) / TCN;
+            // tiles run from the job's start tile, wrapping around
+            const uint32_t t0 = (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
             const uint32_t entry = qs + row;
             const bool valid = entry < qe;
             // an invalid row's infinite |q|^2 makes its bound +inf or NaN: it
@@ -319,6 +329,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             float thr = thr0;
             float ath = (qn - thr) * 0.5f;
             int cnt = 0;
+            bool heaped = false;  // the heap holds entries (a drain moved some there)
 #pragma unroll 4
             for (int j = 0; j < S; ++j) {
                 hd[j * TQ] = __int_as_float(0x7f800000);
@@ -326,6 +337,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             }
             // drain this lane's append buffer into its heap
             auto drain = [&]() {
+                heaped = heaped || cnt > 0;
                 for (int t = 0; t < cnt; ++t) {
                     const float v = bd[t * TQ];
                     if (v < thr) thr = fminf(thr0, shortlist_insert(hd, hi, S, v, bi[t * TQ]));
@@ -343,8 +355,9 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 tc::tc_fence_after();
                 const uint32_t tcol = taddr + lane_base + uint32_t(tb * TCN + g * CPG);
                 // columns of this slice that belong to the bucket
-                const int lim = int(ce) - int(cs + t * TCN + g * CPG);
-                const uint32_t cbase = cs + t * TCN + g * CPG;
+                const uint32_t tt = t0 + t >= nct ? t0 + t - nct : t0 + t;
+                const int lim = int(ce) - int(cs + tt * TCN + g * CPG);
+                const uint32_t cbase = cs + tt * TCN + g * CPG;
                 // fast filter: the slice's four 32-column chunks from registers,
                 // one max and one vote each; flags the chunks some row admits
                 uint32_t slowq = 0;
@@ -380,11 +393,19 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
                         if (q * 32 + j < lim && __uint_as_float(x[j]) > ath) lm |= 1u << j;
-                    if (__reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > uint32_t(BUF)) {
+                    if (__reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > drain_at) {
                         ++drains;
                         drain();  // cnt = 0, and at most 32 admissions follow
                     }
                     const uint32_t wm = __reduce_or_sync(FULL, lm);  // the warp's union
+                    if (t0) {
+                        ++slow;
+                        wmbits += __popc(wm);
+                    }
+                    if (tracing) {
+                        const uint32_t na = __reduce_add_sync(FULL, uint32_t(__popc(lm)));
+                        if (t0) admits += na;
+                    }
                     const uint32_t cb0 = cbase + q * 32;
 #pragma unroll
                     for (int j = 0; j < 32; ++j) {
@@ -411,24 +432,39 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 *abort_flag = 1;
                 break;
             }
-            // job end: drain, sort the heap in registers, write one run of S
+            // job end: the entries (the buffer alone when it never spilled into
+            // the heap and fits the run, else the heap after a drain) sorted in
+            // registers, written as one ascending run of S
             long long c3 = t0 ? clock64() : 0;
-            drain();
+            const bool direct = !heaped && cnt <= S;
+            if (!direct) drain();
+            if (t0) c_end_drain += clock64() - c3;
             if (valid) {
                 float kv[S];
                 uint32_t ki[S];
+                const float* sd_ = direct ? bd : hd;
+                const uint32_t* si_ = direct ? bi : hi;
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
-                    kv[j] = hd[j * TQ];
-                    ki[j] = hi[j * TQ];
+                    const bool live = !direct || j < cnt;
+                    kv[j] = live ? sd_[j * TQ] : __int_as_float(0x7f800000);
+                    ki[j] = live ? si_[j * TQ] : 0xFFFFFFFFu;
                 }
                 sort_pairs<S>(kv, ki);
-                float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
-                uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
+                if constexpr (S % 4 == 0) {
+                    float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
+                    uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
 #pragma unroll
-                for (int j = 0; j < S / 4; ++j) {
-                    od[j] = make_float4(kv[4 * j], kv[4 * j + 1], kv[4 * j + 2], kv[4 * j + 3]);
-                    oi[j] = make_uint4(ki[4 * j], ki[4 * j + 1], ki[4 * j + 2], ki[4 * j + 3]);
+                    for (int j = 0; j < S / 4; ++j) {
+                        od[j] = make_float4(kv[4 * j], kv[4 * j + 1], kv[4 * j + 2], kv[4 * j + 3]);
+                        oi[j] = make_uint4(ki[4 * j], ki[4 * j + 1], ki[4 * j + 2], ki[4 * j + 3]);
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < S; ++j) {
+                        a.out_d[(size_t(entry) * NG + g) * S + j] = kv[j];
+                        a.out_i[(size_t(entry) * NG + g) * S + j] = ki[j];
+                    }
                 }
             }
             ++jobs;
@@ -440,6 +476,10 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             a.trace[IVF_T_EPI_END] = (unsigned long long)c_end;
             a.trace[IVF_T_DRAINS] = drains;
             a.trace[IVF_T_JOBS] = jobs;
+            a.trace[IVF_T_SLOW] = slow;
+            a.trace[IVF_T_ADMITS] = admits;
+            a.trace[IVF_T_WMBITS] = wmbits;
+            a.trace[IVF_T_END_DRAIN] = (unsigned long long)c_end_drain;
         }
     }
     __syncthreads();
@@ -509,6 +549,7 @@ int ivf_shortlist(int want) { return want <= 16 ? 16 : (want <= 32 ? 32 : 0); }
 cudaError_t launch_ivf_tiles(const CUtensorMap& tmQ, const CUtensorMap& tmC,
                              const IvfTileArgs& a, int grid, cudaStream_t st) {
     if (a.njobs == 0) return cudaSuccess;
+    if (a.S == 1) return launch_s<1>(tmQ, tmC, a, grid, st);
     if (a.S == 16) return launch_s<16>(tmQ, tmC, a, grid, st);
     if (a.S == 32) return launch_s<32>(tmQ, tmC, a, grid, st);
     return cudaErrorInvalidValue;

@@ -16,12 +16,14 @@ struct IvfTileArgs {
     const uint32_t* job_bucket;  // the job's candidate bucket
     const uint32_t* job_qstart;  // the job's query entries [qstart, qend)
     const uint32_t* job_qend;
+    const uint32_t* job_tstart;  // optional: the candidate tile each job starts from
     uint32_t njobs;
     const uint32_t* c_off;   // buckets + 1
     const float* qnorm;      // per query entry: |q~|^2 of its BF16 row
     const float* qthr;       // optional per query entry: initial admission bound
     const uint32_t* qself;   // per query entry: its own candidate position, or ~0
-    int S;                   // shortlist length per entry and column half: 16 or 32
+    int S;                   // shortlist length per entry and column half: 1, 16 or 32
+    int drain_at;            // buffer fill that triggers a drain into the heap (0: full)
     float* out_d;            // entries x (ivf_groups() x S): ascending runs of S
     uint32_t* out_i;         // the candidate positions (~0 = none)
     int* err;
@@ -30,7 +32,8 @@ struct IvfTileArgs {
 
 enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT_C = 3,
        IVF_T_MMA_WAIT_T = 4, IVF_T_TMA_WAIT = 5, IVF_T_TILES = 6, IVF_T_DRAINS = 7,
-       IVF_T_TOTAL = 8, IVF_T_JOBS = 9, IVF_TRACE_N = 10 };
+       IVF_T_TOTAL = 8, IVF_T_JOBS = 9, IVF_T_SLOW = 10, IVF_T_ADMITS = 11, IVF_T_WMBITS = 12,
+       IVF_T_END_DRAIN = 13, IVF_TRACE_N = 16 };
 
 bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
 // Runs of one entry's output row.
