@@ -310,42 +310,86 @@ __global__ void __launch_bounds__(128) k_rerank(
     __shared__ uint32_t band_i[4][64];
     __shared__ double band_d[4][64];
     __shared__ float band_f[4][64];
+    __shared__ uint64_t band_key[4][64];
     const uint32_t wg = blockIdx.x * 4 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     if (wg >= n) return;
     const uint32_t i = perm[wg];
-    // 1. merge of the ascending runs (lane L < P * NR owns run L % NR of probe
-    //    L / NR; runs are RS long, an entry's NR runs RS * NR apart)
+    // 1. the R best approximate candidates of the shortlist runs (lane L <
+    //    P * NR owns run L % NR of probe L / NR; runs are RS long, ascending,
+    //    an entry's NR runs RS * NR apart).  Each lane loads its run at once;
+    //    the finite entries (a prefix of each run) are gathered into shared
+    //    memory and sorted as (distance bits, position) keys — 64 at most,
+    //    else the runs are merged head by head.
     const int NR = SO / RS;
+    const bool owner = lane < P * NR;
     size_t base = 0;
-    uint32_t head = 0;
-    if (lane < P * NR)
-        base = size_t(entry_of[size_t(i) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
+    if (owner) base = size_t(entry_of[size_t(i) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
     uint32_t cand[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
-    for (int t = 0; t < R; ++t) {
-        float v = __int_as_float(0x7f800000);
-        uint32_t id = 0xFFFFFFFFu;
-        if (lane < P * NR && head < uint32_t(RS)) {
-            v = sd[base + head];
-            id = si[base + head];
+    float rv[32];
+    uint32_t ri[32];
+    int fin = 0;
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+        rv[j] = __int_as_float(0x7f800000);
+        ri[j] = 0xFFFFFFFFu;
+        if (j < RS && owner) {
+            rv[j] = sd[base + j];
+            ri[j] = si[base + j];
         }
-        // warp argmin by (value, candidate)
-        float bv = v;
-        uint32_t bid = id;
-        int bl = lane;
-        for (int o = 16; o > 0; o >>= 1) {
-            const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
-            const uint32_t oid = __shfl_xor_sync(0xFFFFFFFFu, bid, o);
-            const int ol = __shfl_xor_sync(0xFFFFFFFFu, bl, o);
-            if (ov < bv || (ov == bv && oid < bid)) {
-                bv = ov;
-                bid = oid;
-                bl = ol;
+        fin += (ri[j] != 0xFFFFFFFFu && rv[j] < __int_as_float(0x7f800000)) ? 1 : 0;
+    }
+    int off = fin;  // inclusive prefix sum of the finite counts
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const int t = __shfl_up_sync(0xFFFFFFFFu, off, o);
+        if (lane >= o) off += t;
+    }
+    const int total = __shfl_sync(0xFFFFFFFFu, off, 31);
+    off -= fin;
+    if (total <= 64) {
+        uint64_t* slot = band_key[w];
+        slot[lane] = ~0ull;
+        slot[lane + 32] = ~0ull;
+        __syncwarp();
+#pragma unroll
+        for (int j = 0; j < 32; ++j)
+            if (j < fin)
+                slot[off + j] = (uint64_t(__float_as_uint(fmaxf(rv[j], 0.0f))) << 32) | ri[j];
+        __syncwarp();
+        uint64_t key[2] = {slot[lane], slot[lane + 32]};
+        __syncwarp();
+        warp_sort64(key);
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+            if (lane + 32 * h < R && key[h] != ~0ull) cand[h] = uint32_t(key[h]);
+    } else {
+        uint32_t head = 0;
+        for (int t = 0; t < R; ++t) {
+            float v = __int_as_float(0x7f800000);
+            uint32_t id = 0xFFFFFFFFu;
+            if (owner && head < uint32_t(RS)) {
+                v = sd[base + head];
+                id = si[base + head];
             }
+            // warp argmin by (value, candidate)
+            float bv = v;
+            uint32_t bid = id;
+            int bl = lane;
+            for (int o = 16; o > 0; o >>= 1) {
+                const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
+                const uint32_t oid = __shfl_xor_sync(0xFFFFFFFFu, bid, o);
+                const int ol = __shfl_xor_sync(0xFFFFFFFFu, bl, o);
+                if (ov < bv || (ov == bv && oid < bid)) {
+                    bv = ov;
+                    bid = oid;
+                    bl = ol;
+                }
+            }
+            if (bid == 0xFFFFFFFFu) break;  // every list exhausted
+            if (lane == bl) ++head;
+            if ((t & 31) == lane) cand[t >> 5] = bid;
         }
-        if (bid == 0xFFFFFFFFu) break;  // every list exhausted
-        if (lane == bl) ++head;
-        if ((t & 31) == lane) cand[t >> 5] = bid;
     }
     // 2. exact FP32 distances (reference order) of this lane's candidates
     const float* xi = X + size_t(i) * dp;

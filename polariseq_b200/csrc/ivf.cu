@@ -85,6 +85,21 @@ __device__ __forceinline__ float max32(const float (&v)[32]) {
     return fmaxf(max3f(a, b, c), d);
 }
 
+// x[j] for a per-lane j in [0, 32): a five-level select tree over the
+// registers (no local-memory indexing).
+__device__ __forceinline__ uint32_t select32(const uint32_t (&x)[32], int j) {
+    uint32_t a[16], b[8], c[4], d[2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) a[i] = (j & 16) ? x[i + 16] : x[i];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) b[i] = (j & 8) ? a[i + 8] : a[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) c[i] = (j & 4) ? b[i + 4] : b[i];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) d[i] = (j & 2) ? c[i + 2] : c[i];
+    return (j & 1) ? d[1] : d[0];
+}
+
 // Replace the root of a max-heap of S shortlist entries (one thread's column of
 // a transposed shared-memory tile, entries TQ apart) and sift down; returns
 // the new root (the shortlist's current worst).
@@ -358,65 +373,60 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 const uint32_t tt = t0 + t >= nct ? t0 + t - nct : t0 + t;
                 const int lim = int(ce) - int(cs + tt * TCN + g * CPG);
                 const uint32_t cbase = cs + tt * TCN + g * CPG;
-                // fast filter: the slice's four 32-column chunks from registers,
-                // one max and one vote each; flags the chunks some row admits
-                uint32_t slowq = 0;
-                {
-                    uint32_t r[CPG / 32][32];
-#pragma unroll
-                    for (int q = 0; q < CPG / 32; ++q) tc::tmem_ld32(tcol + uint32_t(q * 32), r[q]);
-                    tc::tmem_ld_wait();
-#pragma unroll
-                    for (int q = 0; q < CPG / 32; ++q) {
-                        float v[32];
-#pragma unroll
-                        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[q][j]);
-                        if (lim < (q + 1) * 32) {
-#pragma unroll
-                            for (int j = 0; j < 32; ++j)
-                                if (q * 32 + j >= lim) v[j] = __int_as_float(0xff800000);
-                        }
-                        if (__any_sync(FULL, max32(v) > ath)) slowq |= 1u << q;
-                    }
-                }
+                // the slice's four 32-column chunks from registers: one max and
+                // one vote each; a chunk some row admits is handled on the spot
                 long long c1 = t0 ? clock64() : 0;
-                // rare: one compact copy of the admission code, the flagged
-                // chunks re-read from TMEM (the buffer is released after this)
-#pragma unroll 1
-                while (slowq) {
-                    const int q = __ffs(slowq) - 1;
-                    slowq &= slowq - 1;
-                    uint32_t x[32];
-                    tc::tmem_ld32(tcol + uint32_t(q * 32), x);
-                    tc::tmem_ld_wait();
+                // two chunks in registers at a time (64 registers), so that a
+                // flagged chunk is handled from registers without spills
+#pragma unroll
+                for (int q2 = 0; q2 < CPG / 32; q2 += 2) {
+                uint32_t r[2][32];
+                tc::tmem_ld32(tcol + uint32_t(q2 * 32), r[0]);
+                tc::tmem_ld32(tcol + uint32_t(q2 * 32 + 32), r[1]);
+                tc::tmem_ld_wait();
+#pragma unroll
+                for (int qq = 0; qq < 2; ++qq) {
+                    const int q = q2 + qq;
+                    float v[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[qq][j]);
+                    if (lim < (q + 1) * 32) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            if (q * 32 + j >= lim) v[j] = __int_as_float(0xff800000);
+                    }
+                    if (!__any_sync(FULL, max32(v) > ath)) continue;
                     uint32_t lm = 0;  // this lane's admitted columns
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
-                        if (q * 32 + j < lim && __uint_as_float(x[j]) > ath) lm |= 1u << j;
+                        if (v[j] > ath) lm |= 1u << j;
                     if (__reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > drain_at) {
                         ++drains;
                         drain();  // cnt = 0, and at most 32 admissions follow
                     }
-                    const uint32_t wm = __reduce_or_sync(FULL, lm);  // the warp's union
-                    if (t0) {
-                        ++slow;
-                        wmbits += __popc(wm);
-                    }
+                    if (t0) ++slow;
                     if (tracing) {
                         const uint32_t na = __reduce_add_sync(FULL, uint32_t(__popc(lm)));
-                        if (t0) admits += na;
+                        const uint32_t wm = __reduce_or_sync(FULL, lm);
+                        if (t0) {
+                            admits += na;
+                            wmbits += __popc(wm);
+                        }
                     }
+                    // each lane appends its own admitted columns, lowest first
                     const uint32_t cb0 = cbase + q * 32;
-#pragma unroll
-                    for (int j = 0; j < 32; ++j) {
-                        if (wm & (1u << j)) {
-                            if (((lm >> j) & 1u) && cb0 + j != qself) {
-                                bd[cnt * TQ] = fmaf(-2.0f, __uint_as_float(x[j]), qn);
+                    while (__any_sync(FULL, lm != 0)) {
+                        if (lm) {
+                            const int j = __ffs(lm) - 1;
+                            lm &= lm - 1;
+                            if (cb0 + j != qself) {
+                                bd[cnt * TQ] = fmaf(-2.0f, __uint_as_float(select32(r[qq], j)), qn);
                                 bi[cnt * TQ] = cb0 + j;
                                 ++cnt;
                             }
                         }
                     }
+                }
                 }
                 tc::tc_fence_before();
                 __syncwarp();
