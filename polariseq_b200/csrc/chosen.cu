@@ -461,6 +461,35 @@ __global__ void __launch_bounds__(128) k_rerank(
     }
 }
 
+// Entries of each ascending list (the EMPTY slots come last).
+__global__ void k_list_count(const uint32_t* __restrict__ li, uint32_t n, int k,
+                             uint32_t* __restrict__ cnt) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t c = 0;
+    for (int s = 0; s < k; ++s) c += li[size_t(i) * k + s] != PQ_EMPTY ? 1u : 0u;
+    cnt[i] = c;
+}
+
+// CSR rows straight from the ascending lists: Euclidean distances (sqrt).
+__global__ void k_list_extract(const uint32_t* __restrict__ li, const float* __restrict__ ld,
+                               uint32_t n, int k, const uint32_t* __restrict__ off,
+                               const uint32_t* __restrict__ cnt, uint32_t* __restrict__ indptr,
+                               uint32_t* __restrict__ indices, float* __restrict__ dists) {
+    const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= size_t(n) * k) return;
+    const size_t i = e / k;
+    const uint32_t s = uint32_t(e - i * k);
+    if (s < cnt[i]) {
+        indices[off[i] + s] = li[e];
+        dists[off[i] + s] = __fsqrt_rn(ld[e]);
+    }
+    if (s == 0) {
+        indptr[i + 1] = off[i] + cnt[i];
+        if (i == 0) indptr[0] = 0;
+    }
+}
+
 // Sorted (ascending) lists -> neighbour heaps: a descending array is a valid
 // max-heap; every entry starts new.
 __global__ void k_list_to_heap(const uint32_t* __restrict__ li, const float* __restrict__ ld,
@@ -791,22 +820,31 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     unsigned long long fixes = 0;
     ck(cudaMemcpyAsync(&fixes, c->d_acc, 8, cudaMemcpyDeviceToHost, st), "fixes");
     // ── 5. NN-Descent rounds from the shortlist lists, then the extract ──
-    uint32_t* hidx = c->get<uint32_t>("hidx", size_t(n) * k);
-    float* hdist = c->get<float>("hdist", size_t(n) * k);
-    uint8_t* hflag = c->get<uint8_t>("hflag", size_t(n) * k);
-    k_list_to_heap<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(ridx, rdist, n, k, hidx, hdist,
-                                                                hflag); count_launch();
     const Resolved RR = resolve(n64, o);
     const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : 0;
     int rounds = 0;
-    if (n > 1 && polish > 0)
-        rounds = run_rounds(c, X, d, dp, n, k, int(RR.max_cand), o.seed, polish, RR.stop_at, hidx,
-                            hdist, hflag, perm, 0, nullptr);
     uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
     uint32_t* eoff = c->get<uint32_t>("eoff", n);
-    launch_extract_count(hidx, n, k, ecnt, st);
-    ck(scan_exclusive_u32(ecnt, eoff, n, stemp, c->d_u64, st), "scan extract");
-    launch_extract(hidx, hdist, n, k, eoff, d_indptr, d_indices, d_dists, st);
+    if (n > 1 && polish > 0) {
+        uint32_t* hidx = c->get<uint32_t>("hidx", size_t(n) * k);
+        float* hdist = c->get<float>("hdist", size_t(n) * k);
+        uint8_t* hflag = c->get<uint8_t>("hflag", size_t(n) * k);
+        k_list_to_heap<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(ridx, rdist, n, k, hidx, hdist,
+                                                                    hflag); count_launch();
+        rounds = run_rounds(c, X, d, dp, n, k, int(RR.max_cand), o.seed, polish, RR.stop_at, hidx,
+                            hdist, hflag, perm, 0, nullptr);
+        launch_extract_count(hidx, n, k, ecnt, st);
+        ck(scan_exclusive_u32(ecnt, eoff, n, stemp, c->d_u64, st), "scan extract");
+        launch_extract(hidx, hdist, n, k, eoff, d_indptr, d_indices, d_dists, st);
+    } else {
+        // the re-ranked lists are already ascending with their entries first
+        KGScope kg(c, PQ_KG_EXTRACT);
+        k_list_count<<<blocks(n, 256), 256, 0, st>>>(ridx, n, k, ecnt); count_launch();
+        ck(scan_exclusive_u32(ecnt, eoff, n, stemp, c->d_u64, st), "scan extract");
+        k_list_extract<<<blocks(size_t(n) * k, 256), 256, 0, st>>>(ridx, rdist, n, k, eoff, ecnt,
+                                                                    d_indptr, d_indices, d_dists);
+        count_launch();
+    }
     uint64_t nnz = 0;
     ck(cudaMemcpyAsync(&nnz, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "nnz");
     ck(cudaStreamSynchronize(st), "extract");
