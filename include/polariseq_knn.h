@@ -172,6 +172,27 @@ int pq_neighbors_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_obs, u
                              uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
                              void* stream);
 
+/* Flags of pq_knn_batched_into_device. */
+enum { PQ_BATCH_AUTOTUNE = 1, PQ_BATCH_GRAPH = 2 };
+
+/* Batched exact kNN: every point's k_s nearest other points within its own
+ * sample, for n_samples samples of uneven size in ONE persistent,
+ * work-queued launch — the per-sample searches of doublet scoring
+ * (crates/polariseq-core/src/doublets.rs:544-650 knn_exact: exact, itself
+ * excluded, ties by index, ascending).  d_data holds all samples' rows back
+ * to back (row-major f32, n_dim <= 64); offsets (HOST, n_samples + 1, rows)
+ * delimit the samples; ks (HOST) gives each sample's k (1 <= k < its size,
+ * k <= 512).  Sample s's rows write k_s entries each, back to back from
+ * sum_{t<s} n_t * k_t: indices local to the sample, Euclidean distances.
+ * PQ_BATCH_AUTOTUNE re-times the tile shapes (otherwise the context's choice
+ * for this n_dim and k range is reused, timing them on first use);
+ * PQ_BATCH_GRAPH captures the launch in a CUDA graph and replays it.
+ * *shape_out (may be null) receives the tile shape used. */
+int pq_knn_batched_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_dim,
+                               uint32_t n_samples, const uint64_t* offsets, const uint32_t* ks,
+                               uint32_t* d_indices, float* d_dists, int32_t flags,
+                               int32_t* shape_out, void* stream);
+
 /* Allocation-free exact kNN.  No counterpart in the reference: it is an
  * addition of this library for callers that must not allocate device memory,
  * such as a host framework that owns the whole device budget through its own

@@ -29,7 +29,7 @@ from . import _lib
 
 __all__ = [
     "PanicException", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
-    "neighbors_dense",
+    "neighbors_dense", "knn_batched",
 ]
 
 
@@ -178,6 +178,28 @@ class Context:
             self._check_neighbors(rc)
         return int(nnz.value)
 
+    # -- batched exact kNN over many samples -------------------------------
+    def knn_batched_device(self, data, offsets: np.ndarray, ks: np.ndarray, indices, dists,
+                           autotune: bool = False, graph: bool = True, stream=None) -> int:
+        """All samples' rows back to back in `data` (float32 [N, d] CUDA
+        tensor); `offsets` (uint64 [S+1]) and `ks` (uint32 [S]) on the host;
+        `indices`/`dists` CUDA tensors of sum(n_s * k_s).  Returns the tile
+        shape used."""
+        offsets = np.ascontiguousarray(offsets, np.uint64)
+        ks = np.ascontiguousarray(ks, np.uint32)
+        flags = (_lib.PQ_BATCH_AUTOTUNE if autotune else 0) | (_lib.PQ_BATCH_GRAPH if graph else 0)
+        shape = C.c_int32(-1)
+        sp = None if stream is None else C.c_void_p(int(stream))
+        with self._lock:
+            rc = _lib.load().pq_knn_batched_into_device(
+                self._h, data.data_ptr(), int(data.shape[1]), int(ks.size), offsets.ctypes.data,
+                ks.ctypes.data, indices.data_ptr(), dists.data_ptr(), flags, C.byref(shape), sp)
+            if rc == _lib.PQ_EINVAL:
+                msg = _lib.load().pq_ctx_last_error(self._h).decode(errors="replace")
+                raise ValueError(f"knn_batched: {msg}")
+            self._check(rc, "knn_batched")
+        return int(shape.value)
+
     # -- parity probes (test hooks) ----------------------------------------
     def probe(self, data: np.ndarray, opts: _lib.NndOpts, stop_after: int) -> dict:
         data = np.ascontiguousarray(data, np.float32)
@@ -288,6 +310,40 @@ def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_
 
 
 METRICS = {"euclidean": _lib.PQ_METRIC_EUCLIDEAN, "cosine": _lib.PQ_METRIC_COSINE}
+
+
+def knn_batched(samples, ks, *, device: int = 0, autotune: bool = False, graph: bool = True):
+    """Exact kNN within each sample, all samples in one persistent launch
+    (the per-sample search of doublet scoring, doublets.rs:544-650).
+
+    ``samples``: list of float32 [n_s, d] arrays (d <= 64); ``ks``: the k of
+    each sample (1 <= k < n_s).  Returns a list of ``(indices, distances)``
+    pairs, [n_s, k_s] each: local indices of the k nearest other points,
+    ascending by (distance, index), Euclidean distances."""
+    import torch
+
+    arrs = [np.ascontiguousarray(a, np.float32) for a in samples]
+    if not arrs:
+        return []
+    d = arrs[0].shape[1]
+    sizes = np.array([a.shape[0] for a in arrs], np.uint64)
+    offsets = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    ks = np.asarray(ks, np.uint32)
+    total = int(np.sum(sizes * ks.astype(np.uint64)))
+    dev = torch.device("cuda", device)
+    x = torch.from_numpy(np.concatenate(arrs, 0)).to(dev)
+    oi = torch.empty(max(total, 1), dtype=torch.int32, device=dev)
+    od = torch.empty(max(total, 1), dtype=torch.float32, device=dev)
+    default_context(device).knn_batched_device(x, offsets, ks, oi, od, autotune=autotune,
+                                               graph=graph)
+    oi = oi.cpu().numpy().view(np.uint32)
+    od = od.cpu().numpy()
+    out, o = [], 0
+    for a, k in zip(arrs, ks):
+        m = a.shape[0] * int(k)
+        out.append((oi[o:o + m].reshape(a.shape[0], int(k)), od[o:o + m].reshape(a.shape[0], int(k))))
+        o += m
+    return out
 
 
 def neighbors_dense(embedding, n_neighbors, metric, *, device: int = 0) -> dict:

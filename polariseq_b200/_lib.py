@@ -16,13 +16,14 @@ PQ_OK, PQ_EINVAL, PQ_ENOMEM, PQ_EDEVICE, PQ_ETIMEOUT, PQ_ENOTSUP, PQ_ETOOBIG = r
 PQ_MODE_PLAIN, PQ_MODE_BF16, PQ_MODE_FP8 = 0, 1, 2
 PQ_INIT_RP, PQ_INIT_LEARNED = 0, 1
 PQ_METRIC_EUCLIDEAN, PQ_METRIC_COSINE = 0, 1
+PQ_BATCH_AUTOTUNE, PQ_BATCH_GRAPH = 1, 2
 
 # Every symbol include/polariseq_knn.h declares.
 EXPORTS = (
     "pq_nnd_opts_default", "pq_effective_k", "pq_ctx_create", "pq_ctx_destroy",
     "pq_ctx_last_error", "pq_ctx_stats", "pq_nndescent_into", "pq_nndescent_into_device",
     "pq_nndescent_probe", "pq_debug_tree", "pq_ctx_set_profiling", "pq_neighbors_into",
-    "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc",
+    "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc", "pq_knn_batched_into_device",
 )
 
 
@@ -131,5 +132,8 @@ def load(build_if_missing: bool = False):
         L.pq_neighbors_into_device_noalloc.argtypes = [P, U64, U64, U64, C.c_int32, P, P, P,
                                                         C.POINTER(U64), P]
         L.pq_neighbors_into_device_noalloc.restype = C.c_int
+        L.pq_knn_batched_into_device.argtypes = [P, P, U64, C.c_uint32, P, P, P, P, C.c_int32,
+                                                  C.POINTER(C.c_int32), P]
+        L.pq_knn_batched_into_device.restype = C.c_int
         _lib = L
         return L

@@ -9,6 +9,7 @@
 
 #include "ctx.cuh"
 #include "exact.cuh"
+#include "batched.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
@@ -766,6 +767,157 @@ int pq_neighbors_into_device(pq_ctx* c, const float* d_data, uint64_t n, uint64_
         ck(cudaStreamWaitEvent(user, ev, 0), "event");
         cudaEventDestroy(ev);
         *nnz_out = n * (kws - 1);
+        return PQ_OK;
+    });
+}
+
+int pq_knn_batched_into_device(pq_ctx* c, const float* d_data, uint64_t d, uint32_t n_samples,
+                               const uint64_t* offsets, const uint32_t* ks, uint32_t* d_indices,
+                               float* d_dists, int32_t flags, int32_t* shape_out, void* stream) {
+    if (!c) return PQ_EINVAL;
+    if (!d_data || !offsets || !ks || !d_indices || !d_dists)
+        return fail(c, PQ_EINVAL, "null buffer");
+    if (d == 0 || d > 64) return fail(c, PQ_ENOTSUP, "the batched search supports 1 <= n_dim <= 64");
+    if (n_samples == 0) return fail(c, PQ_EINVAL, "no samples");
+    if (offsets[0] != 0) return fail(c, PQ_EINVAL, "offsets[0] must be 0");
+    uint32_t kmax = 1;
+    uint64_t total_out = 0;
+    std::vector<uint64_t> s_out(n_samples);
+    for (uint32_t s = 0; s < n_samples; ++s) {
+        if (offsets[s + 1] < offsets[s]) return fail(c, PQ_EINVAL, "offsets must not decrease");
+        const uint64_t ns = offsets[s + 1] - offsets[s];
+        if (ns >= 0xFFFFFFFFull) return fail(c, PQ_EINVAL, "a sample has 2^32 rows or more");
+        if (ns > 0 && (ks[s] == 0 || ks[s] >= ns))
+            return fail(c, PQ_EINVAL, "sample " + std::to_string(s) + ": k must be in [1, n)");
+        if (ks[s] > 512) return fail(c, PQ_ENOTSUP, "the batched search supports k <= 512");
+        kmax = std::max(kmax, ks[s]);
+        s_out[s] = total_out;
+        total_out += ns * ks[s];
+    }
+    int kp = 32;
+    while (kp < int(kmax)) kp <<= 1;
+    return guarded(c, [&]() -> int {
+        cudaStream_t st = c->stream;
+        cudaStream_t user = static_cast<cudaStream_t>(stream);
+        cudaEvent_t ev;
+        ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        ck(cudaEventRecord(ev, user), "event");
+        ck(cudaStreamWaitEvent(st, ev, 0), "event");
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, c->device);
+        uint64_t* ds_off = c->get<uint64_t>("bt_off", n_samples + 1);
+        uint32_t* ds_k = c->get<uint32_t>("bt_k", n_samples);
+        uint64_t* ds_out = c->get<uint64_t>("bt_out", n_samples);
+        uint32_t* counter = c->get<uint32_t>("bt_counter", 1);
+        ck(cudaMemcpyAsync(ds_off, offsets, (n_samples + 1) * 8ull, cudaMemcpyHostToDevice, st), "h2d");
+        ck(cudaMemcpyAsync(ds_k, ks, n_samples * 4ull, cudaMemcpyHostToDevice, st), "h2d");
+        ck(cudaMemcpyAsync(ds_out, s_out.data(), n_samples * 8ull, cudaMemcpyHostToDevice, st), "h2d");
+        // samples largest first, then their query blocks
+        std::vector<uint32_t> order(n_samples);
+        for (uint32_t s = 0; s < n_samples; ++s) order[s] = s;
+        std::stable_sort(order.begin(), order.end(), [&](uint32_t x, uint32_t y) {
+            return offsets[x + 1] - offsets[x] > offsets[y + 1] - offsets[y];
+        });
+        auto items_for = [&](int shape, std::vector<uint32_t>& is, std::vector<uint32_t>& iq) {
+            const uint32_t qpi = uint32_t(pq::batched_queries_per_item(shape));
+            is.clear();
+            iq.clear();
+            for (uint32_t s : order)
+                for (uint64_t q = 0; q < offsets[s + 1] - offsets[s]; q += qpi) {
+                    is.push_back(s);
+                    iq.push_back(uint32_t(q));
+                }
+        };
+        pq::BatchLaunch b{};
+        b.X = d_data;
+        b.d = int(d);
+        b.s_off = ds_off;
+        b.s_k = ds_k;
+        b.s_out = ds_out;
+        b.counter = counter;
+        b.kp = kp;
+        b.sms = sms;
+        b.out_idx = d_indices;
+        b.out_dist = d_dists;
+        std::vector<uint32_t> is, iq;
+        auto upload_items = [&](uint32_t count) {
+            uint32_t* di_s = c->get<uint32_t>("bt_item_s", std::max<size_t>(is.size(), 1));
+            uint32_t* di_q = c->get<uint32_t>("bt_item_q", std::max<size_t>(iq.size(), 1));
+            ck(cudaMemcpyAsync(di_s, is.data(), is.size() * 4, cudaMemcpyHostToDevice, st), "h2d");
+            ck(cudaMemcpyAsync(di_q, iq.data(), iq.size() * 4, cudaMemcpyHostToDevice, st), "h2d");
+            b.item_s = di_s;
+            b.item_q = di_q;
+            b.n_items = count;
+        };
+        // ── autotune: each fitting shape on the largest work items ──
+        const uint64_t key = (d <= 32 ? 32ull : 64ull) << 32 | uint64_t(kp);
+        auto it = c->batch_shape.find(key);
+        int shape = -1;
+        if (it != c->batch_shape.end() && !(flags & PQ_BATCH_AUTOTUNE)) {
+            shape = it->second;
+        } else {
+            float best = 0.f;
+            cudaEvent_t e0, e1;
+            ck(cudaEventCreate(&e0), "event");
+            ck(cudaEventCreate(&e1), "event");
+            for (int sh = 0; sh < pq::batched_shapes(); ++sh) {
+                if (!pq::batched_shape_fits(sh, int(d), kp)) continue;
+                items_for(sh, is, iq);
+                // about four waves of the heaviest items, at equal query count per shape
+                const uint64_t want_q = uint64_t(4) * sms * 32;
+                const uint32_t qpi = uint32_t(pq::batched_queries_per_item(sh));
+                const uint32_t cnt = uint32_t(std::min<uint64_t>(is.size(), (want_q + qpi - 1) / qpi));
+                upload_items(cnt);
+                float ms = 0.f;
+                for (int rep = 0; rep < 2; ++rep) {  // the first run loads the kernel
+                    ck(cudaMemsetAsync(counter, 0, 4, st), "counter");
+                    ck(cudaEventRecord(e0, st), "event");
+                    ck(pq::launch_batched_knn(b, sh, st), "batched kNN (autotune)");
+                    ck(cudaEventRecord(e1, st), "event");
+                    ck(cudaEventSynchronize(e1), "event");
+                    ck(cudaEventElapsedTime(&ms, e0, e1), "event");
+                }
+                if (shape < 0 || ms < best) {
+                    shape = sh;
+                    best = ms;
+                }
+            }
+            cudaEventDestroy(e0);
+            cudaEventDestroy(e1);
+            if (shape < 0) throw DeviceError{"no tile shape fits this k and n_dim"};
+            c->batch_shape[key] = shape;
+        }
+        items_for(shape, is, iq);
+        upload_items(uint32_t(is.size()));
+        if (flags & PQ_BATCH_GRAPH) {
+            cudaStream_t cs;
+            ck(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking), "stream");
+            cudaGraph_t g = nullptr;
+            cudaGraphExec_t ge = nullptr;
+            ck(cudaStreamSynchronize(st), "items");
+            ck(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal), "capture");
+            cudaMemsetAsync(counter, 0, 4, cs);
+            pq::launch_batched_knn(b, shape, cs);
+            const cudaError_t ce = cudaStreamEndCapture(cs, &g);
+            if (ce != cudaSuccess) {
+                cudaStreamDestroy(cs);
+                ck(ce, "capture");
+            }
+            ck(cudaGraphInstantiate(&ge, g, 0), "graph");
+            ck(cudaGraphLaunch(ge, st), "graph launch");
+            ck(cudaStreamSynchronize(st), "graph");
+            cudaGraphExecDestroy(ge);
+            cudaGraphDestroy(g);
+            cudaStreamDestroy(cs);
+        } else {
+            ck(cudaMemsetAsync(counter, 0, 4, st), "counter");
+            ck(pq::launch_batched_knn(b, shape, st), "batched kNN");
+        }
+        ck(cudaEventRecord(ev, st), "event");
+        ck(cudaStreamWaitEvent(user, ev, 0), "event");
+        ck(cudaStreamSynchronize(st), "batched kNN");  // the host item arrays are reused
+        cudaEventDestroy(ev);
+        if (shape_out) *shape_out = shape;
         return PQ_OK;
     });
 }

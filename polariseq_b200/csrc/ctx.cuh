@@ -112,6 +112,7 @@ struct pq_ctx {
         unsigned long long launches;
     };
     std::vector<KGRec> kg_pending;
+    std::map<uint64_t, int> batch_shape;  // autotuned tile shape per (dims, heap size)
 
     template <class T>
     T* get(const std::string& name, size_t count) {

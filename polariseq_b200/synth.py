@@ -82,3 +82,44 @@ def mixture25(n: int, d: int = 30, seed: int = 0) -> np.ndarray:
     centers = rng.normal(size=(25, d)) * 5
     lab = rng.integers(0, 25, size=n)
     return (centers[lab] + rng.normal(size=(n, d))).astype(np.float32)
+
+
+def doublet_samples(count: int = 64, lo: int = 2000, hi: int = 60000, genes: int = 2000,
+                    d: int = 30, comps: int = 10, seed: int = 0, device: str = "cuda"):
+    """Per-sample embeddings of the doublet-scoring workload: each sample has
+    n_s cells (log-uniform in [lo, hi]) from a `comps`-component mixture of
+    negative-binomial counts (r = 2, gene means log-normal) plus 2 n_s
+    simulated doublets (sums of two random parent cells' counts), all
+    log1p-normalised (counts per 10^4) and projected by one seeded random
+    orthonormal genes x d basis.  Generated on the GPU with torch; returns a
+    list of float32 numpy arrays of 3 n_s rows."""
+    import torch
+
+    g = torch.Generator(device=device).manual_seed(seed)
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(lo), np.log(hi), count)).round().astype(int)
+    basis, _ = torch.linalg.qr(torch.randn(genes, d, generator=g, device=device))
+    base = torch.exp(torch.randn(genes, generator=g, device=device)) * 0.5
+    out = []
+    for n in sizes:
+        w = torch.from_numpy(rng.dirichlet(np.ones(comps))).float().to(device)
+        mu = base[None, :] * torch.exp(0.5 * torch.randn(comps, genes, generator=g, device=device))
+        comp = torch.multinomial(w, int(n), replacement=True, generator=g)
+        parts = []
+        cells = []
+        for c0 in range(0, int(n), 8192):
+            m = mu[comp[c0:c0 + 8192]]
+            lam = torch._standard_gamma(torch.full_like(m, 2.0), generator=g) * (m / 2.0)
+            cells.append(torch.poisson(lam, generator=g))
+        cells = torch.cat(cells)
+        pa = torch.randint(0, int(n), (2 * int(n),), generator=g, device=device)
+        pb = torch.randint(0, int(n), (2 * int(n),), generator=g, device=device)
+        for c0 in range(0, 3 * int(n), 8192):
+            idx = torch.arange(c0, min(c0 + 8192, 3 * int(n)), device=device)
+            cnt = torch.where((idx < n)[:, None], cells[idx.clamp(max=int(n) - 1)],
+                              cells[pa[(idx - n).clamp(min=0, max=2 * int(n) - 1)]] +
+                              cells[pb[(idx - n).clamp(min=0, max=2 * int(n) - 1)]])
+            tot = cnt.sum(1, keepdim=True).clamp(min=1.0)
+            parts.append(torch.log1p(cnt / tot * 1e4) @ basis)
+        out.append(torch.cat(parts).float().cpu().numpy())
+    return out
