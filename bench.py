@@ -54,7 +54,7 @@ def parse():
     ap.add_argument("--queries", type=int, default=20_000)
     ap.add_argument("--cpu-sample", type=int, default=262_144)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--form", default="bf16", choices=["plain", "bf16"],
+    ap.add_argument("--form", default="bf16", choices=["plain", "bf16", "fp8"],
                     help="the headline form (the other is measured too unless --skip-other)")
     ap.add_argument("--skip-other", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
@@ -73,8 +73,9 @@ def config(args):
     return {"workload": f"kNN graph build, {args.n} cells x {args.d} PCs f32, k={args.k}, "
                         f"{args.comps}-component log-normal Gaussian mixture, 5% doublets",
             "n_cells": args.n, "n_pcs": args.d, "k": args.k,
-            "form": "plain (bit-exact)" if args.form == "plain" else
-                    "chosen: bf16 tensor-core shortlist + FP32 re-rank + FP64 boundary",
+            "form": {"plain": "plain (bit-exact)",
+                     "bf16": "chosen: bf16 tensor-core shortlist + FP32 re-rank + FP64 boundary",
+                     "fp8": "e4m3 tensor-core shortlist + FP32 re-rank + FP64 boundary"}[args.form],
             "l2": "inputs larger than L2 (embedding 800 MB, graph 480 MB)"}
 
 
@@ -245,10 +246,10 @@ def join_roofline(per, st, args, peaks):
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
 
-def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, world):
+def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, world, k=None):
     """W warm-up then K device-resident builds of one form, timed with CUDA
     events on the launching stream (max over ranks), with per-group events."""
-    n, k = xd.shape[0], args.k
+    n, k = xd.shape[0], (k or args.k)
     cap = n * pq.effective_k(n, k)
     opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[form])
     ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
@@ -358,10 +359,16 @@ def main():
     head = measure_form(torch, pq, _lib, ctx, args.form, xd, dev, stream, args, barrier, world)
     ck = clocks.stop()
     forms = {args.form: head}
+    forms_k30 = {}
     if not args.skip_other:
-        other = "plain" if args.form != "plain" else "bf16"
-        forms[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, args, barrier,
-                                    world)
+        for other in ("plain", "bf16", "fp8"):
+            if other != args.form:
+                forms[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, args,
+                                            barrier, world)
+        # k = 30 (the E4M3 form supports k <= 15)
+        for other in ("bf16", "plain"):
+            forms_k30[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, args,
+                                            barrier, world, k=30)
 
     # ── end to end through the public API with pinned host buffers ──
     hx = torch.from_numpy(x).pin_memory()
@@ -406,6 +413,7 @@ def main():
         return out
 
     forms_out = {f: summary(v) for f, v in forms.items()}
+    forms_k30_out = {f: summary(v) for f, v in forms_k30.items()}
     if "plain" in forms:
         forms_out["plain"]["roofline"] = join_roofline(forms["plain"]["groups"],
                                                        forms["plain"]["stats"], args, peaks)
@@ -418,7 +426,7 @@ def main():
             "quality": {"recall_at_k": head["recall_at_k"],
                         "max_rel_dist_err": head["max_rel_dist_err"],
                         "queries": min(args.queries, n), "oracle": "FP64 brute force"},
-            "forms": forms_out}
+            "forms": forms_out, "forms_k30": forms_k30_out}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -39,7 +39,9 @@ typedef enum pq_status {
 /* Metric of the exact search (neighbors.rs:16-39). */
 enum { PQ_METRIC_EUCLIDEAN = 0, PQ_METRIC_COSINE = 1 };
 
-/* Search form.  PLAIN reproduces the reference graph bit for bit. */
+/* Search form.  PLAIN reproduces the reference graph bit for bit; BF16 and
+ * FP8 are the tensor-core shortlist forms (FP8: E4M3 tiles with per-row query
+ * and per-bucket candidate power-of-two scales, k <= 15). */
 enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
 /* Initial neighbour lists: the reference's RP-tree forest, or learned buckets. */
 enum { PQ_INIT_RP = 0, PQ_INIT_LEARNED = 1 };
@@ -59,7 +61,7 @@ typedef struct pq_nnd_opts {
     int32_t init;            /* PQ_INIT_* */
     /* Tensor-core forms only (ignored by PQ_MODE_PLAIN): */
     int32_t probes;          /* buckets each cell searches (<= 16); 0 -> min(14, buckets) */
-    int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (0) */
+    int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (BF16 0, FP8 1) */
 } pq_nnd_opts;
 
 /* Per-call statistics of the last build on a context. */

@@ -17,6 +17,7 @@
 //   5. optional NN-Descent rounds (the plain form's round kernels) polish the
 //      lists; the extract writes the CSR graph.
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include <algorithm>
 #include <cstdio>
@@ -196,6 +197,78 @@ __global__ void k_merge_runs(const float* __restrict__ rd, const uint32_t* __res
         oi[size_t(r) * s_out + o] = takex ? ix : iy;
         if (takex) ++x;
         else ++y;
+    }
+}
+
+// Largest |x - centre| over each bucket's candidate rows (non-negative floats
+// order as their bits).
+__global__ void k_bucket_absmax(const float* __restrict__ X, int d, int dp,
+                                const uint32_t* __restrict__ perm,
+                                const uint32_t* __restrict__ cbucket,
+                                const float* __restrict__ cent, uint32_t n,
+                                unsigned* __restrict__ amax) {
+    const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= n) return;
+    const uint32_t i = perm[r], b = cbucket[r];
+    float m = 0.f;
+    for (int j = lane; j < d; j += 32)
+        m = fmaxf(m, fabsf(X[size_t(i) * dp + j] - cent[size_t(b) * dp + j]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if (lane == 0) atomicMax(&amax[b], __float_as_uint(m));
+}
+
+// Power-of-two E4M3 scale 2^floor(log2(448 / absmax)) (exact in FP32), 1 for
+// an all-zero row or bucket.
+__device__ __forceinline__ float e4m3_scale(float amax) {
+    return amax > 0.f ? exp2f(floorf(log2f(448.0f / amax))) : 1.0f;
+}
+
+__global__ void k_bucket_scale(const unsigned* __restrict__ amax, uint32_t C,
+                               float* __restrict__ bscale) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b < C) bscale[b] = 1.0f / e4m3_scale(__uint_as_float(amax[b]));
+}
+
+// E4M3 rows (128 one-byte columns, zero padded) of (row(src_i) - centre(c_i))
+// scaled by the row's own power-of-two scale (bucket_amax == null: queries;
+// inv_scale receives 1/scale) or its bucket's (candidates).  norm receives the
+// FP32 |dequantised row|^2, times `norm_mult`.
+__global__ void k_to_fp8(const float* __restrict__ X, int d, int dp,
+                         const uint32_t* __restrict__ src, const uint32_t* __restrict__ cid,
+                         const float* __restrict__ cent, size_t rows,
+                         const unsigned* __restrict__ bucket_amax, uint32_t* __restrict__ out,
+                         float* __restrict__ inv_scale, float* __restrict__ norm,
+                         float norm_mult) {
+    const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (r >= rows) return;
+    const uint32_t i = src[r], c = cid[r];
+    float v[4];
+    float m = 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const int j = 4 * lane + u;
+        v[u] = j < d ? X[size_t(i) * dp + j] - cent[size_t(c) * dp + j] : 0.f;
+        m = fmaxf(m, fabsf(v[u]));
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    const float sc = e4m3_scale(bucket_amax ? __uint_as_float(bucket_amax[c]) : m);
+    uint32_t word = 0;
+    float s = 0.f;
+#pragma unroll
+    for (int u = 0; u < 4; ++u) {
+        const __nv_fp8_storage_t q = __nv_cvt_float_to_fp8(v[u] * sc, __NV_SATFINITE, __NV_E4M3);
+        const __half_raw hr = __nv_cvt_fp8_to_halfraw(q, __NV_E4M3);
+        const float deq = __half2float(__half(hr)) / sc;
+        s = fmaf(deq, deq, s);
+        word |= uint32_t(q) << (8 * u);
+    }
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
+    out[r * 32 + lane] = word;
+    if (lane == 0) {
+        norm[r] = s * norm_mult;
+        if (inv_scale) inv_scale[r] = 1.0f / sc;
     }
 }
 
@@ -652,9 +725,26 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
     uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
     k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, pos_of, cbucket); count_launch();
-    __nv_bfloat16* xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
-    float* xcn = c->get<float>("xc_norm", n);
-    k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, 2, xc, xcn); count_launch();
+    const bool fp8 = o.mode == PQ_MODE_FP8;
+    __nv_bfloat16* xc = nullptr;
+    uint32_t* xc8 = nullptr;
+    float* xch = nullptr;    // E4M3: |x~|^2 / 2 per candidate
+    float* bscale = nullptr;  // E4M3: 1 / the bucket's scale
+    if (!fp8) {
+        xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
+        float* xcn = c->get<float>("xc_norm", n);
+        k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, 2, xc, xcn); count_launch();
+    } else {
+        unsigned* amax = c->get<unsigned>("bucket_amax", C);
+        ck(cudaMemsetAsync(amax, 0, size_t(C) * 4, st), "amax");
+        k_bucket_absmax<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, amax); count_launch();
+        bscale = c->get<float>("bucket_scale", C);
+        k_bucket_scale<<<blocks(C, 256), 256, 0, st>>>(amax, C, bscale); count_launch();
+        xc8 = c->get<uint32_t>("xc_fp8", size_t(n) * 32);
+        xch = c->get<float>("xc_half", n);
+        k_to_fp8<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, amax, xc8,
+                                                nullptr, xch, 0.5f); count_launch();
+    }
     // query entries grouped by probe bucket (stable: cell order within a bucket)
     ck(radix_sort_pairs(ekeys, evals, ekeys2, evals2, ne, key_bits(2 * uint64_t(C) * C - 1),
                         c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
@@ -667,9 +757,19 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                                                      qpoint, qbucket, qself, entry_of); count_launch();
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
     k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, C, 2 * C, q_off); count_launch();
-    __nv_bfloat16* qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
+    __nv_bfloat16* qb = nullptr;
+    uint32_t* qb8 = nullptr;
+    float* qscale = nullptr;
     float* qbn = c->get<float>("q_norm", ne);
-    k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, 1, qb, qbn); count_launch();
+    if (!fp8) {
+        qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
+        k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, 1, qb, qbn); count_launch();
+    } else {
+        qb8 = c->get<uint32_t>("q_fp8", ne * 32);
+        qscale = c->get<float>("q_scale", ne);
+        k_to_fp8<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, nullptr, qb8,
+                                                 qscale, qbn, 1.0f); count_launch();
+    }
     std::vector<uint32_t> hq(2 * C + 1);
     ck(cudaMemcpyAsync(hq.data(), q_off, size_t(2 * C + 1) * 4, cudaMemcpyDeviceToHost, st),
        "q_off");
@@ -713,12 +813,14 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const int Ssh = ivf_shortlist(k + 1);        // per entry and column half
     const int Sout = ivf_groups() * Ssh;         // per entry: ivf_groups() ascending runs
     if (Ssh == 0) throw DeviceError{"the tensor-core form supports k <= 31"};
+    if (fp8 && Ssh > 16) throw DeviceError{"the E4M3 form supports k <= 15"};
     float* sd = c->get<float>("sl_d", ne * Sout);
     uint32_t* si = c->get<uint32_t>("sl_i", ne * Sout);
     {
         CUtensorMap tq, tcm;
-        if (!make_bf16_map(&tq, qb, ne, 128) || !make_bf16_map(&tcm, xc, n, 256))
-            throw DeviceError{"cuTensorMapEncodeTiled failed"};
+        const bool maps = fp8 ? make_fp8_map(&tq, qb8, ne, 128) && make_fp8_map(&tcm, xc8, n, 256)
+                              : make_bf16_map(&tq, qb, ne, 128) && make_bf16_map(&tcm, xc, n, 256);
+        if (!maps) throw DeviceError{"cuTensorMapEncodeTiled failed"};
         float* qthr = c->get<float>("q_thr", ne);
         const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
         unsigned long long* tbuf = nullptr;
@@ -730,7 +832,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         // another bucket can reach the cell's k best only by beating it; the two
         // extra places absorb the BF16 ranking error (recall@15 at 4M matches the
         // 2k-th seed to four digits, with 16% fewer tile-kernel cycles)
-        const int R0 = std::min(Sout, k + 2);
+        // (the E4M3 ranking error is larger: 2k places)
+        const int R0 = std::min(Sout, fp8 ? 2 * k : k + 2);
         // the primary pass starts without a bound and admits often: drain at
         // half a buffer so that its bound tightens sooner
         const int drain_at0 = 16;
@@ -760,6 +863,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.njobs = nj;
             a.c_off = c_off;
             a.qnorm = qbn;
+            a.fp8 = fp8 ? 1 : 0;
+            a.qscale = qscale;
+            a.bscale = bscale;
+            a.chalf = xch;
             a.qthr = pass ? qthr : nullptr;
             a.qself = qself;
             a.S = Ssh;
@@ -804,7 +911,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* ridx = c->get<uint32_t>("list_idx", size_t(n) * k);
     float* rdist = c->get<float>("list_dist", size_t(n) * k);
     // the exact re-rank list: 2k candidates ("2k-4k shortlist"), at most 64
-    const int R = std::min(P * Sout, std::min(64, std::max(2 * k, k + 1)));
+    // (E4M3: 4k, the wider end of the 2k-4k range, for its cruder ranking)
+    const int R = std::min(P * Sout, std::min(64, std::max(fp8 ? 4 * k : 2 * k, k + 1)));
     if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
     ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
     {
@@ -821,7 +929,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     ck(cudaMemcpyAsync(&fixes, c->d_acc, 8, cudaMemcpyDeviceToHost, st), "fixes");
     // ── 5. NN-Descent rounds from the shortlist lists, then the extract ──
     const Resolved RR = resolve(n64, o);
-    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : 0;
+    // auto: no polish round for BF16; one for E4M3, whose shortlist misses more
+    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : (fp8 ? 1 : 0);
     int rounds = 0;
     uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
     uint32_t* eoff = c->get<uint32_t>("eoff", n);

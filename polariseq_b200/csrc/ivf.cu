@@ -153,13 +153,13 @@ __device__ __forceinline__ void sort_pairs(float (&v)[S], uint32_t (&id)[S]) {
             }
 }
 
-__host__ __device__ constexpr int cand_stages(int S) { return S <= 16 ? 3 : 2; }
+__host__ __device__ constexpr int cand_stages(int S, bool f8) { return S <= 16 && !f8 ? 3 : 2; }
 
-template <int S>
+template <int S, bool F8>
 __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUtensorMap tmQ,
                                                      const __grid_constant__ CUtensorMap tmC,
                                                      IvfTileArgs a) {
-    constexpr int NCS = cand_stages(S);
+    constexpr int NCS = cand_stages(S, F8);
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     // 1024-align the dynamic region (the swizzle pattern follows address bits)
     uint8_t* smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
@@ -169,6 +169,9 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     uint32_t* hiall = reinterpret_cast<uint32_t*>(hdall + NG * S * TQ);     // NG x S x TQ
     float* bdall = reinterpret_cast<float*>(hiall + NG * S * TQ);           // NG x BUF x TQ
     uint32_t* biall = reinterpret_cast<uint32_t*>(bdall + NG * BUF * TQ);   // NG x BUF x TQ
+    // E4M3 only: |x~|^2 / 2 of the tile's columns, per TMEM buffer parity and
+    // column half (the four warps of a half write the same values)
+    float* hsall = reinterpret_cast<float*>(biall + NG * BUF * TQ);        // 2 x NG x CPG
     __shared__ IvfBars B;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     volatile int* abort_flag = &B.abort;
@@ -257,7 +260,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     } else if (w == NEPI / 32 + 1) {
         // ── MMA issuer ──
         if (lane == 0) {
-            const uint32_t idesc = tc::idesc_bf16_f32(TQ, TCN);
+            const uint32_t idesc = F8 ? tc::idesc_e4m3_f32(TQ, TCN) : tc::idesc_bf16_f32(TQ, TCN);
             uint32_t qi = 0, ci = 0, ti = 0;
             long long c_wait_c = 0, c_wait_t = 0;
             for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
@@ -285,8 +288,12 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                     const uint64_t dC = tc::desc_k_sw128(tc::smem_u32(sC + s * TCN * ROWB));
 #pragma unroll
                     for (int kk = 0; kk < 4; ++kk)  // K = 64 as four K = 16 steps (32 B each)
-                        tc::umma_f16(taddr + uint32_t(tb * TCN), dQ + uint64_t(2 * kk),
-                                     dC + uint64_t(2 * kk), idesc, kk > 0 ? 1u : 0u);
+                        if constexpr (F8)  // K = 128 one-byte columns as four K = 32 steps
+                            tc::umma_f8(taddr + uint32_t(tb * TCN), dQ + uint64_t(2 * kk),
+                                        dC + uint64_t(2 * kk), idesc, kk > 0 ? 1u : 0u);
+                        else
+                            tc::umma_f16(taddr + uint32_t(tb * TCN), dQ + uint64_t(2 * kk),
+                                         dC + uint64_t(2 * kk), idesc, kk > 0 ? 1u : 0u);
                     tc::umma_commit(&B.c_empty[s]);
                     tc::umma_commit(&B.t_full[tb]);
                     ++ci;
@@ -343,6 +350,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             const float thr0 = (valid && a.qthr) ? a.qthr[entry] : __int_as_float(0x7f800000);
             float thr = thr0;
             float ath = (qn - thr) * 0.5f;
+            // E4M3: the accumulator's scale back to the dot product of the rows
+            const float rq = F8 && valid ? a.qscale[entry] * a.bscale[b] : 1.0f;
             int cnt = 0;
             bool heaped = false;  // the heap holds entries (a drain moved some there)
 #pragma unroll 4
@@ -376,6 +385,15 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 // the slice's four 32-column chunks from registers: one max and
                 // one vote each; a chunk some row admits is handled on the spot
                 long long c1 = t0 ? clock64() : 0;
+                float* hs = hsall + (tb * NG + g) * CPG;
+                if constexpr (F8) {
+#pragma unroll
+                    for (int i = 0; i < CPG / 32; ++i) {
+                        const int col = i * 32 + lane;
+                        hs[col] = col < lim ? a.chalf[cbase + col] : 0.0f;
+                    }
+                    __syncwarp();
+                }
                 // two chunks in registers at a time (64 registers), so that a
                 // flagged chunk is handled from registers without spills
 #pragma unroll
@@ -388,8 +406,19 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 for (int qq = 0; qq < 2; ++qq) {
                     const int q = q2 + qq;
                     float v[32];
+                    if constexpr (F8) {
 #pragma unroll
-                    for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[qq][j]);
+                        for (int j = 0; j < 32; j += 4) {
+                            const float4 h4 = *reinterpret_cast<const float4*>(hs + q * 32 + j);
+                            v[j] = fmaf(__uint_as_float(r[qq][j]), rq, -h4.x);
+                            v[j + 1] = fmaf(__uint_as_float(r[qq][j + 1]), rq, -h4.y);
+                            v[j + 2] = fmaf(__uint_as_float(r[qq][j + 2]), rq, -h4.z);
+                            v[j + 3] = fmaf(__uint_as_float(r[qq][j + 3]), rq, -h4.w);
+                        }
+                    } else {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[qq][j]);
+                    }
                     if (lim < (q + 1) * 32) {
 #pragma unroll
                         for (int j = 0; j < 32; ++j)
@@ -420,7 +449,9 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                             const int j = __ffs(lm) - 1;
                             lm &= lm - 1;
                             if (cb0 + j != qself) {
-                                bd[cnt * TQ] = fmaf(-2.0f, __uint_as_float(select32(r[qq], j)), qn);
+                                float vj = __uint_as_float(select32(r[qq], j));
+                                if constexpr (F8) vj = fmaf(vj, rq, -hs[q * 32 + j]);
+                                bd[cnt * TQ] = fmaf(-2.0f, vj, qn);
                                 bi[cnt * TQ] = cb0 + j;
                                 ++cnt;
                             }
@@ -518,20 +549,20 @@ EncodeTiledFn encode_fn() {
     return fn;
 }
 
-template <int S>
+template <int S, bool F8>
 size_t tiles_smem() {
-    return 1024 + size_t(QST) * TQ * ROWB + size_t(cand_stages(S)) * TCN * ROWB +
-           size_t(NG) * S * TQ * 8 + size_t(NG) * BUF * TQ * 8;
+    return 1024 + size_t(QST) * TQ * ROWB + size_t(cand_stages(S, F8)) * TCN * ROWB +
+           size_t(NG) * S * TQ * 8 + size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * NG * CPG * 4 : 0);
 }
 
-template <int S>
+template <int S, bool F8>
 cudaError_t launch_s(const CUtensorMap& tmQ, const CUtensorMap& tmC, const IvfTileArgs& a,
                      int grid, cudaStream_t st) {
-    const size_t sm = tiles_smem<S>();
-    cudaError_t e = cudaFuncSetAttribute(k_ivf_tiles<S>,
+    const size_t sm = tiles_smem<S, F8>();
+    cudaError_t e = cudaFuncSetAttribute(k_ivf_tiles<S, F8>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
     if (e != cudaSuccess) return e;
-    k_ivf_tiles<S><<<grid, NT, sm, st>>>(tmQ, tmC, a); count_launch();
+    k_ivf_tiles<S, F8><<<grid, NT, sm, st>>>(tmQ, tmC, a); count_launch();
     return cudaGetLastError();
 }
 
@@ -552,6 +583,19 @@ bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t b
     return r == CUDA_SUCCESS;
 }
 
+bool make_fp8_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn) return false;
+    cuuint64_t dims[2] = {128, rows};
+    cuuint64_t strides[1] = {ROWB};
+    cuuint32_t box[2] = {128, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 2, const_cast<void*>(base), dims, strides,
+                    box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 int ivf_groups() { return NG; }
 
 int ivf_shortlist(int want) { return want <= 16 ? 16 : (want <= 32 ? 32 : 0); }
@@ -559,9 +603,14 @@ int ivf_shortlist(int want) { return want <= 16 ? 16 : (want <= 32 ? 32 : 0); }
 cudaError_t launch_ivf_tiles(const CUtensorMap& tmQ, const CUtensorMap& tmC,
                              const IvfTileArgs& a, int grid, cudaStream_t st) {
     if (a.njobs == 0) return cudaSuccess;
-    if (a.S == 1) return launch_s<1>(tmQ, tmC, a, grid, st);
-    if (a.S == 16) return launch_s<16>(tmQ, tmC, a, grid, st);
-    if (a.S == 32) return launch_s<32>(tmQ, tmC, a, grid, st);
+    if (a.fp8) {
+        if (a.S == 16) return launch_s<16, true>(tmQ, tmC, a, grid, st);
+        if (a.S == 32) return launch_s<32, true>(tmQ, tmC, a, grid, st);
+        return cudaErrorInvalidValue;
+    }
+    if (a.S == 1) return launch_s<1, false>(tmQ, tmC, a, grid, st);
+    if (a.S == 16) return launch_s<16, false>(tmQ, tmC, a, grid, st);
+    if (a.S == 32) return launch_s<32, false>(tmQ, tmC, a, grid, st);
     return cudaErrorInvalidValue;
 }
 

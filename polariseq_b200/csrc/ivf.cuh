@@ -24,6 +24,13 @@ struct IvfTileArgs {
     const uint32_t* qself;   // per query entry: its own candidate position, or ~0
     int S;                   // shortlist length per entry and column half: 1, 16 or 32
     int drain_at;            // buffer fill that triggers a drain into the heap (0: full)
+    // E4M3 tiles (the maps hold 128 one-byte columns per row, no norm
+    // columns): the accumulator times qscale[entry] * bscale[bucket] is the
+    // dot product, and chalf[candidate] = |x~|^2 / 2 is subtracted in FP32
+    int fp8;
+    const float* qscale;
+    const float* bscale;
+    const float* chalf;
     float* out_d;            // entries x (ivf_groups() x S): ascending runs of S
     uint32_t* out_i;         // the candidate positions (~0 = none)
     int* err;
@@ -36,6 +43,8 @@ enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT
        IVF_T_END_DRAIN = 13, IVF_TRACE_N = 16 };
 
 bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
+// A [rows x 128] one-byte (E4M3) matrix as 128-byte-swizzled boxes of box_rows x 128.
+bool make_fp8_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
 // Runs of one entry's output row.
 int ivf_groups();
 // The shortlist length the kernel supports for `want` entries (0 = too many).

@@ -1,13 +1,15 @@
 // sm_100a tensor-core building blocks: mbarriers with bounded waits, TMA 2D
 // tile loads (no cluster multicast: every load reads this GPU's own memory),
-// TMEM allocation, tcgen05.mma (kind::f16, BF16 in, FP32 accumulate in TMEM)
-// and tcgen05.ld, plus the shared-memory / instruction descriptors.
+// TMEM allocation, tcgen05.mma (kind::f16 with BF16 inputs, kind::f8f6f4 with
+// E4M3 inputs, FP32 accumulate in TMEM) and tcgen05.ld, plus the
+// shared-memory / instruction descriptors.
 //
 // Descriptor layouts follow the PTX ISA's tcgen05 "shared memory descriptor"
 // and "instruction descriptor" tables: smem descriptor = start address >> 4
 // [0,14), leading byte offset >> 4 [16,30), stride byte offset >> 4 [32,46),
 // version 1 [46,48), layout type [61,64) (2 = 128-byte swizzle); instruction
-// descriptor = D format [4,6) (1 = F32), A/B format [7,10)/[10,13) (1 = BF16),
+// descriptor = D format [4,6) (1 = F32), A/B format [7,10)/[10,13) (kind::f16:
+// 1 = BF16; kind::f8f6f4: 0 = E4M3),
 // A/B major [15]/[16] (0 = K-major), N >> 3 [17,23), M >> 4 [24,29).
 #pragma once
 
@@ -100,6 +102,17 @@ __device__ __forceinline__ void umma_f16(uint32_t d_tmem, uint64_t a_desc, uint6
         "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
         "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
 }
+// D[tmem] (+)= A x B^T, kind::f8f6f4 (E4M3 inputs per the instruction
+// descriptor, FP32 D); K = 32 elements (32 bytes) per instruction.
+__device__ __forceinline__ void umma_f8(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc,
+                                        uint32_t idesc, uint32_t accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+        "l"(a_desc), "l"(b_desc), "r"(idesc), "r"(accumulate));
+}
+
 // Arrives on `bar` once all previously issued tcgen05.mma of this thread complete.
 __device__ __forceinline__ void umma_commit(uint64_t* bar) {
     asm volatile(
@@ -137,6 +150,11 @@ __device__ __forceinline__ uint64_t desc_k_sw128(uint32_t smem_addr) {
     d |= uint64_t(1u) << 46;            // descriptor version
     d |= uint64_t(2u) << 61;            // 128-byte swizzle
     return d;
+}
+
+// kind::f8f6f4 instruction descriptor: E4M3 x E4M3 -> F32 (formats 0), both K-major.
+__host__ __device__ constexpr uint32_t idesc_e4m3_f32(int M, int N) {
+    return (1u << 4) | (uint32_t(N >> 3) << 17) | (uint32_t(M >> 4) << 24);
 }
 
 // kind::f16 instruction descriptor: BF16 x BF16 -> F32, both K-major.

@@ -73,3 +73,27 @@ def test_bf16_form_small_inputs_are_exact():
     g = pq.nndescent_dense(x, 10, mode="bf16")
     q = np.arange(0, 3000, 7, dtype=np.uint32)
     assert recall(g, x, 10, q) >= 0.999
+
+
+def test_fp8_form_recall_and_exact_distances():
+    """E4M3 tiles (per-row query scales, per-bucket candidate scales) with the
+    exact FP32 re-rank and its default polish round: recall against FP64 and
+    exact returned distances."""
+    n, k = 120_000, 15
+    x = synth.mixture_lognormal(n, 50, 30, seed=11)
+    g = pq.nndescent_dense(x, k, mode="fp8")
+    check_structure(g, n, k)
+    q = np.random.default_rng(3).choice(n, 2000, replace=False)
+    assert recall(g, x, k, q) >= 0.99
+    # returned distances are the exact FP32 distances of their pairs
+    ip, ix = g["indptr"], g["indices"]
+    for i in q[:200]:
+        js = ix[ip[i]:ip[i + 1]]
+        want = np.sqrt([oracle.sq_dist(x[i], x[j]) for j in js]).astype(np.float32)
+        np.testing.assert_array_equal(g["data"][ip[i]:ip[i + 1]], want)
+
+
+def test_fp8_form_rejects_large_k():
+    x = synth.mixture_dirichlet(5000, 50, 5, seed=1)
+    with pytest.raises(NotImplementedError):
+        pq.nndescent_dense(x, 30, mode="fp8")
