@@ -43,7 +43,9 @@ enum { PQ_METRIC_EUCLIDEAN = 0, PQ_METRIC_COSINE = 1 };
  * FP8 are the tensor-core shortlist forms (FP8: E4M3 tiles with per-row query
  * and per-bucket candidate power-of-two scales, k <= 15). */
 enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
-/* Initial neighbour lists: the reference's RP-tree forest, or learned buckets. */
+/* Initial neighbour lists: the reference's RP-tree forest, or learned buckets
+ * (tensor-core forms, n_obs >= 65,536: an MLP trained on a subsample's plain
+ * graph routes each cell to the buckets its neighbours live in). */
 enum { PQ_INIT_RP = 0, PQ_INIT_LEARNED = 1 };
 
 /* Mirrors NndescentOptions (nndescent.rs:42-76): zero = auto for the sized
@@ -60,8 +62,10 @@ typedef struct pq_nnd_opts {
     int32_t mode;            /* PQ_MODE_* */
     int32_t init;            /* PQ_INIT_* */
     /* Tensor-core forms only (ignored by PQ_MODE_PLAIN): */
-    int32_t probes;          /* buckets each cell searches (<= 16); 0 -> min(14, buckets) */
+    int32_t probes;          /* buckets each cell searches (<= 16); 0 -> min(14, buckets),
+                              * or 6 with PQ_INIT_LEARNED (1024 buckets, own bucket + MLP) */
     int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (BF16 0, FP8 1) */
+    int32_t buckets;         /* k-means buckets; 0 -> round(n / 4096), 1024 with PQ_INIT_LEARNED */
 } pq_nnd_opts;
 
 /* Per-call statistics of the last build on a context. */
@@ -82,6 +86,10 @@ typedef struct pq_nnd_stats {
      * [3] (query entry, candidate) distances contracted, [4] / [5] tile pairs of
      * the primary pass / the other probes, [6] FP64 boundary resolutions. */
     uint64_t shortlist[8];
+    /* PQ_INIT_LEARNED: mean training loss of the first and of the last epoch
+     * (the untrained router is the nearest-centroid prior), and the time of
+     * the subsample graph + training, and of routing every cell, in ms. */
+    double learn_loss_first, learn_loss_last, ms_learn_train, ms_learn_route;
 } pq_nnd_stats;
 
 /* Kernel groups timed by the profiling mode. */
@@ -173,6 +181,18 @@ int pq_neighbors_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_obs, u
                              uint64_t n_neighbors, int32_t metric, uint32_t* d_indptr,
                              uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
                              void* stream);
+
+/* Learned bucket routing (PQ_INIT_LEARNED), test hooks: the parameter count
+ * of the d -> 256 -> 256 -> 1024 MLP (layout W1 [d x 256], b1, W2 [256 x 256],
+ * b2, W3 [256 x 1024], b3, row-major f32), and one forward + backward pass on
+ * HOST buffers: weights used in BF16 (rounded from `params`), biases in FP32,
+ * softmax cross-entropy against T sparse (bucket, weight) targets per row
+ * (bucket 0xFFFFFFFF unused); writes the gradients of the mean loss, the
+ * per-row losses and (if not null) the logits (rows x 1024). */
+uint64_t pq_mlp_params(uint64_t n_dim);
+int pq_mlp_grad(pq_ctx* ctx, uint64_t n_dim, const float* params, const float* X, uint64_t rows,
+                const uint32_t* tb, const float* tw, uint32_t T, float* grad_out,
+                float* loss_out, float* logits_out);
 
 /* Flags of pq_knn_batched_into_device. */
 enum { PQ_BATCH_AUTOTUNE = 1, PQ_BATCH_GRAPH = 2 };

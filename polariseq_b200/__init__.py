@@ -49,7 +49,7 @@ def effective_k(n_obs: int, k: int) -> int:
 
 def _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size=0, gather_max=0,
           mode=_lib.PQ_MODE_PLAIN, init=_lib.PQ_INIT_RP, probes=0,
-          refine_rounds=-1) -> _lib.NndOpts:
+          refine_rounds=-1, buckets=0) -> _lib.NndOpts:
     o = _lib.NndOpts()
     _lib.load().pq_nnd_opts_default(C.byref(o))
     o.k = int(k)
@@ -64,6 +64,7 @@ def _opts(k, max_iterations, seed, max_candidates, n_trees, delta, leaf_size=0, 
     o.init = int(init)
     o.probes = int(probes)
     o.refine_rounds = int(refine_rounds)
+    o.buckets = int(buckets)
     return o
 
 
@@ -115,7 +116,9 @@ class Context:
             "changed": list(s.changed[:r]), "emitted": list(s.emitted[:r]),
             "pairs": list(s.pairs[:r]), "ms_forest": s.ms_forest, "ms_leaves": s.ms_leaves,
             "ms_rounds": s.ms_rounds, "ms_extract": s.ms_extract, "ms_total": s.ms_total,
-            "shortlist": list(s.shortlist),
+            "shortlist": list(s.shortlist), "learn_loss_first": s.learn_loss_first,
+            "learn_loss_last": s.learn_loss_last, "ms_learn_train": s.ms_learn_train,
+            "ms_learn_route": s.ms_learn_route,
         }
 
     # -- host-buffer build (the drop-in) ------------------------------------
@@ -273,7 +276,7 @@ INITS = {"rp": _lib.PQ_INIT_RP, "learned": _lib.PQ_INIT_LEARNED}
 
 def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_trees=0,
                     delta=0.001, out=None, *, device: int = 0, mode: str = "plain",
-                    init: str = "rp", probes: int = 0, refine_rounds: int = -1):
+                    init: str = "rp", probes: int = 0, refine_rounds: int = -1, buckets: int = 0):
     """Approximate kNN graph by NN-Descent, bit-exact with the reference
     (crates/polariseq-python/src/lib.rs:503-566).
 
@@ -283,7 +286,7 @@ def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_
     emb = _as_embedding(embedding)
     n_obs, _ = emb.shape
     opts = _opts(k, max_iterations, seed, max_candidates, n_trees, delta, mode=MODES[mode],
-                 init=INITS[init], probes=probes, refine_rounds=refine_rounds)
+                 init=INITS[init], probes=probes, refine_rounds=refine_rounds, buckets=buckets)
     cap = n_obs * effective_k(n_obs, k)
     # the same order as the binding: the out sizes are validated (ValueError)
     # before the core runs and panics on empty data or k == 0

@@ -24,6 +24,7 @@ EXPORTS = (
     "pq_ctx_last_error", "pq_ctx_stats", "pq_nndescent_into", "pq_nndescent_into_device",
     "pq_nndescent_probe", "pq_debug_tree", "pq_ctx_set_profiling", "pq_neighbors_into",
     "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc", "pq_knn_batched_into_device",
+    "pq_mlp_params", "pq_mlp_grad",
 )
 
 
@@ -43,6 +44,7 @@ class NndOpts(C.Structure):
         ("init", C.c_int32),
         ("probes", C.c_int32),
         ("refine_rounds", C.c_int32),
+        ("buckets", C.c_int32),
     ]
 
 
@@ -67,6 +69,10 @@ class NndStats(C.Structure):
         ("kg_ms", C.c_double * 16),
         ("kg_launches", C.c_uint64 * 16),
         ("shortlist", C.c_uint64 * 8),
+        ("learn_loss_first", C.c_double),
+        ("learn_loss_last", C.c_double),
+        ("ms_learn_train", C.c_double),
+        ("ms_learn_route", C.c_double),
     ]
 
 
@@ -135,5 +141,9 @@ def load(build_if_missing: bool = False):
         L.pq_knn_batched_into_device.argtypes = [P, P, U64, C.c_uint32, P, P, P, P, C.c_int32,
                                                   C.POINTER(C.c_int32), P]
         L.pq_knn_batched_into_device.restype = C.c_int
+        L.pq_mlp_params.argtypes = [U64]
+        L.pq_mlp_params.restype = U64
+        L.pq_mlp_grad.argtypes = [P, U64, P, P, U64, P, P, C.c_uint32, P, P, P]
+        L.pq_mlp_grad.restype = C.c_int
         _lib = L
         return L

@@ -10,6 +10,7 @@
 #include "ctx.cuh"
 #include "exact.cuh"
 #include "batched.cuh"
+#include "mlp.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
@@ -492,8 +493,11 @@ int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
         return fail(c, PQ_ENOTSUP, "mode not available in this build");
     if (o->mode == PQ_MODE_FP8 && R.k > 15)
         return fail(c, PQ_ENOTSUP, "the E4M3 form supports k <= 15");
-    if (o->init != PQ_INIT_RP)
+    if (o->init != PQ_INIT_RP && o->init != PQ_INIT_LEARNED)
         return fail(c, PQ_ENOTSUP, "init not available in this build");
+    if (o->init == PQ_INIT_LEARNED && (o->mode == PQ_MODE_PLAIN || n < 65536))
+        return fail(c, PQ_ENOTSUP,
+                    "learned probes need a tensor-core form and at least 65,536 cells");
     if (o->mode != PQ_MODE_PLAIN && d > 62)
         return fail(c, PQ_ENOTSUP, "the tensor-core form supports n_dim <= 62");
     if (o->mode != PQ_MODE_PLAIN && R.k > 31)
@@ -920,6 +924,50 @@ int pq_knn_batched_into_device(pq_ctx* c, const float* d_data, uint64_t d, uint3
         ck(cudaStreamSynchronize(st), "batched kNN");  // the host item arrays are reused
         cudaEventDestroy(ev);
         if (shape_out) *shape_out = shape;
+        return PQ_OK;
+    });
+}
+
+uint64_t pq_mlp_params(uint64_t n_dim) { return pq::mlp_params(int(n_dim)); }
+
+int pq_mlp_grad(pq_ctx* c, uint64_t d, const float* params, const float* X, uint64_t rows,
+                const uint32_t* tb, const float* tw, uint32_t T, float* grad_out,
+                float* loss_out, float* logits_out) {
+    if (!c) return PQ_EINVAL;
+    if (!params || !X || !tb || !tw || !grad_out || !loss_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    if (d == 0 || d > 4096 || rows == 0 || rows > (1u << 20) || T == 0 || T > 32)
+        return fail(c, PQ_EINVAL, "bad sizes");
+    return guarded(c, [&]() -> int {
+        cudaStream_t st = c->stream;
+        const size_t np = pq::mlp_params(int(d));
+        pq::MlpView net{int(d), c->get<float>("mg_w", np), c->get<__nv_bfloat16>("mg_wb", np)};
+        float* dx = c->get<float>("mg_x", rows * d);
+        uint32_t* dtb = c->get<uint32_t>("mg_tb", rows * T);
+        float* dtw = c->get<float>("mg_tw", rows * T);
+        float* h1 = c->get<float>("mg_h1", rows * pq::MLP_H);
+        float* h2 = c->get<float>("mg_h2", rows * pq::MLP_H);
+        float* z = c->get<float>("mg_z", rows * pq::MLP_OUT);
+        float* dh1 = c->get<float>("mg_dh1", rows * pq::MLP_H);
+        float* dh2 = c->get<float>("mg_dh2", rows * pq::MLP_H);
+        float* g = c->get<float>("mg_g", np);
+        float* loss = c->get<float>("mg_loss", rows);
+        float* scratch = c->get<float>("mg_scratch", pq::mlp_scratch_floats());
+        ck(cudaMemcpyAsync(net.w, params, np * 4, cudaMemcpyHostToDevice, st), "h2d");
+        ck(cudaMemcpyAsync(dx, X, rows * d * 4, cudaMemcpyHostToDevice, st), "h2d");
+        ck(cudaMemcpyAsync(dtb, tb, rows * T * 4, cudaMemcpyHostToDevice, st), "h2d");
+        ck(cudaMemcpyAsync(dtw, tw, rows * T * 4, cudaMemcpyHostToDevice, st), "h2d");
+        pq::mlp_sync_bf16(net, st);
+        pq::mlp_forward(net, dx, int(rows), h1, h2, z, st);
+        if (logits_out)
+            ck(cudaMemcpyAsync(logits_out, z, rows * pq::MLP_OUT * 4, cudaMemcpyDeviceToHost, st),
+               "d2h");
+        pq::mlp_backward(net, dx, int(rows), h1, h2, z, dtb, dtw, int(T), loss, dh1, dh2, g,
+                         scratch, st);
+        ck(cudaGetLastError(), "mlp");
+        ck(cudaMemcpyAsync(grad_out, g, np * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        ck(cudaMemcpyAsync(loss_out, loss, rows * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        ck(cudaStreamSynchronize(st), "mlp");
         return PQ_OK;
     });
 }

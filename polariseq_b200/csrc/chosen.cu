@@ -605,8 +605,13 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     tm.start();
     std::optional<KGScope> kg_sec;
     kg_sec.emplace(c, PQ_KG_BUCKETS);
-    const uint32_t C = std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
-    const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : 14u, std::min(C, 16u)));
+    const bool learned = o.init == PQ_INIT_LEARNED;
+    // learned probes: the MLP's 1024 buckets; else about 4096 cells per bucket
+    const uint32_t C = learned ? 1024u
+                       : o.buckets > 0 ? std::min<uint32_t>(uint32_t(o.buckets), n)
+                                       : std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
+    const uint32_t P_auto = learned ? 6u : 14u;
+    const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : P_auto, std::min(C, 16u)));
     const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
     if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};
     if (uint64_t(C) * C * 2 >= 0xFFFFFFFFull)
@@ -691,7 +696,16 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan); count_launch();
     uint32_t* probes = c->get<uint32_t>("probes", size_t(n) * P);
     float* probe_d = c->get<float>("probe_d", size_t(n) * P);
-    centroid_search(qa, qan, n, P, probe_d, probes);
+    double ms_train = 0.0, ms_route = 0.0;
+    if (learned) {  // own bucket by k-means, the other probes from the MLP
+        uint32_t* prim = c->get<uint32_t>("primary", n);
+        float* prim_d = c->get<float>("primary_d", n);
+        centroid_search(qa, qan, n, 1, prim_d, prim);
+        ms_route = learned_probes(c, X, d, dp, n, C, prim, prim_d, cent, P, o.seed, probes,
+                                  &ms_train, &S_.learn_loss_first, &S_.learn_loss_last);
+    } else {
+        centroid_search(qa, qan, n, P, probe_d, probes);
+    }
     int herr0 = 0;
     ck(cudaMemcpy(&herr0, c->d_err, 4, cudaMemcpyDeviceToHost), "err");
     if (herr0) throw DeviceError{"centroid tiles: a bounded wait gave up"};
@@ -960,6 +974,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     S_.ms_extract = tm.stop();
     S_.ms_total = tot.stop();
     S_.shortlist[6] = fixes;
+    S_.ms_learn_train = ms_train;
+    S_.ms_learn_route = ms_route;
     S_.rounds_run = rounds;  // polish rounds after the shortlist
     S_.n_trees = int32_t(C);
     S_.max_candidates = uint64_t(P) << 32 | uint64_t(Ssh);

@@ -185,6 +185,14 @@ int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int 
                const uint32_t* perm, int stats_offset,
                const std::function<bool(int, const uint32_t*, const uint32_t*)>& after_round);
 
+// Learned probes (learned.cu): probes[i * P] = primary[i], then the MLP's P - 1
+// most likely other buckets; trains the MLP on a subsample's plain graph.
+// Returns the routing (inference) time in ms; *ms_train gets the training time.
+double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint32_t C,
+                      const uint32_t* primary, const float* primary_d, const float* cent, int P,
+                      uint64_t seed, uint32_t* probes, double* ms_train, double* loss_first,
+                      double* loss_last);
+
 // The chosen form (tensor-core shortlist), chosen.cu.
 uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64,
                       uint64_t d64, const pq_nnd_opts& o, uint32_t* d_indptr,

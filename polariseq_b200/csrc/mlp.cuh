@@ -1,0 +1,57 @@
+// Learned bucket routing MLP (mlp.cu): d -> 256 -> 256 -> 1024, ReLU.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+namespace pq {
+
+constexpr int MLP_H = 256;     // hidden width
+constexpr int MLP_OUT = 1024;  // bucket logits
+
+// Offsets (in parameters) of W1 [d x H], b1 [H], W2 [H x H], b2, W3 [H x OUT], b3.
+struct MlpLayout {
+    size_t w1, b1, w2, b2, w3, b3;
+};
+MlpLayout mlp_layout(int d);
+size_t mlp_params(int d);
+size_t mlp_scratch_floats();
+
+// FP32 master parameters `w` and their BF16 copies `wb` (same layout); the
+// GEMMs read the BF16 weights and the FP32 biases.
+struct MlpView {
+    int d;
+    float* w;
+    __nv_bfloat16* wb;
+};
+
+// The nearest-centroid prior added to the logits: -beta |x - c_b|^2 up to a
+// per-row constant, i.e. X . cs_b^T + cb_b with cs = 2 beta c (1024 x d rows,
+// stride ld) and cb = -beta |c_b|^2.  The MLP learns a correction to it.
+struct MlpPrior {
+    const float* cs = nullptr;
+    int ld = 0;
+    const float* cb = nullptr;
+};
+
+// H1 = relu(X W1 + b1), H2 = relu(H1 W2 + b2), Z = H2 W3 + b3 (+ prior)
+// (rows x 1024).
+void mlp_forward(const MlpView& net, const float* X, int rows, float* H1, float* H2, float* Z,
+                 cudaStream_t st, const MlpPrior* prior = nullptr);
+// Softmax cross-entropy against sparse soft targets (T pairs per row, bucket
+// ~0 unused) and the parameter gradients of the mean loss into `grad`
+// (overwritten); Z is overwritten with dZ, loss gets the per-row loss.
+void mlp_backward(const MlpView& net, const float* X, int rows, float* H1, float* H2, float* Z,
+                  const uint32_t* tb, const float* tw, int T, float* loss, float* dH1,
+                  float* dH2, float* grad, float* scratch, cudaStream_t st);
+// One Adam step (step >= 1) on the master weights; refreshes the BF16 copies.
+void mlp_adam(MlpView& net, float* m, float* v, const float* grad, int step, float lr,
+              cudaStream_t st);
+void mlp_sync_bf16(MlpView& net, cudaStream_t st);
+// The P largest logits of each row, skipping skip[r] (may be null).
+void mlp_topp(const float* Z, int rows, int P, const uint32_t* skip, uint32_t* out,
+              cudaStream_t st);
+
+}  // namespace pq
