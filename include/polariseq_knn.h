@@ -182,6 +182,29 @@ int pq_neighbors_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_obs, u
                              uint32_t* d_indices, float* d_dists, uint64_t* nnz_out,
                              void* stream);
 
+/* umap::fuzzy_connectivities_from (crates/polariseq-core/src/umap.rs:122-138,
+ * 283-620; PyO3 fuzzy_connectivities, crates/polariseq-python/src/lib.rs:
+ * 568-589): the symmetrised fuzzy simplicial set of a kNN distance graph —
+ * per-row membership strengths (smooth_knn_dist), their transpose, and the
+ * fuzzy union a + b - a*b per pair, pruned at 1e-5 — as a symmetric CSR with
+ * both directions stored, rows sorted by column, no self-loops.  HOST
+ * buffers: the distance graph (indptr n_obs+1, indices/data indptr[n_obs]);
+ * the result needs at most 2 * indptr[n_obs] entries (out_cap).  Rows of the
+ * input may hold at most 256 entries (PQ_ENOTSUP beyond). */
+int pq_fuzzy_connectivities(pq_ctx* ctx, uint64_t n_obs, const uint32_t* indptr,
+                            const uint32_t* indices, const float* data, uint32_t* out_indptr,
+                            uint32_t* out_indices, float* out_weights, uint64_t out_cap,
+                            uint64_t* nnz_out);
+
+/* The same on DEVICE buffers (nnz = the input's entry count), so the graph of
+ * pq_nndescent_into_device / pq_neighbors_into_device is used where it is;
+ * synchronises the context's stream once (to size the result). */
+int pq_fuzzy_connectivities_device(pq_ctx* ctx, uint64_t n_obs, const uint32_t* d_indptr,
+                                   const uint32_t* d_indices, const float* d_data, uint64_t nnz,
+                                   uint32_t* d_out_indptr, uint32_t* d_out_indices,
+                                   float* d_out_weights, uint64_t out_cap, uint64_t* nnz_out,
+                                   void* stream);
+
 /* Learned bucket routing (PQ_INIT_LEARNED), test hooks: the parameter count
  * of the d -> 256 -> 256 -> 1024 MLP (layout W1 [d x 256], b1, W2 [256 x 256],
  * b2, W3 [256 x 1024], b3, row-major f32), and one forward + backward pass on

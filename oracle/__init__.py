@@ -2,8 +2,10 @@
 
 ctypes bindings to the C++ restatement of the reference's CPU NN-Descent
 (``nndescent_ref.cpp``, restating crates/polariseq-core/src/nndescent.rs:78-1003
-and simd.rs:14-81) and to the FP64 exact kNN / exact f32 search restatement
-(``exact_ref.cpp``, neighbors.rs:101-241).
+and simd.rs:14-81), to the FP64 exact kNN / exact f32 search restatement
+(``exact_ref.cpp``, neighbors.rs:101-241) and to the fuzzy simplicial set
+restatement (``fuzzy_ref.cpp``, umap.rs:283-620); ``mlp_ref.py`` restates the
+learned router's gradients in float64 NumPy.
 
 Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py``'s CPU-baseline
 leg may import this module; the product package never does.
@@ -94,6 +96,10 @@ def lib():
         L.oracle_neighbors_exact.argtypes = [P, C.c_uint64, C.c_uint64, C.c_uint64, C.c_int,
                                              P, P, P]
         L.oracle_neighbors_exact.restype = C.c_int
+        L.oracle_smooth_knn_dist.argtypes = [P, C.c_uint64, P]
+        L.oracle_smooth_knn_dist.restype = None
+        L.oracle_fuzzy.argtypes = [C.c_uint64, P, P, P, P, P, P, C.c_uint64]
+        L.oracle_fuzzy.restype = C.c_uint64
         _lib = L
     return _lib
 
@@ -254,3 +260,24 @@ def neighbors_exact(emb: np.ndarray, n_neighbors: int, metric: str = "euclidean"
         raise ValueError(f"oracle neighbors rejected the input (code {rc})")
     m = int(ip[-1])
     return {"indptr": ip, "indices": ix[:m].copy(), "data": dx[:m].copy(), "n_obs": n}
+
+
+def smooth_knn_dist(dists) -> np.ndarray:
+    """umap.rs:551-620: membership strengths of one row of ascending distances."""
+    d = np.ascontiguousarray(dists, np.float32)
+    out = np.zeros(d.size, np.float32)
+    lib().oracle_smooth_knn_dist(_ptr(d), d.size, _ptr(out))
+    return out
+
+
+def fuzzy_connectivities(indptr, indices, data, n_obs: int) -> dict:
+    """umap.rs:122-138 fuzzy_connectivities_from: the symmetric CSR."""
+    ip = np.ascontiguousarray(indptr, np.uint32)
+    ix = np.ascontiguousarray(indices, np.uint32)
+    dx = np.ascontiguousarray(data, np.float32)
+    cap = max(2 * int(ip[-1]), 1)
+    oip = np.zeros(n_obs + 1, np.uint32)
+    oix = np.zeros(cap, np.uint32)
+    ow = np.zeros(cap, np.float32)
+    nnz = lib().oracle_fuzzy(n_obs, _ptr(ip), _ptr(ix), _ptr(dx), _ptr(oip), _ptr(oix), _ptr(ow), cap)
+    return {"indptr": oip, "indices": oix[:nnz].copy(), "data": ow[:nnz].copy()}

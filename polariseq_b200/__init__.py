@@ -29,7 +29,7 @@ from . import _lib
 
 __all__ = [
     "PanicException", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
-    "neighbors_dense", "knn_batched",
+    "neighbors_dense", "knn_batched", "fuzzy_connectivities",
 ]
 
 
@@ -203,6 +203,24 @@ class Context:
             self._check(rc, "knn_batched")
         return int(shape.value)
 
+    # -- fuzzy connectivities ------------------------------------------------
+    def fuzzy_connectivities(self, indptr, indices, data, n_obs: int) -> dict:
+        ip = np.ascontiguousarray(indptr, np.uint32)
+        ix = np.ascontiguousarray(indices, np.uint32)
+        dx = np.ascontiguousarray(data, np.float32)
+        cap = max(2 * int(ip[n_obs]), 1)
+        oip = np.zeros(n_obs + 1, np.uint32)
+        oix = np.zeros(cap, np.uint32)
+        ow = np.zeros(cap, np.float32)
+        nnz = C.c_uint64(0)
+        with self._lock:
+            rc = _lib.load().pq_fuzzy_connectivities(
+                self._h, n_obs, ip.ctypes.data, ix.ctypes.data, dx.ctypes.data, oip.ctypes.data,
+                oix.ctypes.data, ow.ctypes.data, cap, C.byref(nnz))
+            self._check(rc, "fuzzy_connectivities")
+        m = int(nnz.value)
+        return {"indptr": oip, "indices": oix[:m].copy(), "data": ow[:m].copy()}
+
     # -- parity probes (test hooks) ----------------------------------------
     def probe(self, data: np.ndarray, opts: _lib.NndOpts, stop_after: int) -> dict:
         data = np.ascontiguousarray(data, np.float32)
@@ -313,6 +331,17 @@ def nndescent_dense(embedding, k, max_iterations=0, seed=0, max_candidates=0, n_
 
 
 METRICS = {"euclidean": _lib.PQ_METRIC_EUCLIDEAN, "cosine": _lib.PQ_METRIC_COSINE}
+
+
+def fuzzy_connectivities(indptr, indices, data, n_obs, *, device: int = 0) -> dict:
+    """The symmetrised fuzzy connectivities of a kNN distance graph, as the
+    reference's ``fuzzy_connectivities`` (crates/polariseq-python/src/
+    lib.rs:568-589, umap.rs:122-138): ``{"indptr", "indices", "data"}``, a
+    symmetric CSR with both directions stored, rows sorted by column."""
+    ip = np.asarray(indptr)
+    if ip.size != int(n_obs) + 1:
+        raise ValueError("indptr must have n_obs + 1 entries")
+    return default_context(device).fuzzy_connectivities(indptr, indices, data, int(n_obs))
 
 
 def knn_batched(samples, ks, *, device: int = 0, autotune: bool = False, graph: bool = True):

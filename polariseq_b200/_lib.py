@@ -24,7 +24,7 @@ EXPORTS = (
     "pq_ctx_last_error", "pq_ctx_stats", "pq_nndescent_into", "pq_nndescent_into_device",
     "pq_nndescent_probe", "pq_debug_tree", "pq_ctx_set_profiling", "pq_neighbors_into",
     "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc", "pq_knn_batched_into_device",
-    "pq_mlp_params", "pq_mlp_grad",
+    "pq_mlp_params", "pq_mlp_grad", "pq_fuzzy_connectivities", "pq_fuzzy_connectivities_device",
 )
 
 
@@ -145,5 +145,10 @@ def load(build_if_missing: bool = False):
         L.pq_mlp_params.restype = U64
         L.pq_mlp_grad.argtypes = [P, U64, P, P, U64, P, P, C.c_uint32, P, P, P]
         L.pq_mlp_grad.restype = C.c_int
+        L.pq_fuzzy_connectivities.argtypes = [P, U64, P, P, P, P, P, P, U64, C.POINTER(U64)]
+        L.pq_fuzzy_connectivities.restype = C.c_int
+        L.pq_fuzzy_connectivities_device.argtypes = [P, U64, P, P, P, U64, P, P, P, U64,
+                                                     C.POINTER(U64), P]
+        L.pq_fuzzy_connectivities_device.restype = C.c_int
         _lib = L
         return L

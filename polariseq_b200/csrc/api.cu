@@ -11,6 +11,7 @@
 #include "exact.cuh"
 #include "batched.cuh"
 #include "mlp.cuh"
+#include "fuzzy.cuh"
 #include "kernels.cuh"
 #include "primitives.cuh"
 
@@ -969,6 +970,87 @@ int pq_mlp_grad(pq_ctx* c, uint64_t d, const float* params, const float* X, uint
         ck(cudaMemcpyAsync(loss_out, loss, rows * 4, cudaMemcpyDeviceToHost, st), "d2h");
         ck(cudaStreamSynchronize(st), "mlp");
         return PQ_OK;
+    });
+}
+
+namespace {
+int fuzzy_run(pq_ctx* c, uint64_t n, uint64_t nnz, const uint32_t* d_ip, const uint32_t* d_ix,
+              const float* d_dx, uint32_t* d_oip, uint32_t* d_oix, float* d_ow, uint64_t out_cap,
+              uint64_t* nnz_out, cudaStream_t st) {
+    uint8_t* temp = c->get<uint8_t>("fz_temp", pq::fuzzy_temp_bytes(n, nnz));
+    uint64_t h = 0;
+    const cudaError_t e = pq::launch_fuzzy(n, nnz, d_ip, d_ix, d_dx, temp, d_oip, d_oix, d_ow,
+                                           out_cap, c->d_u64, c->d_err, &h, st);
+    if (e == cudaErrorNotSupported)
+        return fail(c, PQ_ENOTSUP, "a row of the graph has more than 256 entries");
+    if (e == cudaErrorInvalidValue)
+        return fail(c, PQ_EINVAL, "the connectivity arrays are too short");
+    ck(e, "fuzzy connectivities");
+    *nnz_out = h;
+    return PQ_OK;
+}
+}  // namespace
+
+int pq_fuzzy_connectivities(pq_ctx* c, uint64_t n, const uint32_t* indptr,
+                            const uint32_t* indices, const float* data, uint32_t* out_indptr,
+                            uint32_t* out_indices, float* out_weights, uint64_t out_cap,
+                            uint64_t* nnz_out) {
+    if (!c) return PQ_EINVAL;
+    if (!indptr || !indices || !data || !out_indptr || !out_indices || !out_weights || !nnz_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    if (n == 0 || n >= 0xFFFFFFFFull) return fail(c, PQ_EINVAL, "n_obs must be in [1, 2^32 - 1)");
+    const uint64_t nnz = indptr[n];
+    return guarded(c, [&]() -> int {
+        cudaStream_t st = c->stream;
+        uint32_t* ip = c->get<uint32_t>("fz_ip", n + 1);
+        uint32_t* ix = c->get<uint32_t>("fz_ix", std::max<uint64_t>(nnz, 1));
+        float* dx = c->get<float>("fz_dx", std::max<uint64_t>(nnz, 1));
+        const uint64_t cap = std::max<uint64_t>(2 * nnz, 1);
+        uint32_t* oip = c->get<uint32_t>("fz_oip", n + 1);
+        uint32_t* oix = c->get<uint32_t>("fz_oix", cap);
+        float* ow = c->get<float>("fz_ow", cap);
+        ck(cudaMemcpyAsync(ip, indptr, (n + 1) * 4, cudaMemcpyHostToDevice, st), "h2d");
+        if (nnz) {
+            ck(cudaMemcpyAsync(ix, indices, nnz * 4, cudaMemcpyHostToDevice, st), "h2d");
+            ck(cudaMemcpyAsync(dx, data, nnz * 4, cudaMemcpyHostToDevice, st), "h2d");
+        }
+        uint64_t m = 0;
+        const int rc = fuzzy_run(c, n, nnz, ip, ix, dx, oip, oix, ow, cap, &m, st);
+        if (rc != PQ_OK) return rc;
+        if (m > out_cap) return fail(c, PQ_EINVAL, "the connectivity arrays are too short");
+        ck(cudaMemcpyAsync(out_indptr, oip, (n + 1) * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        if (m) {
+            ck(cudaMemcpyAsync(out_indices, oix, m * 4, cudaMemcpyDeviceToHost, st), "d2h");
+            ck(cudaMemcpyAsync(out_weights, ow, m * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        }
+        ck(cudaStreamSynchronize(st), "d2h");
+        *nnz_out = m;
+        return PQ_OK;
+    });
+}
+
+int pq_fuzzy_connectivities_device(pq_ctx* c, uint64_t n, const uint32_t* d_indptr,
+                                   const uint32_t* d_indices, const float* d_data, uint64_t nnz,
+                                   uint32_t* d_out_indptr, uint32_t* d_out_indices,
+                                   float* d_out_weights, uint64_t out_cap, uint64_t* nnz_out,
+                                   void* stream) {
+    if (!c) return PQ_EINVAL;
+    if (!d_indptr || !d_indices || !d_data || !d_out_indptr || !d_out_indices || !d_out_weights ||
+        !nnz_out)
+        return fail(c, PQ_EINVAL, "null buffer");
+    if (n == 0 || n >= 0xFFFFFFFFull) return fail(c, PQ_EINVAL, "n_obs must be in [1, 2^32 - 1)");
+    return guarded(c, [&]() -> int {
+        cudaStream_t user = static_cast<cudaStream_t>(stream);
+        cudaEvent_t ev;
+        ck(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming), "event");
+        ck(cudaEventRecord(ev, user), "event");
+        ck(cudaStreamWaitEvent(c->stream, ev, 0), "event");
+        const int rc = fuzzy_run(c, n, nnz, d_indptr, d_indices, d_data, d_out_indptr,
+                                 d_out_indices, d_out_weights, out_cap, nnz_out, c->stream);
+        ck(cudaEventRecord(ev, c->stream), "event");
+        ck(cudaStreamWaitEvent(user, ev, 0), "event");
+        cudaEventDestroy(ev);
+        return rc;
     });
 }
 
