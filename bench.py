@@ -63,6 +63,18 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(torch, value: float, device, world: int) -> float:
+    """The largest of every rank's value (per-step times are reported as the
+    slowest rank's); a no-op on one rank."""
+    if world <= 1:
+        return value
+    import torch.distributed as dist
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload(args, rank):
     from polariseq_b200 import synth
 
@@ -284,13 +296,7 @@ def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, wor
     torch.cuda.synchronize(dev)
     barrier()
     _lib.load().pq_ctx_set_profiling(ctx._h, 0)
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        import torch.distributed as dist
-
-        t = torch.tensor([ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(torch, e0.elapsed_time(e1) / args.steps, dev, world)
     names = _lib.KERNEL_GROUPS
     per = {names[g]: {"ms_per_build": float(kg_ms[g] / args.steps),
                       "launches_per_build": int(kg_l[g] // args.steps)}
@@ -383,11 +389,7 @@ def main():
     e2e_steps = max(1, min(args.steps, 3))
     for _ in range(e2e_steps):
         r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
-    e2e_ms = (time.perf_counter() - t0) * 1000.0 / e2e_steps
-    if world > 1:
-        t = torch.tensor([e2e_ms], device=dev, dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(torch, (time.perf_counter() - t0) * 1000.0 / e2e_steps, dev, world)
     e2e = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(x.nbytes),
            "d2h_bytes_per_step": int(4 * (n + 1) + 8 * r["nnz"]), "steps": e2e_steps}
