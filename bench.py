@@ -209,10 +209,12 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel,
-# from an ncu capture of the same kernel (profiles/k_ivf_tiles_*.md); the
-# traffic of a launch scales with the tile pairs it processes.
-TILE_DRAM_BYTES_PER_PAIR = None
+# DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel:
+# an ncu capture of its two passes at 1M x 50 (profiles/k_ivf_tiles_1m.md) read
+# and wrote 0.481 GB over 184,341 tile pairs (primary pass) and 5.240 GB over
+# 1,258,220 (other probes), 3,966 bytes per pair over both; a launch's traffic
+# is taken to scale with the tile pairs it processes.
+TILE_DRAM_BYTES_PER_PAIR = 3966.0
 
 
 def tiles_roofline(per, st, args, peaks):
@@ -349,8 +351,10 @@ def main():
         for _ in range(args.warmup + args.steps):
             ctx.nndescent_device(xd, opts, ip, ix, dx, stream=stream.cuda_stream)
         torch.cuda.synchronize(dev)
+        st = ctx.stats()
         print(json.dumps({"profile_only": True, "n": n, "form": args.form,
-                          "ms_total": ctx.stats()["ms_total"]}), flush=True)
+                          "ms_total": st["ms_total"], "shortlist": st.get("shortlist")}),
+              flush=True)
         return
 
     peaks = {}

@@ -309,7 +309,7 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
                                size_t ne, int P, uint32_t C, const uint32_t* __restrict__ probes,
                                const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpoint,
                                uint32_t* __restrict__ qbucket, uint32_t* __restrict__ qself,
-                               uint32_t* __restrict__ entry_of) {
+                               uint32_t* __restrict__ entry_of, uint32_t* __restrict__ slot) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= ne) return;
     const uint64_t v = vals[e];
@@ -320,6 +320,7 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
     qbucket[e] = b;
     qself[e] = b == probes[size_t(i) * P] ? pos_of[i] : 0xFFFFFFFFu;
     entry_of[v] = uint32_t(e);
+    slot[e] = uint32_t(v);
     (void)r;
 }
 
@@ -377,9 +378,9 @@ template <int D>
 __global__ void __launch_bounds__(128) k_rerank(
     const float* __restrict__ X, int d, int dp, uint32_t n, int k, int P, int SO, int RS, int R,
     const uint32_t* __restrict__ entry_of, const float* __restrict__ sd,
-    const uint32_t* __restrict__ si, const uint32_t* __restrict__ perm,
-    uint32_t* __restrict__ out_idx, float* __restrict__ out_dist,
-    unsigned long long* boundary_fixes) {
+    const uint32_t* __restrict__ si, const uint8_t* __restrict__ sn,
+    const uint32_t* __restrict__ perm, uint32_t* __restrict__ out_idx,
+    float* __restrict__ out_dist, unsigned long long* boundary_fixes) {
     __shared__ uint32_t band_i[4][64];
     __shared__ double band_d[4][64];
     __shared__ float band_f[4][64];
@@ -389,30 +390,22 @@ __global__ void __launch_bounds__(128) k_rerank(
     if (wg >= n) return;
     const uint32_t i = perm[wg];
     // 1. the R best approximate candidates of the shortlist runs (lane L <
-    //    P * NR owns run L % NR of probe L / NR; runs are RS long, ascending,
-    //    an entry's NR runs RS * NR apart).  Each lane loads its run at once;
-    //    the finite entries (a prefix of each run) are gathered into shared
-    //    memory and sorted as (distance bits, position) keys — 64 at most,
-    //    else the runs are merged head by head.
+    //    P * NR owns run L % NR of probe L / NR; runs are RS long (a multiple
+    //    of 4), ascending, an entry's NR runs RS * NR apart, and the first
+    //    sn[cell * P * NR + L] entries of run L are its finite ones).  The
+    //    live prefixes are copied into shared memory (four entries per vector
+    //    load, all issued at once) and sorted as (distance bits, position)
+    //    keys — 64 at most, else the runs are merged head by head.
     const int NR = SO / RS;
     const bool owner = lane < P * NR;
     size_t base = 0;
-    if (owner) base = size_t(entry_of[size_t(i) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
-    uint32_t cand[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
-    float rv[32];
-    uint32_t ri[32];
     int fin = 0;
-#pragma unroll
-    for (int j = 0; j < 32; ++j) {
-        rv[j] = __int_as_float(0x7f800000);
-        ri[j] = 0xFFFFFFFFu;
-        if (j < RS && owner) {
-            rv[j] = sd[base + j];
-            ri[j] = si[base + j];
-        }
-        fin += (ri[j] != 0xFFFFFFFFu && rv[j] < __int_as_float(0x7f800000)) ? 1 : 0;
+    if (owner) {
+        base = size_t(entry_of[size_t(i) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
+        fin = sn[size_t(i) * P * NR + lane];
     }
-    int off = fin;  // inclusive prefix sum of the finite counts
+    uint32_t cand[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
+    int off = fin;  // inclusive prefix sum of the live counts
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
         const int t = __shfl_up_sync(0xFFFFFFFFu, off, o);
@@ -425,10 +418,24 @@ __global__ void __launch_bounds__(128) k_rerank(
         slot[lane] = ~0ull;
         slot[lane + 32] = ~0ull;
         __syncwarp();
+        float4 v4[8];
+        uint4 i4[8];
 #pragma unroll
-        for (int j = 0; j < 32; ++j)
-            if (j < fin)
-                slot[off + j] = (uint64_t(__float_as_uint(fmaxf(rv[j], 0.0f))) << 32) | ri[j];
+        for (int q = 0; q < 8; ++q)
+            if (4 * q < fin) {
+                v4[q] = *reinterpret_cast<const float4*>(sd + base + 4 * q);
+                i4[q] = *reinterpret_cast<const uint4*>(si + base + 4 * q);
+            }
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const float vv[4] = {v4[q].x, v4[q].y, v4[q].z, v4[q].w};
+            const uint32_t ii[4] = {i4[q].x, i4[q].y, i4[q].z, i4[q].w};
+#pragma unroll
+            for (int t = 0; t < 4; ++t)
+                if (4 * q + t < fin)
+                    slot[off + 4 * q + t] =
+                        (uint64_t(__float_as_uint(fmaxf(vv[t], 0.0f))) << 32) | ii[t];
+        }
         __syncwarp();
         uint64_t key[2] = {slot[lane], slot[lane + 32]};
         __syncwarp();
@@ -441,7 +448,7 @@ __global__ void __launch_bounds__(128) k_rerank(
         for (int t = 0; t < R; ++t) {
             float v = __int_as_float(0x7f800000);
             uint32_t id = 0xFFFFFFFFu;
-            if (owner && head < uint32_t(RS)) {
+            if (head < uint32_t(fin)) {
                 v = sd[base + head];
                 id = si[base + head];
             }
@@ -767,8 +774,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* qbucket = c->get<uint32_t>("qbucket", ne);
     uint32_t* qself = c->get<uint32_t>("qself", ne);
     uint32_t* entry_of = c->get<uint32_t>("entry_of", ne);
+    uint32_t* eslot = c->get<uint32_t>("entry_slot", ne);  // entry -> cell * P + probe rank
     k_entry_layout<<<blocks(ne, 256), 256, 0, st>>>(evals, ekeys, ne, P, C, probes, pos_of,
-                                                     qpoint, qbucket, qself, entry_of); count_launch();
+                                                     qpoint, qbucket, qself, entry_of, eslot);
+    count_launch();
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
     k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, C, 2 * C, q_off); count_launch();
     __nv_bfloat16* qb = nullptr;
@@ -830,6 +839,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (fp8 && Ssh > 16) throw DeviceError{"the E4M3 form supports k <= 15"};
     float* sd = c->get<float>("sl_d", ne * Sout);
     uint32_t* si = c->get<uint32_t>("sl_i", ne * Sout);
+    // live length of each run, cell-major: [cell * P + probe rank][run]
+    uint8_t* sn = c->get<uint8_t>("sl_n", ne * ivf_groups());
     {
         CUtensorMap tq, tcm;
         const bool maps = fp8 ? make_fp8_map(&tq, qb8, ne, 128) && make_fp8_map(&tcm, xc8, n, 256)
@@ -887,6 +898,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.drain_at = pass == 0 ? drain_at0 : 0;
             a.out_d = sd;
             a.out_i = si;
+            a.out_n = sn;
+            a.out_slot = eslot;
             a.err = c->d_err;
             a.trace = tbuf;
             {
@@ -933,10 +946,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         KGScope kg(c, PQ_KG_RERANK);
         if (d == 50)
             k_rerank<50><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
-                                                       si, perm, ridx, rdist, c->d_acc);
+                                                       si, sn, perm, ridx, rdist, c->d_acc);
         else
             k_rerank<0><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
-                                                      si, perm, ridx, rdist, c->d_acc);
+                                                      si, sn, perm, ridx, rdist, c->d_acc);
         count_launch();
     }
     unsigned long long fixes = 0;

@@ -33,7 +33,8 @@
 //                      per-thread append buffer drained into a shared-memory
 //                      max-heap of S (one heap per row and column half).
 // At job end each thread sorts its heap in registers and writes one ascending
-// run of S: the output row of an entry is NG runs of S.
+// run of S: the output row of an entry is NG runs of S (and, when asked, the
+// number of finite entries of each run).
 //
 // Every wait is bounded: a wait that gives up raises the CTA's abort flag,
 // every role leaves its loop, in-flight copies and MMAs are waited for (again
@@ -128,15 +129,16 @@ __device__ __forceinline__ float shortlist_insert(float* hd, uint32_t* hi, int S
     return hd[0];
 }
 
-// Ascending bitonic sort of S register pairs by (value, id).
-template <int S>
-__device__ __forceinline__ void sort_pairs(float (&v)[S], uint32_t (&id)[S]) {
+// Ascending bitonic sort of the first N of S register pairs by (value, id)
+// (N a power of two, N <= S).
+template <int N, int S>
+__device__ __forceinline__ void sort_prefix(float (&v)[S], uint32_t (&id)[S]) {
 #pragma unroll
-    for (int size = 2; size <= S; size <<= 1)
+    for (int size = 2; size <= N; size <<= 1)
 #pragma unroll
         for (int stride = size >> 1; stride > 0; stride >>= 1)
 #pragma unroll
-            for (int i = 0; i < S; ++i) {
+            for (int i = 0; i < N; ++i) {
                 const int j = i ^ stride;
                 if (j > i) {
                     const bool up = (i & size) == 0;
@@ -475,11 +477,14 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             }
             // job end: the entries (the buffer alone when it never spilled into
             // the heap and fits the run, else the heap after a drain) sorted in
-            // registers, written as one ascending run of S
+            // registers, written as one ascending run of S.  Only the warp's
+            // longest live prefix is sorted (a direct row holds cnt entries, a
+            // heap S): the other places hold +inf in every row of the warp
             long long c3 = t0 ? clock64() : 0;
             const bool direct = !heaped && cnt <= S;
             if (!direct) drain();
             if (t0) c_end_drain += clock64() - c3;
+            const int m = int(__reduce_max_sync(FULL, uint32_t(direct ? cnt : S)));
             if (valid) {
                 float kv[S];
                 uint32_t ki[S];
@@ -487,11 +492,28 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 const uint32_t* si_ = direct ? bi : hi;
 #pragma unroll
                 for (int j = 0; j < S; ++j) {
-                    const bool live = !direct || j < cnt;
+                    const bool live = j < m && (!direct || j < cnt);
                     kv[j] = live ? sd_[j * TQ] : __int_as_float(0x7f800000);
                     ki[j] = live ? si_[j * TQ] : 0xFFFFFFFFu;
                 }
-                sort_pairs<S>(kv, ki);
+                if constexpr (S >= 8) {
+                    if (m <= 4)
+                        sort_prefix<4, S>(kv, ki);
+                    else if (m <= 8)
+                        sort_prefix<8, S>(kv, ki);
+                    else if (m <= S / 2)
+                        sort_prefix<S / 2, S>(kv, ki);
+                    else
+                        sort_prefix<S, S>(kv, ki);
+                } else {
+                    sort_prefix<S, S>(kv, ki);
+                }
+                if (a.out_n) {
+                    int live = 0;
+#pragma unroll
+                    for (int j = 0; j < S; ++j) live += kv[j] < __int_as_float(0x7f800000) ? 1 : 0;
+                    a.out_n[size_t(a.out_slot ? a.out_slot[entry] : entry) * NG + g] = uint8_t(live);
+                }
                 if constexpr (S % 4 == 0) {
                     float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
                     uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);

@@ -33,6 +33,10 @@ struct IvfTileArgs {
     const float* chalf;
     float* out_d;            // entries x (ivf_groups() x S): ascending runs of S
     uint32_t* out_i;         // the candidate positions (~0 = none)
+    // optional: the number of finite entries of each run (a prefix), written
+    // to out_n[out_slot[entry] * ivf_groups() + half] (out_slot null: entry)
+    uint8_t* out_n;
+    const uint32_t* out_slot;
     int* err;
     unsigned long long* trace;  // optional: block 0 cycle counters (IVF_T_*)
 };
