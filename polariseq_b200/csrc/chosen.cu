@@ -682,9 +682,24 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         a.out_d = c->get<float>("arun_d", size_t(nq) * 2 * 16);
         a.out_i = c->get<uint32_t>("arun_i", size_t(nq) * 2 * 16);
         a.err = c->d_err;
+        if (std::getenv("POLARISEQ_TRACE")) {
+            a.trace = c->get<unsigned long long>("ivf_trace", IVF_TRACE_N);
+            ck(cudaMemsetAsync(a.trace, 0, IVF_TRACE_N * 8, st), "trace");
+        }
         ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "centroid tiles");
         k_merge_runs<<<blocks(nq, 256), 256, 0, st>>>(a.out_d, a.out_i, nq, sr, s_out, od, oi); count_launch();
         ck(cudaStreamSynchronize(st), "centroid tiles");  // the host job arrays are reused
+        if (a.trace) {
+            unsigned long long h[IVF_TRACE_N];
+            ck(cudaMemcpy(h, a.trace, sizeof(h), cudaMemcpyDeviceToHost), "trace");
+            std::fprintf(stderr,
+                         "[chosen] centroid search (%u queries, S %d) block 0: jobs %llu tiles %llu "
+                         "| cycles epi-wait %llu epi-work %llu epi-end %llu flagged-chunk %llu "
+                         "total %llu | warp 0: slow chunks %llu admits %llu\n",
+                         nq, sr, h[IVF_T_JOBS], h[IVF_T_TILES], h[IVF_T_EPI_WAIT],
+                         h[IVF_T_EPI_WORK], h[IVF_T_EPI_END], h[IVF_T_SLOW_CYC], h[IVF_T_TOTAL],
+                         h[IVF_T_SLOW], h[IVF_T_ADMITS]);
+        }
     };
     ck(cudaMemsetAsync(c->d_err, 0, 4, st), "err");
     const int lloyd = 8;
@@ -859,9 +874,6 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         // 2k-th seed to four digits, with 16% fewer tile-kernel cycles)
         // (the E4M3 ranking error is larger: 2k places)
         const int R0 = std::min(Sout, fp8 ? 2 * k : k + 2);
-        // the primary pass starts without a bound and admits often: drain at
-        // half a buffer so that its bound tightens sooner
-        const int drain_at0 = 16;
         for (int pass = 0; pass < 2; ++pass) {
             const uint32_t nj = uint32_t(jb[pass].size());
             if (nj == 0) continue;
@@ -895,7 +907,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.qthr = pass ? qthr : nullptr;
             a.qself = qself;
             a.S = Ssh;
-            a.drain_at = pass == 0 ? drain_at0 : 0;
+            a.buffered = pass;  // the other probes start from the primary's bound
             a.out_d = sd;
             a.out_i = si;
             a.out_n = sn;
@@ -915,15 +927,14 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                 unsigned long long h[IVF_TRACE_N];
                 ck(cudaMemcpy(h, tbuf, sizeof(h), cudaMemcpyDeviceToHost), "trace");
                 std::fprintf(stderr,
-                             "[chosen] pass %d tiles block 0: jobs %llu tiles %llu drains %llu | "
-                             "cycles epi-wait %llu epi-work %llu epi-end %llu mma-wait-c %llu "
-                             "mma-wait-t %llu tma-wait %llu total %llu | warp 0: slow chunks %llu "
-                             "admits %llu union bits %llu end-drain cycles %llu\n",
-                             pass, h[IVF_T_JOBS], h[IVF_T_TILES], h[IVF_T_DRAINS],
-                             h[IVF_T_EPI_WAIT], h[IVF_T_EPI_WORK], h[IVF_T_EPI_END],
-                             h[IVF_T_MMA_WAIT_C], h[IVF_T_MMA_WAIT_T], h[IVF_T_TMA_WAIT],
-                             h[IVF_T_TOTAL], h[IVF_T_SLOW], h[IVF_T_ADMITS], h[IVF_T_WMBITS],
-                             h[IVF_T_END_DRAIN]);
+                             "[chosen] pass %d tiles block 0: jobs %llu tiles %llu | cycles "
+                             "epi-wait %llu epi-work %llu epi-end %llu mma-wait-c %llu mma-wait-t "
+                             "%llu tma-wait %llu total %llu | warp 0: slow chunks %llu admits %llu "
+                             "union bits %llu flagged-chunk cycles %llu\n",
+                             pass, h[IVF_T_JOBS], h[IVF_T_TILES], h[IVF_T_EPI_WAIT],
+                             h[IVF_T_EPI_WORK], h[IVF_T_EPI_END], h[IVF_T_MMA_WAIT_C],
+                             h[IVF_T_MMA_WAIT_T], h[IVF_T_TMA_WAIT], h[IVF_T_TOTAL], h[IVF_T_SLOW],
+                             h[IVF_T_ADMITS], h[IVF_T_WMBITS], h[IVF_T_SLOW_CYC]);
             }
         }
     }

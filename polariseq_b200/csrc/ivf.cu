@@ -20,21 +20,24 @@
 // warp-specialised roles and mbarrier hand-offs, no CTA-wide barrier inside
 // the loop:
 //   warp 8 (one lane)  TMA loads: the job's Q tile (2 stages) and candidate
-//                      tiles (2-3 stages, 128-byte swizzled, K-major);
+//                      tiles (3 stages, 128-byte swizzled, K-major);
 //   warp 9 (one lane)  tcgen05.mma M=128 N=256 K=16 x4 into one of two TMEM
 //                      accumulator buffers (256 columns each); commits free
 //                      the candidate stage and fill the TMEM buffer;
 //   warps 0-7          epilogue: warp w reads TMEM lanes 32(w%4).. (its query
-//                      rows) for column half w/4 (tcgen05.ld 32x32b) and
-//                      filters; the few flagged chunks are re-read by one
-//                      compact (not unrolled) admission loop, so the rarely
-//                      run code stays small in the instruction cache; then the
-//                      TMEM buffer is freed.  Admitted entries go to a
-//                      per-thread append buffer drained into a shared-memory
-//                      max-heap of S (one heap per row and column half).
-// At job end each thread sorts its heap in registers and writes one ascending
-// run of S: the output row of an entry is NG runs of S (and, when asked, the
-// number of finite entries of each run).
+//                      rows) for column half w/4 (tcgen05.ld 32x32b), 32
+//                      columns at a time, and filters; in a chunk that some
+//                      row admits, each lane takes its admitted columns, then
+//                      the TMEM buffer is freed.
+// Each thread keeps its row's shortlist for its column half in registers: S
+// (distance, candidate) pairs in ascending order, a new entry shifting the
+// worse ones up by one place (S - 1 compare-and-selects, no memory traffic).
+// Launches that start unbounded insert every admitted column at once, so the
+// bound tightens with each insertion; seeded launches (few admissions) stage
+// them in a shared-memory buffer merged when it fills and at job end.  At job
+// end the shortlist is written as it stands: the output row of an entry is NG
+// ascending runs of S (and, when asked, the number of finite entries of each
+// run).
 //
 // Every wait is bounded: a wait that gives up raises the CTA's abort flag,
 // every role leaves its loop, in-flight copies and MMAs are waited for (again
@@ -55,7 +58,7 @@ constexpr int NG = 2;     // epilogue warpgroups: each owns half of a tile's col
 constexpr int NEPI = TQ * NG;   // epilogue threads
 constexpr int NT = NEPI + 64;   // + TMA warp + MMA warp
 constexpr int CPG = TCN / NG;   // columns per warpgroup
-constexpr int BUF = 32;         // append buffer entries per (row, warpgroup)
+constexpr int BUF = 32;         // staged admissions per (row, column half), buffered mode
 constexpr int QST = 2;          // Q tile stages
 constexpr int MAXCS = 3;        // candidate tile stages (at most)
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
@@ -101,61 +104,26 @@ __device__ __forceinline__ uint32_t select32(const uint32_t (&x)[32], int j) {
     return (j & 1) ? d[1] : d[0];
 }
 
-// Replace the root of a max-heap of S shortlist entries (one thread's column of
-// a transposed shared-memory tile, entries TQ apart) and sift down; returns
-// the new root (the shortlist's current worst).
-__device__ __forceinline__ float shortlist_insert(float* hd, uint32_t* hi, int S, float d,
-                                                  uint32_t id) {
-    int p = 0;
-    for (;;) {
-        const int l = 2 * p + 1;
-        if (l >= S) break;
-        int c = l;
-        float vc = hd[l * TQ];
-        if (l + 1 < S) {
-            const float vr = hd[(l + 1) * TQ];
-            if (vr > vc) {
-                c = l + 1;
-                vc = vr;
-            }
-        }
-        if (!(vc > d)) break;
-        hd[p * TQ] = vc;
-        hi[p * TQ] = hi[c * TQ];
-        p = c;
+// Inserts (d, id) into an ascending register shortlist of S entries (the
+// caller checked d < v[S - 1]): the entries after it move up one place and
+// the last one drops out.  Equal distances keep their arrival order.
+template <int S>
+__device__ __forceinline__ void shortlist_push(float (&v)[S], uint32_t (&x)[S], float d,
+                                               uint32_t id) {
+#pragma unroll
+    for (int j = S - 1; j > 0; --j) {
+        const bool up = d < v[j - 1];
+        const bool here = !up && d < v[j];
+        v[j] = up ? v[j - 1] : (here ? d : v[j]);
+        x[j] = up ? x[j - 1] : (here ? id : x[j]);
     }
-    hd[p * TQ] = d;
-    hi[p * TQ] = id;
-    return hd[0];
+    if (d < v[0]) {
+        v[0] = d;
+        x[0] = id;
+    }
 }
 
-// Ascending bitonic sort of the first N of S register pairs by (value, id)
-// (N a power of two, N <= S).
-template <int N, int S>
-__device__ __forceinline__ void sort_prefix(float (&v)[S], uint32_t (&id)[S]) {
-#pragma unroll
-    for (int size = 2; size <= N; size <<= 1)
-#pragma unroll
-        for (int stride = size >> 1; stride > 0; stride >>= 1)
-#pragma unroll
-            for (int i = 0; i < N; ++i) {
-                const int j = i ^ stride;
-                if (j > i) {
-                    const bool up = (i & size) == 0;
-                    const bool gt = v[i] > v[j] || (v[i] == v[j] && id[i] > id[j]);
-                    if (gt == up) {
-                        const float tv = v[i];
-                        v[i] = v[j];
-                        v[j] = tv;
-                        const uint32_t ti = id[i];
-                        id[i] = id[j];
-                        id[j] = ti;
-                    }
-                }
-            }
-}
-
-__host__ __device__ constexpr int cand_stages(int S, bool f8) { return S <= 16 && !f8 ? 3 : 2; }
+__host__ __device__ constexpr int cand_stages(int, bool) { return 3; }
 
 template <int S, bool F8>
 __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUtensorMap tmQ,
@@ -167,10 +135,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     uint8_t* smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
     uint8_t* sQ = smem;                                          // QST x 16 KB
     uint8_t* sC = sQ + QST * TQ * ROWB;                          // NCS x 32 KB
-    float* hdall = reinterpret_cast<float*>(sC + NCS * TCN * ROWB);         // NG x S x TQ
-    uint32_t* hiall = reinterpret_cast<uint32_t*>(hdall + NG * S * TQ);     // NG x S x TQ
-    float* bdall = reinterpret_cast<float*>(hiall + NG * S * TQ);           // NG x BUF x TQ
-    uint32_t* biall = reinterpret_cast<uint32_t*>(bdall + NG * BUF * TQ);   // NG x BUF x TQ
+    float* bdall = reinterpret_cast<float*>(sC + NCS * TCN * ROWB);        // NG x BUF x TQ
+    uint32_t* biall = reinterpret_cast<uint32_t*>(bdall + NG * BUF * TQ);  // NG x BUF x TQ
     // E4M3 only: |x~|^2 / 2 of the tile's columns, per TMEM buffer parity and
     // column half (the four warps of a half write the same values)
     float* hsall = reinterpret_cast<float*>(biall + NG * BUF * TQ);        // 2 x NG x CPG
@@ -219,7 +185,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
                 const uint32_t nct = (ce - cs + TCN - 1) / TCN;
                 // tiles run from the job's start tile, wrapping around
-                const uint32_t t0 = (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
+                const uint32_t tfirst = (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
                 if (nct == 0) continue;
                 const int qsd = int(qi % QST);
                 long long c0 = clock64();
@@ -240,7 +206,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                     }
                     c_wait += clock64() - c0;
                     tc::mbar_expect_tx(&B.c_full[s], TCN * ROWB);
-                    const uint32_t tt = t0 + t >= nct ? t0 + t - nct : t0 + t;
+                    const uint32_t tt = tfirst + t >= nct ? tfirst + t - nct : tfirst + t;
                     tc::tma_load_2d(sC + s * TCN * ROWB, &tmC, &B.c_full[s], 0, int(cs + tt * TCN));
                     ++ci;
                 }
@@ -323,18 +289,12 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
         const int g = w >> 2;
         const int row = (w & 3) * 32 + lane;
         const uint32_t lane_base = uint32_t((w & 3) * 32) << 16;
-        float* hd = hdall + size_t(g) * S * TQ + row;
-        uint32_t* hi = hiall + size_t(g) * S * TQ + row;
+        const bool t0 = tracing && tid == 0;
+        const bool buffered = a.buffered != 0;
         float* bd = bdall + size_t(g) * BUF * TQ + row;
         uint32_t* bi = biall + size_t(g) * BUF * TQ + row;
-        const bool t0 = tracing && tid == 0;
-        // drain once some lane's buffer would pass this fill: early drains
-        // tighten the admission bound sooner where admissions are frequent
-        const uint32_t drain_at = a.drain_at > 0 && a.drain_at < BUF ? uint32_t(a.drain_at)
-                                                                     : uint32_t(BUF);
-        long long c_wait = 0, c_work = 0, c_end = 0;
-        unsigned long long drains = 0, jobs = 0, slow = 0, admits = 0, wmbits = 0;
-        long long c_end_drain = 0;
+        long long c_wait = 0, c_work = 0, c_end = 0, c_slow = 0;
+        unsigned long long jobs = 0, slow = 0, admits = 0, wmbits = 0;
         uint32_t ti = 0;
         for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
             const uint32_t b = a.job_bucket[job];
@@ -342,7 +302,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
             const uint32_t nct = (ce - cs + TCN - 1) / TCN;
             // tiles run from the job's start tile, wrapping around
-            const uint32_t t0 = (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
+            const uint32_t tfirst =
+                (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
             const uint32_t entry = qs + row;
             const bool valid = entry < qe;
             // an invalid row's infinite |q|^2 makes its bound +inf or NaN: it
@@ -354,19 +315,23 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             float ath = (qn - thr) * 0.5f;
             // E4M3: the accumulator's scale back to the dot product of the rows
             const float rq = F8 && valid ? a.qscale[entry] * a.bscale[b] : 1.0f;
-            int cnt = 0;
-            bool heaped = false;  // the heap holds entries (a drain moved some there)
-#pragma unroll 4
+            // the shortlist: S ascending (distance, candidate) pairs in registers
+            float sv[S];
+            uint32_t sx[S];
+#pragma unroll
             for (int j = 0; j < S; ++j) {
-                hd[j * TQ] = __int_as_float(0x7f800000);
-                hi[j * TQ] = 0xFFFFFFFFu;
+                sv[j] = __int_as_float(0x7f800000);
+                sx[j] = 0xFFFFFFFFu;
             }
-            // drain this lane's append buffer into its heap
-            auto drain = [&]() {
-                heaped = heaped || cnt > 0;
-                for (int t = 0; t < cnt; ++t) {
-                    const float v = bd[t * TQ];
-                    if (v < thr) thr = fminf(thr0, shortlist_insert(hd, hi, S, v, bi[t * TQ]));
+            int cnt = 0;  // staged entries (buffered mode)
+            // merge the staged entries into the shortlist
+            auto flush = [&]() {
+                for (int u = 0; u < cnt; ++u) {
+                    const float d = bd[u * TQ];
+                    if (d < thr) {
+                        shortlist_push<S>(sv, sx, d, bi[u * TQ]);
+                        thr = fminf(thr0, sv[S - 1]);
+                    }
                 }
                 cnt = 0;
                 ath = (qn - thr) * 0.5f;
@@ -381,11 +346,9 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 tc::tc_fence_after();
                 const uint32_t tcol = taddr + lane_base + uint32_t(tb * TCN + g * CPG);
                 // columns of this slice that belong to the bucket
-                const uint32_t tt = t0 + t >= nct ? t0 + t - nct : t0 + t;
+                const uint32_t tt = tfirst + t >= nct ? tfirst + t - nct : tfirst + t;
                 const int lim = int(ce) - int(cs + tt * TCN + g * CPG);
                 const uint32_t cbase = cs + tt * TCN + g * CPG;
-                // the slice's four 32-column chunks from registers: one max and
-                // one vote each; a chunk some row admits is handled on the spot
                 long long c1 = t0 ? clock64() : 0;
                 float* hs = hsall + (tb * NG + g) * CPG;
                 if constexpr (F8) {
@@ -396,30 +359,26 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                     }
                     __syncwarp();
                 }
-                // two chunks in registers at a time (64 registers), so that a
-                // flagged chunk is handled from registers without spills
-#pragma unroll
-                for (int q2 = 0; q2 < CPG / 32; q2 += 2) {
-                uint32_t r[2][32];
-                tc::tmem_ld32(tcol + uint32_t(q2 * 32), r[0]);
-                tc::tmem_ld32(tcol + uint32_t(q2 * 32 + 32), r[1]);
-                tc::tmem_ld_wait();
-#pragma unroll
-                for (int qq = 0; qq < 2; ++qq) {
-                    const int q = q2 + qq;
+                // the slice's four 32-column chunks, one at a time: one max and
+                // one vote each; a chunk some row admits is handled on the spot
+#pragma unroll 1
+                for (int q = 0; q < CPG / 32; ++q) {
+                    uint32_t r[32];
+                    tc::tmem_ld32(tcol + uint32_t(q * 32), r);
+                    tc::tmem_ld_wait();
                     float v[32];
                     if constexpr (F8) {
 #pragma unroll
                         for (int j = 0; j < 32; j += 4) {
                             const float4 h4 = *reinterpret_cast<const float4*>(hs + q * 32 + j);
-                            v[j] = fmaf(__uint_as_float(r[qq][j]), rq, -h4.x);
-                            v[j + 1] = fmaf(__uint_as_float(r[qq][j + 1]), rq, -h4.y);
-                            v[j + 2] = fmaf(__uint_as_float(r[qq][j + 2]), rq, -h4.z);
-                            v[j + 3] = fmaf(__uint_as_float(r[qq][j + 3]), rq, -h4.w);
+                            v[j] = fmaf(__uint_as_float(r[j]), rq, -h4.x);
+                            v[j + 1] = fmaf(__uint_as_float(r[j + 1]), rq, -h4.y);
+                            v[j + 2] = fmaf(__uint_as_float(r[j + 2]), rq, -h4.z);
+                            v[j + 3] = fmaf(__uint_as_float(r[j + 3]), rq, -h4.w);
                         }
                     } else {
 #pragma unroll
-                        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[qq][j]);
+                        for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
                     }
                     if (lim < (q + 1) * 32) {
 #pragma unroll
@@ -427,45 +386,55 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                             if (q * 32 + j >= lim) v[j] = __int_as_float(0xff800000);
                     }
                     if (!__any_sync(FULL, max32(v) > ath)) continue;
+                    const long long cs0 = t0 ? clock64() : 0;
                     uint32_t lm = 0;  // this lane's admitted columns
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
                         if (v[j] > ath) lm |= 1u << j;
-                    if (__reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > drain_at) {
-                        ++drains;
-                        drain();  // cnt = 0, and at most 32 admissions follow
-                    }
-                    if (t0) ++slow;
                     if (tracing) {
                         const uint32_t na = __reduce_add_sync(FULL, uint32_t(__popc(lm)));
                         const uint32_t wm = __reduce_or_sync(FULL, lm);
                         if (t0) {
+                            ++slow;
                             admits += na;
                             wmbits += __popc(wm);
                         }
                     }
-                    // each lane appends its own admitted columns, lowest first
+                    // each lane takes its admitted columns, lowest first: into
+                    // the shortlist at once (each checked against the bound its
+                    // predecessors tightened), or staged (buffered mode; the
+                    // buffer is merged first when this chunk could overflow it)
+                    if (buffered &&
+                        __reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > uint32_t(BUF))
+                        flush();
                     const uint32_t cb0 = cbase + q * 32;
                     while (__any_sync(FULL, lm != 0)) {
                         if (lm) {
                             const int j = __ffs(lm) - 1;
                             lm &= lm - 1;
-                            if (cb0 + j != qself) {
-                                float vj = __uint_as_float(select32(r[qq], j));
-                                if constexpr (F8) vj = fmaf(vj, rq, -hs[q * 32 + j]);
-                                bd[cnt * TQ] = fmaf(-2.0f, vj, qn);
-                                bi[cnt * TQ] = cb0 + j;
-                                ++cnt;
+                            float vj = __uint_as_float(select32(r, j));
+                            if constexpr (F8) vj = fmaf(vj, rq, -hs[q * 32 + j]);
+                            const float dj = fmaf(-2.0f, vj, qn);
+                            if (dj < thr && cb0 + j != qself) {
+                                if (buffered) {
+                                    bd[cnt * TQ] = dj;
+                                    bi[cnt * TQ] = cb0 + j;
+                                    ++cnt;
+                                } else {
+                                    shortlist_push<S>(sv, sx, dj, cb0 + j);
+                                    thr = fminf(thr0, sv[S - 1]);
+                                    ath = (qn - thr) * 0.5f;
+                                }
                             }
                         }
                     }
-                }
+                    if (t0) c_slow += clock64() - cs0;
                 }
                 tc::tc_fence_before();
                 __syncwarp();
                 if (lane == 0) tc::mbar_arrive(&B.t_empty[tb]);
                 ++ti;
-                if (t0) {  // epi-wait: wait + fast filter; epi-work: admissions
+                if (t0) {  // epi-wait: wait; epi-work: filter and admissions
                     const long long c2 = clock64();
                     c_wait += c1 - c0;
                     c_work += c2 - c1;
@@ -475,59 +444,31 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 *abort_flag = 1;
                 break;
             }
-            // job end: the entries (the buffer alone when it never spilled into
-            // the heap and fits the run, else the heap after a drain) sorted in
-            // registers, written as one ascending run of S.  Only the warp's
-            // longest live prefix is sorted (a direct row holds cnt entries, a
-            // heap S): the other places hold +inf in every row of the warp
+            // job end: the shortlist (staged entries merged) is one ascending
+            // run of S
             long long c3 = t0 ? clock64() : 0;
-            const bool direct = !heaped && cnt <= S;
-            if (!direct) drain();
-            if (t0) c_end_drain += clock64() - c3;
-            const int m = int(__reduce_max_sync(FULL, uint32_t(direct ? cnt : S)));
+            if (cnt > 0) flush();
             if (valid) {
-                float kv[S];
-                uint32_t ki[S];
-                const float* sd_ = direct ? bd : hd;
-                const uint32_t* si_ = direct ? bi : hi;
-#pragma unroll
-                for (int j = 0; j < S; ++j) {
-                    const bool live = j < m && (!direct || j < cnt);
-                    kv[j] = live ? sd_[j * TQ] : __int_as_float(0x7f800000);
-                    ki[j] = live ? si_[j * TQ] : 0xFFFFFFFFu;
-                }
-                if constexpr (S >= 8) {
-                    if (m <= 4)
-                        sort_prefix<4, S>(kv, ki);
-                    else if (m <= 8)
-                        sort_prefix<8, S>(kv, ki);
-                    else if (m <= S / 2)
-                        sort_prefix<S / 2, S>(kv, ki);
-                    else
-                        sort_prefix<S, S>(kv, ki);
-                } else {
-                    sort_prefix<S, S>(kv, ki);
-                }
-                if (a.out_n) {
-                    int live = 0;
-#pragma unroll
-                    for (int j = 0; j < S; ++j) live += kv[j] < __int_as_float(0x7f800000) ? 1 : 0;
-                    a.out_n[size_t(a.out_slot ? a.out_slot[entry] : entry) * NG + g] = uint8_t(live);
-                }
                 if constexpr (S % 4 == 0) {
                     float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
                     uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
 #pragma unroll
                     for (int j = 0; j < S / 4; ++j) {
-                        od[j] = make_float4(kv[4 * j], kv[4 * j + 1], kv[4 * j + 2], kv[4 * j + 3]);
-                        oi[j] = make_uint4(ki[4 * j], ki[4 * j + 1], ki[4 * j + 2], ki[4 * j + 3]);
+                        od[j] = make_float4(sv[4 * j], sv[4 * j + 1], sv[4 * j + 2], sv[4 * j + 3]);
+                        oi[j] = make_uint4(sx[4 * j], sx[4 * j + 1], sx[4 * j + 2], sx[4 * j + 3]);
                     }
                 } else {
 #pragma unroll
                     for (int j = 0; j < S; ++j) {
-                        a.out_d[(size_t(entry) * NG + g) * S + j] = kv[j];
-                        a.out_i[(size_t(entry) * NG + g) * S + j] = ki[j];
+                        a.out_d[(size_t(entry) * NG + g) * S + j] = sv[j];
+                        a.out_i[(size_t(entry) * NG + g) * S + j] = sx[j];
                     }
+                }
+                if (a.out_n) {
+                    int live = 0;
+#pragma unroll
+                    for (int j = 0; j < S; ++j) live += sv[j] < __int_as_float(0x7f800000) ? 1 : 0;
+                    a.out_n[size_t(a.out_slot ? a.out_slot[entry] : entry) * NG + g] = uint8_t(live);
                 }
             }
             ++jobs;
@@ -537,12 +478,11 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             a.trace[IVF_T_EPI_WAIT] = (unsigned long long)c_wait;
             a.trace[IVF_T_EPI_WORK] = (unsigned long long)c_work;
             a.trace[IVF_T_EPI_END] = (unsigned long long)c_end;
-            a.trace[IVF_T_DRAINS] = drains;
             a.trace[IVF_T_JOBS] = jobs;
             a.trace[IVF_T_SLOW] = slow;
             a.trace[IVF_T_ADMITS] = admits;
             a.trace[IVF_T_WMBITS] = wmbits;
-            a.trace[IVF_T_END_DRAIN] = (unsigned long long)c_end_drain;
+            a.trace[IVF_T_SLOW_CYC] = (unsigned long long)c_slow;
         }
     }
     __syncthreads();
@@ -574,7 +514,7 @@ EncodeTiledFn encode_fn() {
 template <int S, bool F8>
 size_t tiles_smem() {
     return 1024 + size_t(QST) * TQ * ROWB + size_t(cand_stages(S, F8)) * TCN * ROWB +
-           size_t(NG) * S * TQ * 8 + size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * NG * CPG * 4 : 0);
+           size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * NG * CPG * 4 : 0);
 }
 
 template <int S, bool F8>

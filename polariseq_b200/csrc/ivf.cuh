@@ -23,7 +23,11 @@ struct IvfTileArgs {
     const float* qthr;       // optional per query entry: initial admission bound
     const uint32_t* qself;   // per query entry: its own candidate position, or ~0
     int S;                   // shortlist length per entry and column half: 1, 16 or 32
-    int drain_at;            // buffer fill that triggers a drain into the heap (0: full)
+    // 1: admitted entries are staged in a shared-memory buffer and merged
+    // into the shortlist when it fills and at job end (for launches whose
+    // bound starts tight, qthr, so that admissions are rare); 0: each is
+    // inserted at once, tightening the bound (launches that start unbounded)
+    int buffered;
     // E4M3 tiles (the maps hold 128 one-byte columns per row, no norm
     // columns): the accumulator times qscale[entry] * bscale[bucket] is the
     // dot product, and chalf[candidate] = |x~|^2 / 2 is subtracted in FP32
@@ -42,9 +46,9 @@ struct IvfTileArgs {
 };
 
 enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT_C = 3,
-       IVF_T_MMA_WAIT_T = 4, IVF_T_TMA_WAIT = 5, IVF_T_TILES = 6, IVF_T_DRAINS = 7,
-       IVF_T_TOTAL = 8, IVF_T_JOBS = 9, IVF_T_SLOW = 10, IVF_T_ADMITS = 11, IVF_T_WMBITS = 12,
-       IVF_T_END_DRAIN = 13, IVF_TRACE_N = 16 };
+       IVF_T_MMA_WAIT_T = 4, IVF_T_TMA_WAIT = 5, IVF_T_TILES = 6, IVF_T_TOTAL = 7,
+       IVF_T_JOBS = 8, IVF_T_SLOW = 9, IVF_T_ADMITS = 10, IVF_T_WMBITS = 11,
+       IVF_T_SLOW_CYC = 12, IVF_TRACE_N = 16 };
 
 bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
 // A [rows x 128] one-byte (E4M3) matrix as 128-byte-swizzled boxes of box_rows x 128.
