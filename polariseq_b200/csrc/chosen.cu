@@ -73,18 +73,34 @@ __global__ void k_kmeans_accumulate(const float* __restrict__ xs, uint32_t ns, i
 // candidate tile; the others follow by (probe bucket, the cell's primary
 // bucket), so that a job's queries come from one neighbouring bucket and meet
 // the candidates on that side of the probe bucket first.
-__global__ void k_entry_keys(const uint32_t* __restrict__ probes, size_t ne, int P, uint32_t C,
+// Entry e = (candidate position p, probe rank r), p = e / P, of cell
+// perm[p]: key (primary entries) = the cell's candidate key, (others) =
+// (C + probe bucket) * C + primary bucket; value = cell * P + r.  Generated in
+// candidate order, so that after the stable sort the entries of one (probe,
+// primary) pair follow the primary bucket's candidate order.
+__global__ void k_entry_keys(const uint32_t* __restrict__ probes,
+                             const uint32_t* __restrict__ perm, size_t ne, int P, uint32_t C,
                              uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= ne) return;
-    const size_t i = e / P;
-    const uint32_t r = uint32_t(e - i * P);
+    const size_t p = e / P;
+    const uint32_t r = uint32_t(e - p * P);
+    const size_t i = perm[p];
     const uint32_t a = probes[i * P];
     if (r == 0)
         keys[e] = a * C + (P > 1 ? probes[i * P + 1] : 0u);
     else
-        keys[e] = (C + probes[e]) * C + a;
-    vals[e] = e;
+        keys[e] = (C + probes[i * P + r]) * C + a;
+    vals[e] = i * P + r;
+}
+
+// The embedding rows in candidate order (xp[p] = X[perm[p]], dp floats each).
+__global__ void k_gather_rows(const float4* __restrict__ X, const uint32_t* __restrict__ perm,
+                              uint32_t n, int dq, float4* __restrict__ xp) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(n) * dq) return;
+    const size_t p = t / dq;
+    xp[t] = X[size_t(perm[p]) * dq + (t - p * dq)];
 }
 
 // First candidate tile of each job of the non-primary pass: where the probe
@@ -210,7 +226,7 @@ __global__ void k_bucket_absmax(const float* __restrict__ X, int d, int dp,
     const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (r >= n) return;
-    const uint32_t i = perm[r], b = cbucket[r];
+    const uint32_t i = perm ? perm[r] : uint32_t(r), b = cbucket[r];
     float m = 0.f;
     for (int j = lane; j < d; j += 32)
         m = fmaxf(m, fabsf(X[size_t(i) * dp + j] - cent[size_t(b) * dp + j]));
@@ -243,7 +259,7 @@ __global__ void k_to_fp8(const float* __restrict__ X, int d, int dp,
     const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (r >= rows) return;
-    const uint32_t i = src[r], c = cid[r];
+    const uint32_t i = src ? src[r] : uint32_t(r), c = cid[r];
     float v[4];
     float m = 0.f;
 #pragma unroll
@@ -307,7 +323,7 @@ __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n, uin
 
 __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t* __restrict__ keys,
                                size_t ne, int P, uint32_t C, const uint32_t* __restrict__ probes,
-                               const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpoint,
+                               const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpos,
                                uint32_t* __restrict__ qbucket, uint32_t* __restrict__ qself,
                                uint32_t* __restrict__ entry_of, uint32_t* __restrict__ slot) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -316,9 +332,10 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
     const uint32_t i = uint32_t(v / P), r = uint32_t(v % P);
     const uint32_t kb = keys[e] / C;
     const uint32_t b = kb >= C ? kb - C : kb;
-    qpoint[e] = i;
+    const uint32_t pos = pos_of[i];
+    qpos[e] = pos;
     qbucket[e] = b;
-    qself[e] = b == probes[size_t(i) * P] ? pos_of[i] : 0xFFFFFFFFu;
+    qself[e] = b == probes[size_t(i) * P] ? pos : 0xFFFFFFFFu;
     entry_of[v] = uint32_t(e);
     slot[e] = uint32_t(v);
     (void)r;
@@ -376,7 +393,8 @@ __device__ __forceinline__ double sq_dist_f64(const float* a, const float* b, in
 // nearest (ascending) per cell.
 template <int D>
 __global__ void __launch_bounds__(128) k_rerank(
-    const float* __restrict__ X, int d, int dp, uint32_t n, int k, int P, int SO, int RS, int R,
+    const float* __restrict__ X, const float* __restrict__ xp, int d, int dp, uint32_t n, int k,
+    int P, int SO, int RS, int R,
     const uint32_t* __restrict__ entry_of, const float* __restrict__ sd,
     const uint32_t* __restrict__ si, const uint8_t* __restrict__ sn,
     const uint32_t* __restrict__ perm, uint32_t* __restrict__ out_idx,
@@ -472,14 +490,15 @@ __global__ void __launch_bounds__(128) k_rerank(
         }
     }
     // 2. exact FP32 distances (reference order) of this lane's candidates
-    const float* xi = X + size_t(i) * dp;
+    //    (rows from the candidate-ordered copy: this cell is position wg)
+    const float* xi = xp + size_t(wg) * dp;
     uint64_t key[2];
 #pragma unroll
     for (int h = 0; h < 2; ++h) {
         key[h] = ~0ull;
         if (cand[h] != 0xFFFFFFFFu) {
             const uint32_t j = perm[cand[h]];
-            const float dd = sq_dist_exact_t<D>(xi, X + size_t(j) * dp, d);
+            const float dd = sq_dist_exact_t<D>(xi, xp + size_t(cand[h]) * dp, d);
             key[h] = (uint64_t(__float_as_uint(dd)) << 32) | j;
         }
     }
@@ -736,7 +755,6 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint64_t* evals = c->get<uint64_t>("evals", ne);
     uint32_t* ekeys2 = c->get<uint32_t>("ekeys2", ne);
     uint64_t* evals2 = c->get<uint64_t>("evals2", ne);
-    k_entry_keys<<<blocks(ne, 256), 256, 0, st>>>(probes, ne, P, C, ekeys, evals); count_launch();
     kg_sec.reset();
     S_.ms_forest = tm.stop();
 
@@ -761,6 +779,13 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
     uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
     k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, pos_of, cbucket); count_launch();
+    // the embedding in candidate order: the conversions below and the re-rank
+    // read it in runs instead of gathering rows
+    float* xp = c->get<float>("xp_f32", size_t(n) * dp);
+    k_gather_rows<<<blocks(size_t(n) * (dp / 4), 256), 256, 0, st>>>(
+        reinterpret_cast<const float4*>(X), perm, n, dp / 4, reinterpret_cast<float4*>(xp));
+    count_launch();
+    k_entry_keys<<<blocks(ne, 256), 256, 0, st>>>(probes, perm, ne, P, C, ekeys, evals); count_launch();
     const bool fp8 = o.mode == PQ_MODE_FP8;
     __nv_bfloat16* xc = nullptr;
     uint32_t* xc8 = nullptr;
@@ -769,29 +794,29 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (!fp8) {
         xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
         float* xcn = c->get<float>("xc_norm", n);
-        k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, 2, xc, xcn); count_launch();
+        k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, 2, xc, xcn); count_launch();
     } else {
         unsigned* amax = c->get<unsigned>("bucket_amax", C);
         ck(cudaMemsetAsync(amax, 0, size_t(C) * 4, st), "amax");
-        k_bucket_absmax<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, amax); count_launch();
+        k_bucket_absmax<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax); count_launch();
         bscale = c->get<float>("bucket_scale", C);
         k_bucket_scale<<<blocks(C, 256), 256, 0, st>>>(amax, C, bscale); count_launch();
         xc8 = c->get<uint32_t>("xc_fp8", size_t(n) * 32);
         xch = c->get<float>("xc_half", n);
-        k_to_fp8<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, perm, cbucket, cent, n, amax, xc8,
+        k_to_fp8<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax, xc8,
                                                 nullptr, xch, 0.5f); count_launch();
     }
     // query entries grouped by probe bucket (stable: cell order within a bucket)
     ck(radix_sort_pairs(ekeys, evals, ekeys2, evals2, ne, key_bits(2 * uint64_t(C) * C - 1),
                         c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
        "sort entries");
-    uint32_t* qpoint = c->get<uint32_t>("qpoint", ne);
+    uint32_t* qpos = c->get<uint32_t>("qpos", ne);  // entry -> its cell's candidate position
     uint32_t* qbucket = c->get<uint32_t>("qbucket", ne);
     uint32_t* qself = c->get<uint32_t>("qself", ne);
     uint32_t* entry_of = c->get<uint32_t>("entry_of", ne);
     uint32_t* eslot = c->get<uint32_t>("entry_slot", ne);  // entry -> cell * P + probe rank
     k_entry_layout<<<blocks(ne, 256), 256, 0, st>>>(evals, ekeys, ne, P, C, probes, pos_of,
-                                                     qpoint, qbucket, qself, entry_of, eslot);
+                                                     qpos, qbucket, qself, entry_of, eslot);
     count_launch();
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
     k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, C, 2 * C, q_off); count_launch();
@@ -801,11 +826,11 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     float* qbn = c->get<float>("q_norm", ne);
     if (!fp8) {
         qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
-        k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, 1, qb, qbn); count_launch();
+        k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(xp, d, dp, qpos, qbucket, cent, ne, 1, qb, qbn); count_launch();
     } else {
         qb8 = c->get<uint32_t>("q_fp8", ne * 32);
         qscale = c->get<float>("q_scale", ne);
-        k_to_fp8<<<blocks(ne, 8), 256, 0, st>>>(X, d, dp, qpoint, qbucket, cent, ne, nullptr, qb8,
+        k_to_fp8<<<blocks(ne, 8), 256, 0, st>>>(xp, d, dp, qpos, qbucket, cent, ne, nullptr, qb8,
                                                  qscale, qbn, 1.0f); count_launch();
     }
     std::vector<uint32_t> hq(2 * C + 1);
@@ -956,10 +981,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     {
         KGScope kg(c, PQ_KG_RERANK);
         if (d == 50)
-            k_rerank<50><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
+            k_rerank<50><<<blocks(n, 4), 128, 0, st>>>(X, xp, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
                                                        si, sn, perm, ridx, rdist, c->d_acc);
         else
-            k_rerank<0><<<blocks(n, 4), 128, 0, st>>>(X, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
+            k_rerank<0><<<blocks(n, 4), 128, 0, st>>>(X, xp, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
                                                       si, sn, perm, ridx, rdist, c->d_acc);
         count_launch();
     }
