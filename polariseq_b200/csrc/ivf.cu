@@ -185,7 +185,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
                 const uint32_t nct = (ce - cs + TCN - 1) / TCN;
                 // tiles run from the job's start tile, wrapping around
-                const uint32_t tfirst = (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
+                const uint32_t tfirst =
+                    (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
                 if (nct == 0) continue;
                 const int qsd = int(qi % QST);
                 long long c0 = clock64();
@@ -467,8 +468,10 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 if (a.out_n) {
                     int live = 0;
 #pragma unroll
-                    for (int j = 0; j < S; ++j) live += sv[j] < __int_as_float(0x7f800000) ? 1 : 0;
-                    a.out_n[size_t(a.out_slot ? a.out_slot[entry] : entry) * NG + g] = uint8_t(live);
+                    for (int j = 0; j < S; ++j)
+                        live += sv[j] < __int_as_float(0x7f800000) ? 1 : 0;
+                    const uint32_t sl = a.out_slot ? a.out_slot[entry] : entry;
+                    a.out_n[size_t(sl) * NG + g] = uint8_t(live);
                 }
             }
             ++jobs;
