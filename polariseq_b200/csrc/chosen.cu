@@ -160,39 +160,59 @@ __global__ void k_kmeans_update(float* __restrict__ cent, const float* __restric
 // squared norms computed in FP32 from the rounded values.  Columns d and d+1
 // carry the augmentation of the tensor-core tiles: -1/2, -1/2 for a query row
 // (aug 1), and hi, lo with hi + lo = the row's norm for a candidate row (aug 2).
+// A half-warp per row (lane h: columns 4h..4h+3, one 16-byte load of the row
+// and of the centre, one 8-byte store), grid-stride over the rows; needs
+// dp <= 64 and d <= 62.
 __global__ void k_to_bf16(const float* __restrict__ X, int d, int dp,
                           const uint32_t* __restrict__ src, const uint32_t* __restrict__ cid,
                           const float* __restrict__ cent, size_t rows, int aug,
                           __nv_bfloat16* __restrict__ out, float* __restrict__ norm) {
-    const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (r >= rows) return;
-    const uint32_t i = src ? src[r] : uint32_t(r);
-    const uint32_t c = cid ? cid[r] : 0u;
-    float s = 0.f;
-    __nv_bfloat16 bv[2];
+    const int h = threadIdx.x & 15;
+    const unsigned hm = 0xFFFFu << (threadIdx.x & 16);  // this half-warp's lanes
+    const size_t nh = (size_t(gridDim.x) * blockDim.x) >> 4;
+    for (size_t r = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 4; r < rows; r += nh) {
+        const uint32_t i = src ? src[r] : uint32_t(r);
+        const uint32_t c = cid ? cid[r] : 0u;
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        if (4 * h < dp) {
+            const float4 x4 = *reinterpret_cast<const float4*>(X + size_t(i) * dp + 4 * h);
+            const float4 c4 = *reinterpret_cast<const float4*>(cent + size_t(c) * dp + 4 * h);
+            v[0] = x4.x - c4.x;
+            v[1] = x4.y - c4.y;
+            v[2] = x4.z - c4.z;
+            v[3] = x4.w - c4.w;
+        }
+        __nv_bfloat16 bv[4];
+        float s = 0.f;
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int j = lane + 32 * h;
-        float v = 0.f;
-        if (j < d) v = X[size_t(i) * dp + j] - (cent ? cent[size_t(c) * dp + j] : 0.f);
-        bv[h] = __float2bfloat16_rn(v);
-        const float f = __bfloat162float(bv[h]);
-        s = fmaf(f, f, s);
-    }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-    const __nv_bfloat16 hi = __float2bfloat16_rn(s);
-    const __nv_bfloat16 lo = __float2bfloat16_rn(s - __bfloat162float(hi));
+        for (int u = 0; u < 4; ++u) {
+            bv[u] = __float2bfloat16_rn(4 * h + u < d ? v[u] : 0.f);
+            const float f = __bfloat162float(bv[u]);
+            s = fmaf(f, f, s);
+        }
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int j = lane + 32 * h;
-        __nv_bfloat16 o = bv[h];
-        if (aug == 1 && (j == d || j == d + 1)) o = __float2bfloat16_rn(-0.5f);
-        if (aug == 2 && j == d) o = hi;
-        if (aug == 2 && j == d + 1) o = lo;
-        out[r * 64 + j] = o;
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(hm, s, o);
+        const __nv_bfloat16 hi = __float2bfloat16_rn(s);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(s - __bfloat162float(hi));
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int j = 4 * h + u;
+            if (aug == 1 && (j == d || j == d + 1)) bv[u] = __float2bfloat16_rn(-0.5f);
+            if (aug == 2 && j == d) bv[u] = hi;
+            if (aug == 2 && j == d + 1) bv[u] = lo;
+        }
+        uint2 w;
+        w.x = uint32_t(__bfloat16_as_ushort(bv[0])) | (uint32_t(__bfloat16_as_ushort(bv[1])) << 16);
+        w.y = uint32_t(__bfloat16_as_ushort(bv[2])) | (uint32_t(__bfloat16_as_ushort(bv[3])) << 16);
+        *reinterpret_cast<uint2*>(out + r * 64 + 4 * h) = w;
+        if (h == 0) norm[r] = s;
     }
-    if (lane == 0) norm[r] = s;
+}
+
+// Grid of the BF16 conversion: 16 rows per 256-thread block, at most 4096 blocks.
+inline unsigned cvt_blocks(size_t rows) {
+    const size_t b = (rows + 15) / 16;
+    return unsigned(b < 4096 ? (b > 0 ? b : 1) : 4096);
 }
 
 // The s_out nearest of two ascending runs of S per row (distinct ids).
@@ -661,7 +681,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     k_sample_rows<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(xs, dp, ns, C, cent); count_launch();
     __nv_bfloat16* xsb = c->get<__nv_bfloat16>("km_sample_bf16", size_t(ns) * 64);
     float* xsn = c->get<float>("km_sample_norm", ns);
-    k_to_bf16<<<blocks(ns, 8), 256, 0, st>>>(xs, d, dp, nullptr, zeros, mean, ns, 1, xsb, xsn); count_launch();
+    k_to_bf16<<<cvt_blocks(ns), 256, 0, st>>>(xs, d, dp, nullptr, zeros, mean, ns, 1, xsb, xsn); count_launch();
     __nv_bfloat16* cb = c->get<__nv_bfloat16>("cent_bf16", size_t(C) * 64);
     float* cbn = c->get<float>("cent_norm", C);
     float* lab_d = c->get<float>("km_lab_d", ns);
@@ -723,18 +743,18 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     ck(cudaMemsetAsync(c->d_err, 0, 4, st), "err");
     const int lloyd = 8;
     for (int it = 0; it < lloyd; ++it) {
-        k_to_bf16<<<blocks(C, 8), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
+        k_to_bf16<<<cvt_blocks(C), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
         centroid_search(xsb, xsn, ns, 1, lab_d, lab);
         ck(cudaMemsetAsync(sums, 0, size_t(C) * dp * 4, st), "km");
         ck(cudaMemsetAsync(cnt, 0, size_t(C) * 4, st), "km");
         k_kmeans_accumulate<<<blocks(ns, 256), 256, 0, st>>>(xs, ns, d, dp, lab, sums, cnt); count_launch();
         k_kmeans_update<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(cent, sums, cnt, C, d, dp); count_launch();
     }
-    k_to_bf16<<<blocks(C, 8), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
+    k_to_bf16<<<cvt_blocks(C), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
     // every cell's P nearest centroids, ascending; the first is its primary bucket
     __nv_bfloat16* qa = c->get<__nv_bfloat16>("assign_q", size_t(n) * 64);
     float* qan = c->get<float>("assign_qn", n);
-    k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan); count_launch();
+    k_to_bf16<<<cvt_blocks(n), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan); count_launch();
     uint32_t* probes = c->get<uint32_t>("probes", size_t(n) * P);
     float* probe_d = c->get<float>("probe_d", size_t(n) * P);
     double ms_train = 0.0, ms_route = 0.0;
@@ -794,7 +814,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (!fp8) {
         xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
         float* xcn = c->get<float>("xc_norm", n);
-        k_to_bf16<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, 2, xc, xcn); count_launch();
+        k_to_bf16<<<cvt_blocks(n), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, 2, xc, xcn); count_launch();
     } else {
         unsigned* amax = c->get<unsigned>("bucket_amax", C);
         ck(cudaMemsetAsync(amax, 0, size_t(C) * 4, st), "amax");
@@ -826,7 +846,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     float* qbn = c->get<float>("q_norm", ne);
     if (!fp8) {
         qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
-        k_to_bf16<<<blocks(ne, 8), 256, 0, st>>>(xp, d, dp, qpos, qbucket, cent, ne, 1, qb, qbn); count_launch();
+        k_to_bf16<<<cvt_blocks(ne), 256, 0, st>>>(xp, d, dp, qpos, qbucket, cent, ne, 1, qb, qbn); count_launch();
     } else {
         qb8 = c->get<uint32_t>("q_fp8", ne * 32);
         qscale = c->get<float>("q_scale", ne);
