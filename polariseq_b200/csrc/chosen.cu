@@ -121,27 +121,31 @@ __global__ void k_job_tstart(const uint32_t* __restrict__ job_bucket,
 
 // Seed thresholds of the non-primary entries: the R-th best approximate
 // distance of the cell's primary shortlist (a candidate of another bucket can
-// only enter the cell's R best if it beats that).
+// only enter the cell's R best if it beats that); +inf when the primary
+// shortlist holds fewer than R.  sn holds the runs' live lengths, cell-major.
 __global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_t n, int P,
-                                  const float* __restrict__ sd, int S, int R,
-                                  float* __restrict__ qthr) {
+                                  const float* __restrict__ sd, const uint8_t* __restrict__ sn,
+                                  int S, int R, float* __restrict__ qthr) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t e0 = entry_of[size_t(i) * P];
-    // the R-th smallest of the entry's two ascending runs of S
+    // the R-th smallest of the entry's two ascending runs (live prefixes)
     const float* r0 = sd + size_t(e0) * 2 * S;
     const float* r1 = r0 + S;
+    const int n0 = sn[size_t(i) * P * 2], n1 = sn[size_t(i) * P * 2 + 1];
     int x = 0, y = 0;
     float t = __int_as_float(0x7f800000);
-    for (int o = 0; o < R && (x < S || y < S); ++o) {
-        const float vx = x < S ? r0[x] : __int_as_float(0x7f800000);
-        const float vy = y < S ? r1[y] : __int_as_float(0x7f800000);
-        if (vx <= vy) {
-            t = vx;
-            ++x;
-        } else {
-            t = vy;
-            ++y;
+    if (n0 + n1 >= R) {
+        for (int o = 0; o < R; ++o) {
+            const float vx = x < n0 ? r0[x] : __int_as_float(0x7f800000);
+            const float vy = y < n1 ? r1[y] : __int_as_float(0x7f800000);
+            if (vx <= vy) {
+                t = vx;
+                ++x;
+            } else {
+                t = vy;
+                ++y;
+            }
         }
     }
     qthr[e0] = __int_as_float(0x7f800000);
@@ -964,7 +968,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                 ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "ivf tiles");
             }
             if (pass == 0) {  // seed the other probes with the primary shortlist's R-th best
-                k_seed_thresholds<<<blocks(n, 256), 256, 0, st>>>(entry_of, n, P, sd, Ssh, R0, qthr);
+                k_seed_thresholds<<<blocks(n, 256), 256, 0, st>>>(entry_of, n, P, sd, sn, Ssh, R0,
+                                                                  qthr);
                 count_launch();
             }
             ck(cudaStreamSynchronize(st), "jobs");  // the host job arrays are reused

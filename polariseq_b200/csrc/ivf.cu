@@ -450,28 +450,34 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             long long c3 = t0 ? clock64() : 0;
             if (cnt > 0) flush();
             if (valid) {
-                if constexpr (S % 4 == 0) {
-                    float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
-                    uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
-#pragma unroll
-                    for (int j = 0; j < S / 4; ++j) {
-                        od[j] = make_float4(sv[4 * j], sv[4 * j + 1], sv[4 * j + 2], sv[4 * j + 3]);
-                        oi[j] = make_uint4(sx[4 * j], sx[4 * j + 1], sx[4 * j + 2], sx[4 * j + 3]);
-                    }
-                } else {
-#pragma unroll
-                    for (int j = 0; j < S; ++j) {
-                        a.out_d[(size_t(entry) * NG + g) * S + j] = sv[j];
-                        a.out_i[(size_t(entry) * NG + g) * S + j] = sx[j];
-                    }
-                }
+                // with run lengths asked for, only the live prefix is written
+                int live = S;
                 if (a.out_n) {
-                    int live = 0;
+                    live = 0;
 #pragma unroll
                     for (int j = 0; j < S; ++j)
                         live += sv[j] < __int_as_float(0x7f800000) ? 1 : 0;
                     const uint32_t sl = a.out_slot ? a.out_slot[entry] : entry;
                     a.out_n[size_t(sl) * NG + g] = uint8_t(live);
+                }
+                if constexpr (S % 4 == 0) {
+                    float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
+                    uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
+#pragma unroll
+                    for (int j = 0; j < S / 4; ++j)
+                        if (4 * j < live) {
+                            od[j] = make_float4(sv[4 * j], sv[4 * j + 1], sv[4 * j + 2],
+                                                sv[4 * j + 3]);
+                            oi[j] = make_uint4(sx[4 * j], sx[4 * j + 1], sx[4 * j + 2],
+                                               sx[4 * j + 3]);
+                        }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < S; ++j)
+                        if (j < live) {
+                            a.out_d[(size_t(entry) * NG + g) * S + j] = sv[j];
+                            a.out_i[(size_t(entry) * NG + g) * S + j] = sx[j];
+                        }
                 }
             }
             ++jobs;

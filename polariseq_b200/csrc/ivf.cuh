@@ -38,7 +38,8 @@ struct IvfTileArgs {
     float* out_d;            // entries x (ivf_groups() x S): ascending runs of S
     uint32_t* out_i;         // the candidate positions (~0 = none)
     // optional: the number of finite entries of each run (a prefix), written
-    // to out_n[out_slot[entry] * ivf_groups() + half] (out_slot null: entry)
+    // to out_n[out_slot[entry] * ivf_groups() + half] (out_slot null: entry);
+    // when given, only that prefix of the run is written
     uint8_t* out_n;
     const uint32_t* out_slot;
     int* err;
