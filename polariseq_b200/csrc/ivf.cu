@@ -297,14 +297,25 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
         long long c_wait = 0, c_work = 0, c_end = 0, c_slow = 0;
         unsigned long long jobs = 0, slow = 0, admits = 0, wmbits = 0;
         uint32_t ti = 0;
+        // each job's descriptor is loaded one job ahead, so that a job's start
+        // waits for one dependent load (the bucket's bounds), not two
+        uint32_t nb = 0, nqs = 0, nqe = 0, nts = 0;
+        auto load_job = [&](uint32_t j) {
+            if (j < a.njobs) {
+                nb = a.job_bucket[j];
+                nqs = a.job_qstart[j];
+                nqe = a.job_qend[j];
+                nts = a.job_tstart ? a.job_tstart[j] : 0u;
+            }
+        };
+        load_job(blockIdx.x);
         for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
-            const uint32_t b = a.job_bucket[job];
-            const uint32_t qs = a.job_qstart[job], qe = a.job_qend[job];
+            const uint32_t b = nb, qs = nqs, qe = nqe, ts = nts;
+            load_job(job + gridDim.x);
             const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
             const uint32_t nct = (ce - cs + TCN - 1) / TCN;
             // tiles run from the job's start tile, wrapping around
-            const uint32_t tfirst =
-                (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
+            const uint32_t tfirst = ts < nct ? ts : 0u;
             const uint32_t entry = qs + row;
             const bool valid = entry < qe;
             // an invalid row's infinite |q|^2 makes its bound +inf or NaN: it
@@ -312,6 +323,8 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             const float qn = valid ? a.qnorm[entry] : __int_as_float(0x7f800000);
             const uint32_t qself = valid ? a.qself[entry] : 0xFFFFFFFFu;
             const float thr0 = (valid && a.qthr) ? a.qthr[entry] : __int_as_float(0x7f800000);
+            // where the run length goes, loaded with the row's other inputs
+            const uint32_t slot = (valid && a.out_slot) ? a.out_slot[entry] : entry;
             float thr = thr0;
             float ath = (qn - thr) * 0.5f;
             // E4M3: the accumulator's scale back to the dot product of the rows
@@ -457,8 +470,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
 #pragma unroll
                     for (int j = 0; j < S; ++j)
                         live += sv[j] < __int_as_float(0x7f800000) ? 1 : 0;
-                    const uint32_t sl = a.out_slot ? a.out_slot[entry] : entry;
-                    a.out_n[size_t(sl) * NG + g] = uint8_t(live);
+                    a.out_n[size_t(slot) * NG + g] = uint8_t(live);
                 }
                 if constexpr (S % 4 == 0) {
                     float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
