@@ -12,12 +12,16 @@
 // stages 128 candidate rows at a time in shared memory, dimension-major with a
 // padded stride (coalesced reads, conflict-free lane access); each warp
 // computes QW queries x 32 candidates per step (lane = candidate, the queries
-// broadcast from shared memory as [dim][QW]) and keeps one bounded max-heap
-// of (distance, index) keys per query in shared memory with the sequential
-// rule (push while short, then replace the root when a key is smaller, lanes
-// visited in index order).  The final heap is sorted by a warp bitonic
-// network.  The tile shape (QW, NW) is chosen by an autotuner
-// that times each shape on the largest work items of the call.
+// broadcast from shared memory as [dim][QW]) and keeps, per query, the kp
+// smallest (distance, index) keys: with kp <= 256 (and at most 32 registers
+// of keys per lane) in registers, sorted across the warp's lanes — a key
+// below the k-th is inserted by one shuffle and KPL compare-and-selects per
+// lane, with no shared-memory round trips — otherwise in a bounded max-heap
+// in shared memory with the sequential rule (push while short, then replace
+// the root when a key is smaller, lanes visited in index order) and sorted
+// by a warp bitonic network at the end.  Either way the result is the exact k
+// smallest keys.  The tile shape (QW, NW) is chosen by an autotuner that
+// times each shape on the largest work items of the call.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -102,7 +106,33 @@ __device__ __forceinline__ void sort_keys(uint64_t* h, int len, int kp, int lane
         }
 }
 
-template <int DP, int QW, int NW>
+// Register selection (kp <= 32 * KPL): a query's kp best keys sorted
+// ascending across the warp, lane l holding places l*KPL .. l*KPL+KPL-1.  A new
+// key x (smaller than the k-th) shifts every larger key up one place, the
+// last lane's last place passing to the next lane: KPL compare-and-selects
+// per lane and one shuffle, no shared memory.
+template <int KPL>
+__device__ __forceinline__ void sorted_insert(uint64_t (&v)[KPL], uint64_t x, int lane) {
+    uint64_t prev = __shfl_up_sync(FULL, v[KPL - 1], 1);
+    if (lane == 0) prev = 0;
+#pragma unroll
+    for (int t = KPL - 1; t >= 0; --t) {
+        const uint64_t below = t > 0 ? v[t - 1] : prev;
+        v[t] = x < below ? below : (x < v[t] ? x : v[t]);
+    }
+}
+// The key at place k-1 (the k-th smallest), broadcast to the warp.
+template <int KPL>
+__device__ __forceinline__ uint64_t kth_key(const uint64_t (&v)[KPL], int k) {
+    const int p = k - 1, owner = p / KPL, place = p - owner * KPL;
+    uint64_t mine = v[0];
+#pragma unroll
+    for (int t = 1; t < KPL; ++t)
+        if (place == t) mine = v[t];
+    return __shfl_sync(FULL, mine, owner);
+}
+
+template <int DP, int QW, int NW, int KPL>
 __global__ void __launch_bounds__(NW * 32) k_batched_knn(BatchArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     float* sq = reinterpret_cast<float*>(smem);          // NW x DP x QW (dim-major per warp)
@@ -129,8 +159,16 @@ __global__ void __launch_bounds__(NW * 32) k_batched_knn(BatchArgs a) {
             sq[t] = (q < ns && dim < a.d) ? a.X[(base + q) * uint64_t(a.d) + dim] : 0.0f;
         }
         int hlen[QW];
+        // register selection (KPL > 0): the sorted places and the k-th key
+        uint64_t kv[QW][KPL > 0 ? KPL : 1];
+        uint64_t thr[QW];
 #pragma unroll
-        for (int qi = 0; qi < QW; ++qi) hlen[qi] = 0;
+        for (int qi = 0; qi < QW; ++qi) {
+            hlen[qi] = 0;
+            thr[qi] = ~0ull;
+#pragma unroll
+            for (int t = 0; t < (KPL > 0 ? KPL : 1); ++t) kv[qi][t] = ~0ull;
+        }
         const float* qw = sq + w * DP * QW;
         for (uint32_t j0 = 0; j0 < ns; j0 += ET) {
             const uint32_t cnt = ns - j0 < uint32_t(ET) ? ns - j0 : uint32_t(ET);
@@ -178,8 +216,23 @@ __global__ void __launch_bounds__(NW * 32) k_batched_knn(BatchArgs a) {
                 for (int qi = 0; qi < QW; ++qi) {
                     const uint32_t q = q0 + uint32_t(w * QW + qi);
                     if (q >= ns) continue;  // warp-uniform
-                    uint64_t* h = heaps + size_t(w * QW + qi) * kp;
                     const uint64_t key = dkey(acc[qi], j);
+                    if constexpr (KPL > 0) {
+                        // lanes below the k-th key, in index order, each
+                        // re-checked against the k-th after an insertion
+                        uint32_t pending = live & ~__ballot_sync(FULL, j == q) &
+                                           __ballot_sync(FULL, key < thr[qi]);
+                        while (pending) {
+                            const int l = __ffs(pending) - 1;
+                            const uint64_t x = __shfl_sync(FULL, key, l);
+                            sorted_insert<KPL>(kv[qi], x, lane);
+                            thr[qi] = kth_key<KPL>(kv[qi], k);
+                            pending &= (l == 31) ? 0u : ~((2u << l) - 1u);
+                            pending &= __ballot_sync(FULL, key < thr[qi]);
+                        }
+                        continue;
+                    }
+                    uint64_t* h = heaps + size_t(w * QW + qi) * kp;
                     uint32_t pending = live & ~__ballot_sync(FULL, j == q);
                     // while short, every candidate is pushed in index order
                     while (pending && hlen[qi] < k) {
@@ -210,30 +263,51 @@ __global__ void __launch_bounds__(NW * 32) k_batched_knn(BatchArgs a) {
                 }
             }
         }
-        // sort each query's heap (padded to kp) and write its k nearest
-#pragma unroll 1
-        for (int qi = 0; qi < QW; ++qi) {
-            const uint32_t q = q0 + uint32_t(w * QW + qi);
-            if (q >= ns) continue;
-            uint64_t* h = heaps + size_t(w * QW + qi) * kp;
-            sort_keys(h, hlen[qi], kp, lane);
-            const uint64_t o = a.s_out[s] + uint64_t(q) * uint64_t(k);
-            for (int t = lane; t < k; t += 32) {
-                const uint64_t v = h[t];
-                const bool ok = t < hlen[qi];
-                a.out_idx[o + t] = ok ? uint32_t(v) : 0xFFFFFFFFu;
-                a.out_dist[o + t] =
-                    ok ? __fsqrt_rn(__uint_as_float(uint32_t(v >> 32))) : __int_as_float(0x7f800000);
+        // write each query's k nearest: the register places as they stand, or
+        // the heap sorted (padded to kp)
+        if constexpr (KPL > 0) {
+#pragma unroll
+            for (int qi = 0; qi < QW; ++qi) {
+                const uint32_t q = q0 + uint32_t(w * QW + qi);
+                if (q >= ns) continue;
+                const uint64_t o = a.s_out[s] + uint64_t(q) * uint64_t(k);
+#pragma unroll
+                for (int t = 0; t < KPL; ++t) {
+                    const int p = lane * KPL + t;
+                    if (p < k) {
+                        const uint64_t v = kv[qi][t];
+                        const bool ok = v != ~0ull;
+                        a.out_idx[o + p] = ok ? uint32_t(v) : 0xFFFFFFFFu;
+                        a.out_dist[o + p] = ok ? __fsqrt_rn(__uint_as_float(uint32_t(v >> 32)))
+                                               : __int_as_float(0x7f800000);
+                    }
+                }
             }
-            __syncwarp();
+        } else {
+#pragma unroll 1
+            for (int qi = 0; qi < QW; ++qi) {
+                const uint32_t q = q0 + uint32_t(w * QW + qi);
+                if (q >= ns) continue;
+                uint64_t* h = heaps + size_t(w * QW + qi) * kp;
+                sort_keys(h, hlen[qi], kp, lane);
+                const uint64_t o = a.s_out[s] + uint64_t(q) * uint64_t(k);
+                for (int t = lane; t < k; t += 32) {
+                    const uint64_t v = h[t];
+                    const bool ok = t < hlen[qi];
+                    a.out_idx[o + t] = ok ? uint32_t(v) : 0xFFFFFFFFu;
+                    a.out_dist[o + t] = ok ? __fsqrt_rn(__uint_as_float(uint32_t(v >> 32)))
+                                           : __int_as_float(0x7f800000);
+                }
+                __syncwarp();
+            }
         }
     }
 }
 
-template <int DP, int QW, int NW>
+template <int DP, int QW, int NW, int KPL>
 size_t smem_bytes(int kp) {
     return size_t(NW) * DP * QW * 4 + size_t((DP * ETP + 1) & ~1) * 4 +
-           size_t(NW) * QW * kp * 8;
+           (KPL > 0 ? 0 : size_t(NW) * QW * kp * 8);
 }
 
 struct Shape {
@@ -241,22 +315,39 @@ struct Shape {
 };
 constexpr Shape SHAPES[] = {{4, 4}, {8, 4}, {4, 8}, {8, 8}};
 
-template <int DP, int QW, int NW>
-cudaError_t launch_shape(const BatchArgs& a, int sms, cudaStream_t st) {
-    const size_t sm = smem_bytes<DP, QW, NW>(a.kp);
-    cudaError_t e = cudaFuncSetAttribute(k_batched_knn<DP, QW, NW>,
+template <int DP, int QW, int NW, int KPL>
+cudaError_t launch_kpl(const BatchArgs& a, int sms, cudaStream_t st) {
+    const size_t sm = smem_bytes<DP, QW, NW, KPL>(a.kp);
+    cudaError_t e = cudaFuncSetAttribute(k_batched_knn<DP, QW, NW, KPL>,
                                          cudaFuncAttributeMaxDynamicSharedMemorySize, int(sm));
     if (e != cudaSuccess) return e;
     int per_sm = 0;
-    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batched_knn<DP, QW, NW>,
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batched_knn<DP, QW, NW, KPL>,
                                                       NW * 32, sm);
     if (e != cudaSuccess) return e;
     if (per_sm < 1) return cudaErrorInvalidConfiguration;
     const uint32_t grid =
         uint32_t(std::min<uint64_t>(uint64_t(per_sm) * sms, std::max<uint32_t>(a.n_items, 1)));
-    k_batched_knn<DP, QW, NW><<<grid, NW * 32, sm, st>>>(a);
+    k_batched_knn<DP, QW, NW, KPL><<<grid, NW * 32, sm, st>>>(a);
     count_launch();
     return cudaGetLastError();
+}
+
+// Places per lane of the register selection for a heap capacity kp, 0 (the
+// shared-memory heap) when the QW queries' places would exceed 32 registers
+// of keys per lane.
+constexpr int reg_places(int qw, int kp) {
+    return kp <= 64 ? 2 : (kp <= 128 ? (qw * 4 <= 32 ? 4 : 0) : (kp <= 256 && qw * 8 <= 32 ? 8 : 0));
+}
+
+template <int DP, int QW, int NW>
+cudaError_t launch_shape(const BatchArgs& a, int sms, cudaStream_t st) {
+    switch (reg_places(QW, a.kp)) {
+        case 2: return launch_kpl<DP, QW, NW, 2>(a, sms, st);
+        case 4: return launch_kpl<DP, QW, NW, 4>(a, sms, st);
+        case 8: return launch_kpl<DP, QW, NW, 8>(a, sms, st);
+        default: return launch_kpl<DP, QW, NW, 0>(a, sms, st);
+    }
 }
 
 template <int DP>
@@ -278,8 +369,8 @@ int batched_queries_per_item(int shape) { return SHAPES[shape].qw * SHAPES[shape
 bool batched_shape_fits(int shape, int d, int kp) {
     const int DP = d <= 32 ? 32 : 64;
     const Shape sh = SHAPES[shape];
-    const size_t sm = size_t(sh.nw) * DP * sh.qw * 4 + size_t((DP * ETP + 1) & ~1) * 4 +
-                      size_t(sh.nw) * sh.qw * kp * 8;
+    const size_t heap = reg_places(sh.qw, kp) > 0 ? 0 : size_t(sh.nw) * sh.qw * kp * 8;
+    const size_t sm = size_t(sh.nw) * DP * sh.qw * 4 + size_t((DP * ETP + 1) & ~1) * 4 + heap;
     return sm <= 200 * 1024;
 }
 
