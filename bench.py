@@ -9,8 +9,9 @@ data standing in for a PCA embedding; no dataset is needed or available).
   e2e    cells/s through the C ABI with pinned HOST buffers: the embedding's
          host->device copy and the graph's device->host copy are inside the
          timed region
-  roofline  the dominant kernel group's algorithmic bytes per launch over its
-         CUDA-event duration, against the measured HBM copy bandwidth
+  roofline  the dominant kernel's algorithmic work per launch (flops for the
+         tensor-core tiles, bytes for the plain form's join) over its CUDA-event
+         duration, against the measured peak (sustained BF16 GEMM, HBM copy)
   cpu_baseline  the C++ restatement of the reference's CPU NN-Descent (oracle/)
          on a bounded sample of the same workload, all host threads
 
@@ -211,10 +212,10 @@ def run_reference(args):
 
 # DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel:
 # an ncu capture of its two passes at 1M x 50 (profiles/k_ivf_tiles_1m.md) read
-# and wrote 0.481 GB over 184,341 tile pairs (primary pass) and 5.240 GB over
-# 1,258,220 (other probes), 3,966 bytes per pair over both; a launch's traffic
+# and wrote 0.547 GB over 184,443 tile pairs (primary pass) and 2.823 GB over
+# 1,258,551 (other probes), 2,336 bytes per pair over both; a launch's traffic
 # is taken to scale with the tile pairs it processes.
-TILE_DRAM_BYTES_PER_PAIR = 3966.0
+TILE_DRAM_BYTES_PER_PAIR = 2336.0
 
 
 def tiles_roofline(per, st, args, peaks):
