@@ -84,7 +84,9 @@ typedef struct pq_nnd_stats {
     uint64_t kg_launches[16];
     /* Tensor-core form: [0] 128x256 tile pairs, [1] largest bucket, [2] buckets,
      * [3] (query entry, candidate) distances contracted, [4] / [5] tile pairs of
-     * the primary pass / the other probes, [6] FP64 boundary resolutions. */
+     * the primary pass / the other probes, [6] FP64 boundary resolutions,
+     * [7] other-probe entries dropped (a lower bound shows they can admit no
+     * candidate). */
     uint64_t shortlist[8];
     /* PQ_INIT_LEARNED: mean training loss of the first and of the last epoch
      * (the untrained router is the nearest-centroid prior), and the time of

@@ -125,7 +125,7 @@ __global__ void k_job_tstart(const uint32_t* __restrict__ job_bucket,
 // shortlist holds fewer than R.  sn holds the runs' live lengths, cell-major.
 __global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_t n, int P,
                                   const float* __restrict__ sd, const uint8_t* __restrict__ sn,
-                                  int S, int R, float* __restrict__ qthr) {
+                                  int S, int R, float* __restrict__ cseed) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const uint32_t e0 = entry_of[size_t(i) * P];
@@ -148,8 +148,142 @@ __global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_
             }
         }
     }
-    qthr[e0] = __int_as_float(0x7f800000);
-    for (int r = 1; r < P; ++r) qthr[entry_of[size_t(i) * P + r]] = t;
+    cseed[i] = t;
+}
+
+// Exact FP32 squared distance of every cell to each of its P probe centroids
+// (d[i * P + r]), and each bucket's squared radius over its own cells
+// (rad2[b] = max over cells whose primary is b; non-negative floats order as
+// their bits).  One warp per cell, lane r < P.
+template <int DQ>  // row length in float4s (0: dp / 4 at run time)
+__global__ void k_probe_dist(const float* __restrict__ X, int d, int dp, uint32_t n,
+                             const uint32_t* __restrict__ probes, int P,
+                             const float* __restrict__ cent, const float* __restrict__ un,
+                             float* __restrict__ dist, unsigned* __restrict__ rad2,
+                             unsigned* __restrict__ umax2) {
+    const uint32_t i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (i >= n || lane >= P) return;
+    const uint32_t c = probes[size_t(i) * P + lane];
+    const float* xi = X + size_t(i) * dp;
+    const float* cc = cent + size_t(c) * dp;
+    float s = 0.f;
+    if constexpr (DQ > 0) {
+        float4 xv[DQ], cv[DQ];
+#pragma unroll
+        for (int q = 0; q < DQ; ++q) {
+            xv[q] = reinterpret_cast<const float4*>(xi)[q];
+            cv[q] = reinterpret_cast<const float4*>(cc)[q];
+        }
+#pragma unroll
+        for (int q = 0; q < DQ; ++q) {
+            const float e[4] = {xv[q].x - cv[q].x, xv[q].y - cv[q].y, xv[q].z - cv[q].z,
+                                xv[q].w - cv[q].w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+                if (4 * q + u < d) s = fmaf(e[u], e[u], s);
+        }
+    } else {
+        for (int t = 0; t < d; ++t) {
+            const float df = xi[t] - cc[t];
+            s = fmaf(df, df, s);
+        }
+    }
+    dist[size_t(i) * P + lane] = s;
+    if (lane == 0) {
+        atomicMax(&rad2[c], __float_as_uint(s));
+        atomicMax(&umax2[c], __float_as_uint(un[i]));
+    }
+}
+
+// Exact distances between centroids: cd[a * C + b] = |c_a - c_b|.
+__global__ void k_cent_dist(const float* __restrict__ cent, uint32_t C, int d, int dp,
+                            float* __restrict__ cd) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(C) * C) return;
+    const size_t a = t / C, b = t - a * C;
+    float s = 0.f;
+    for (int j = 0; j < d; ++j) {
+        const float df = cent[a * dp + j] - cent[b * dp + j];
+        s = fmaf(df, df, s);
+    }
+    cd[t] = sqrtf(s);
+}
+
+// The largest of m non-negative floats (one block).
+__global__ void k_max_nonneg(const float* __restrict__ v, uint32_t m, unsigned* __restrict__ out) {
+    unsigned best = 0;
+    for (uint32_t t = threadIdx.x; t < m; t += blockDim.x) best = max(best, __float_as_uint(v[t]));
+    atomicMax(out, best);
+}
+
+// Which other-probe entries can hold a candidate that the tile pass would
+// admit.  Two exact lower bounds on |x - y| for every candidate y of bucket B
+// (x's own bucket A):
+//  - ball: y lies within B's radius r_B of c_B: |x - y| >= |x - c_B| - r_B;
+//  - bisector: y was assigned to B by BF16 distances (rows centred on the
+//    global mean, |y - mean| + |c - mean| <= U_B), so |y - c_B|^2 <=
+//    |y - c_A|^2 + delta with delta = 2^-6 (2 r_B + L) U_B + 2^-14 U_B^2
+//    (twice the rounding bound, using |y - c_A| <= r_B + L, L = |c_A - c_B|),
+//    and then |x - y| >= (|x - c_B|^2 - |x - c_A|^2 - delta) / (2 L).
+// The pass admits y only if its BF16 distance (rows centred on c_B) is below
+// the cell's seed; that distance is at least f(|x - y|^2) with
+// f(t) = t - 2^-6 sqrt(t) a - 2^-15 a^2 - 2^-9 (|x - c_B|^2 + r_B^2),
+// a = |x - c_B| + r_B (twice the worst case of the rounding of both rows to
+// BF16, each coordinate within 2^-8 relative, plus the FP32 accumulation and
+// the split norm columns), and f grows with t where it is positive.  So an
+// entry with f(lb^2) >= seed (lb the larger bound) admits nothing and is
+// dropped: keep[j] = 0.  Entries j are the sorted other-probe entries (key =
+// (C + B) * C + A, value = cell * P + rank); distances are FP32 (their
+// rounding is covered by the 2^-20 and 2^-18 terms).
+__global__ void k_prune_keep(const uint32_t* __restrict__ keys, const uint64_t* __restrict__ vals,
+                             size_t m, int P, uint32_t C, const float* __restrict__ dist,
+                             const unsigned* __restrict__ rad2, const unsigned* __restrict__ umax2,
+                             const unsigned* __restrict__ wmax2, const float* __restrict__ cd,
+                             const float* __restrict__ cseed, uint32_t* __restrict__ keep) {
+    const size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= m) return;
+    const uint64_t v = vals[j];
+    const uint64_t i = v / uint64_t(P);
+    const uint32_t key = keys[j];
+    const uint32_t b = key / C - C, pa = key % C;
+    const float dxb = dist[v], dxa = dist[i * P];
+    const float r2 = __uint_as_float(rad2[b]);
+    const float dx = sqrtf(dxb), rb = sqrtf(r2);
+    float lb = dx * (1.0f - 0x1p-20f) - rb * (1.0f + 0x1p-20f);
+    const float L = cd[size_t(pa) * C + b];
+    if (L > 0.f) {
+        const float ub = sqrtf(__uint_as_float(umax2[b])) + sqrtf(__uint_as_float(*wmax2));
+        const float delta = 0x1p-6f * (2.0f * rb + L) * ub + 0x1p-14f * ub * ub +
+                            0x1p-18f * (dxa + dxb);
+        lb = fmaxf(lb, (dxb - dxa - delta) / (2.0f * L * (1.0f + 0x1p-20f)));
+    }
+    uint32_t k = 1;
+    if (lb > 0.f) {
+        const float t = lb * lb, a = dx + rb;
+        const float f = t - 0x1p-6f * lb * a - 0x1p-15f * a * a - 0x1p-9f * (dxb + r2);
+        if (f >= cseed[i]) k = 0;
+    }
+    keep[j] = k;
+}
+
+// Stable compaction of the kept entries: pos = exclusive scan of keep.
+__global__ void k_compact_entries(const uint32_t* __restrict__ keys,
+                                  const uint64_t* __restrict__ vals, size_t m,
+                                  const uint32_t* __restrict__ keep,
+                                  const uint32_t* __restrict__ pos, uint32_t* __restrict__ okeys,
+                                  uint64_t* __restrict__ ovals) {
+    const size_t j = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (j >= m || !keep[j]) return;
+    okeys[pos[j]] = keys[j];
+    ovals[pos[j]] = vals[j];
+}
+
+// Admission bound of each laid-out other-probe entry: its cell's seed.
+__global__ void k_entry_thr(const uint32_t* __restrict__ slot, size_t m, int P,
+                            const float* __restrict__ cseed, float* __restrict__ qthr) {
+    const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e < m) qthr[e] = cseed[slot[e] / uint32_t(P)];
 }
 
 __global__ void k_kmeans_update(float* __restrict__ cent, const float* __restrict__ sums,
@@ -346,7 +480,8 @@ __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n, uin
 }
 
 __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t* __restrict__ keys,
-                               size_t ne, int P, uint32_t C, const uint32_t* __restrict__ probes,
+                               size_t ne, uint32_t e0, int P, uint32_t C,
+                               const uint32_t* __restrict__ probes,
                                const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpos,
                                uint32_t* __restrict__ qbucket, uint32_t* __restrict__ qself,
                                uint32_t* __restrict__ entry_of, uint32_t* __restrict__ slot) {
@@ -360,7 +495,7 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
     qpos[e] = pos;
     qbucket[e] = b;
     qself[e] = b == probes[size_t(i) * P] ? pos : 0xFFFFFFFFu;
-    entry_of[v] = uint32_t(e);
+    entry_of[v] = e0 + uint32_t(e);
     slot[e] = uint32_t(v);
     (void)r;
 }
@@ -830,7 +965,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         k_to_fp8<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax, xc8,
                                                 nullptr, xch, 0.5f); count_launch();
     }
-    // query entries grouped by probe bucket (stable: cell order within a bucket)
+    // query entries grouped by probe bucket (stable: cell order within a bucket);
+    // the n primary entries (keys below C * C) come first, in candidate order
     ck(radix_sort_pairs(ekeys, evals, ekeys2, evals2, ne, key_bits(2 * uint64_t(C) * C - 1),
                         c->get<uint8_t>("radix_c", radix_temp_bytes(std::max<size_t>(n, ne))), st),
        "sort entries");
@@ -839,59 +975,85 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* qself = c->get<uint32_t>("qself", ne);
     uint32_t* entry_of = c->get<uint32_t>("entry_of", ne);
     uint32_t* eslot = c->get<uint32_t>("entry_slot", ne);  // entry -> cell * P + probe rank
-    k_entry_layout<<<blocks(ne, 256), 256, 0, st>>>(evals, ekeys, ne, P, C, probes, pos_of,
-                                                     qpos, qbucket, qself, entry_of, eslot);
-    count_launch();
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
-    k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, C, 2 * C, q_off); count_launch();
     __nv_bfloat16* qb = nullptr;
     uint32_t* qb8 = nullptr;
     float* qscale = nullptr;
     float* qbn = c->get<float>("q_norm", ne);
     if (!fp8) {
         qb = c->get<__nv_bfloat16>("q_bf16", ne * 64);
-        k_to_bf16<<<cvt_blocks(ne), 256, 0, st>>>(xp, d, dp, qpos, qbucket, cent, ne, 1, qb, qbn); count_launch();
     } else {
         qb8 = c->get<uint32_t>("q_fp8", ne * 32);
         qscale = c->get<float>("q_scale", ne);
-        k_to_fp8<<<blocks(ne, 8), 256, 0, st>>>(xp, d, dp, qpos, qbucket, cent, ne, nullptr, qb8,
-                                                 qscale, qbn, 1.0f); count_launch();
     }
+    // the query entries [e0, e0 + m) laid out (from keys/vals) and their rows
+    // converted
+    auto lay_entries = [&](const uint32_t* keys, const uint64_t* vals, uint32_t e0, size_t m) {
+        if (m == 0) return;
+        k_entry_layout<<<blocks(m, 256), 256, 0, st>>>(vals, keys, m, e0, P, C, probes, pos_of,
+                                                       qpos + e0, qbucket + e0, qself + e0,
+                                                       entry_of, eslot + e0);
+        count_launch();
+        if (!fp8) {
+            k_to_bf16<<<cvt_blocks(m), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
+                                                      1, qb + size_t(e0) * 64, qbn + e0);
+        } else {
+            k_to_fp8<<<blocks(m, 8), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
+                                                    nullptr, qb8 + size_t(e0) * 32,
+                                                    qscale + e0, qbn + e0, 1.0f);
+        }
+        count_launch();
+    };
+    // primary entries now; the other probes after the primary pass, which
+    // bounds them
+    lay_entries(ekeys, evals, 0, n);
+    k_key_bounds<<<blocks(ne + 1, 256), 256, 0, st>>>(ekeys, ne, C, 2 * C, q_off); count_launch();
+    // exact distances of every cell to its probe centroids, bucket radii
+    float* pdist = c->get<float>("probe_dist", ne);
+    unsigned* rad2 = c->get<unsigned>("bucket_rad2", 2 * size_t(C) + 1);
+    unsigned* umax2 = rad2 + C;      // per bucket: max |y - mean|^2 of its cells
+    unsigned* wmax2 = rad2 + 2 * C;  // max |c - mean|^2 over the centroids
+    ck(cudaMemsetAsync(rad2, 0, (2 * size_t(C) + 1) * 4, st), "rad2");
+    if (dp == 52)
+        k_probe_dist<13><<<blocks(n, 8), 256, 0, st>>>(X, d, dp, n, probes, P, cent, qan, pdist,
+                                                        rad2, umax2);
+    else
+        k_probe_dist<0><<<blocks(n, 8), 256, 0, st>>>(X, d, dp, n, probes, P, cent, qan, pdist,
+                                                       rad2, umax2);
+    count_launch();
+    k_max_nonneg<<<1, 256, 0, st>>>(cbn, C, wmax2); count_launch();
+    float* cdist = c->get<float>("cent_dist", size_t(C) * C);
+    k_cent_dist<<<blocks(size_t(C) * C, 256), 256, 0, st>>>(cent, C, d, dp, cdist); count_launch();
     std::vector<uint32_t> hq(2 * C + 1);
     ck(cudaMemcpyAsync(hq.data(), q_off, size_t(2 * C + 1) * 4, cudaMemcpyDeviceToHost, st),
        "q_off");
     ck(cudaStreamSynchronize(st), "layout");
     std::vector<uint32_t> hc(C + 1);
     ck(cudaMemcpy(hc.data(), c_off, size_t(C + 1) * 4, cudaMemcpyDeviceToHost), "c_off");
-    // jobs: pass 0 = primary entries (keys [0, C)), pass 1 = the others
+    // jobs of one pass from its entries' bucket bounds (hq[key] for key in
+    // [key0, key0 + C)): 128 entries of one probe bucket each
     std::vector<uint32_t> jb[2], jq[2], je[2], jt0;
     uint64_t tile_pairs = 0, maxb = 0, cells = 0, pass_pairs[2] = {0, 0};
-    for (int pass = 0; pass < 2; ++pass)
+    auto make_jobs = [&](int pass, const std::vector<uint32_t>& bounds, uint32_t key0,
+                         uint32_t base) {
         for (uint32_t b = 0; b < C; ++b) {
-            const uint32_t key = b + (pass ? C : 0);
+            const uint32_t key = b + key0;
             const uint64_t nct = (hc[b + 1] - hc[b] + 255) / 256;
             maxb = std::max<uint64_t>(maxb, hc[b + 1] - hc[b]);
-            for (uint32_t q0 = hq[key]; q0 < hq[key + 1]; q0 += 128) {
+            for (uint32_t q0 = base + bounds[key]; q0 < base + bounds[key + 1]; q0 += 128) {
+                const uint32_t q1 = std::min(q0 + 128, base + bounds[key + 1]);
                 jb[pass].push_back(b);
                 jq[pass].push_back(q0);
-                je[pass].push_back(std::min(q0 + 128, hq[key + 1]));
+                je[pass].push_back(q1);
                 // a primary job's own cells are its candidates at the same offset
-                if (pass == 0) jt0.push_back((q0 - hq[key]) / 256);
+                if (pass == 0) jt0.push_back((q0 - base - bounds[key]) / 256);
                 tile_pairs += nct;
                 pass_pairs[pass] += nct;
-                cells += uint64_t(std::min(q0 + 128, hq[key + 1]) - q0) * (hc[b + 1] - hc[b]);
+                cells += uint64_t(q1 - q0) * (hc[b + 1] - hc[b]);
             }
         }
-    S_.shortlist[0] = tile_pairs;
-    S_.shortlist[1] = maxb;
-    S_.shortlist[2] = C;
-    S_.shortlist[3] = cells;
-    S_.shortlist[4] = pass_pairs[0];
-    S_.shortlist[5] = pass_pairs[1];
-    if (std::getenv("POLARISEQ_TRACE"))
-        std::fprintf(stderr, "[chosen] %u buckets, largest %llu, %zu + %zu query tiles, %llu tile pairs\n",
-                     C, (unsigned long long)maxb, jb[0].size(), jb[1].size(),
-                     (unsigned long long)tile_pairs);
+    };
+    make_jobs(0, hq, 0, 0);
     kg_sec.reset();
     S_.ms_leaves = tm.stop();
 
@@ -903,14 +1065,13 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (fp8 && Ssh > 16) throw DeviceError{"the E4M3 form supports k <= 15"};
     float* sd = c->get<float>("sl_d", ne * Sout);
     uint32_t* si = c->get<uint32_t>("sl_i", ne * Sout);
-    // live length of each run, cell-major: [cell * P + probe rank][run]
+    // live length of each run, cell-major: [cell * P + probe rank][run]; a
+    // dropped entry's runs stay empty
     uint8_t* sn = c->get<uint8_t>("sl_n", ne * ivf_groups());
+    ck(cudaMemsetAsync(sn, 0, ne * ivf_groups(), st), "run lengths");
+    float* qthr = c->get<float>("q_thr", ne);
+    float* cseed = c->get<float>("cell_seed", n);
     {
-        CUtensorMap tq, tcm;
-        const bool maps = fp8 ? make_fp8_map(&tq, qb8, ne, 128) && make_fp8_map(&tcm, xc8, n, 256)
-                              : make_bf16_map(&tq, qb, ne, 128) && make_bf16_map(&tcm, xc, n, 256);
-        if (!maps) throw DeviceError{"cuTensorMapEncodeTiled failed"};
-        float* qthr = c->get<float>("q_thr", ne);
         const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
         unsigned long long* tbuf = nullptr;
         if (trace) {
@@ -923,9 +1084,56 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         // 2k-th seed to four digits, with 16% fewer tile-kernel cycles)
         // (the E4M3 ranking error is larger: 2k places)
         const int R0 = std::min(Sout, fp8 ? 2 * k : k + 2);
+        uint64_t pruned = 0;
         for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) {
+                // the other-probe entries that can admit anything, compacted
+                // in order, laid out after the primary ones
+                KGScope kg(c, PQ_KG_LAYOUT);
+                const size_t m = ne - n;
+                uint32_t* keep = c->get<uint32_t>("prune_keep", std::max<size_t>(m, 1));
+                uint32_t* kpos = c->get<uint32_t>("prune_pos", std::max<size_t>(m, 1));
+                uint64_t* dtot = c->get<uint64_t>("prune_total", 1);
+                uint64_t m1 = 0;
+                if (m > 0) {
+                    k_prune_keep<<<blocks(m, 256), 256, 0, st>>>(ekeys + n, evals + n, m, P, C,
+                                                                 pdist, rad2, umax2, wmax2,
+                                                                 cdist, cseed, keep);
+                    count_launch();
+                    ck(scan_exclusive_u32(keep, kpos, m,
+                                          c->get<uint8_t>("prune_scan", scan_temp_bytes(m)), dtot,
+                                          st),
+                       "scan kept");
+                    k_compact_entries<<<blocks(m, 256), 256, 0, st>>>(ekeys + n, evals + n, m,
+                                                                      keep, kpos, ekeys2 + n,
+                                                                      evals2 + n);
+                    count_launch();
+                    ck(cudaMemcpyAsync(&m1, dtot, 8, cudaMemcpyDeviceToHost, st), "kept");
+                    ck(cudaStreamSynchronize(st), "kept");
+                }
+                pruned = m - m1;
+                lay_entries(ekeys2 + n, evals2 + n, uint32_t(n), m1);
+                if (m1 > 0) {
+                    k_entry_thr<<<blocks(m1, 256), 256, 0, st>>>(eslot + n, m1, P, cseed,
+                                                                 qthr + n);
+                    count_launch();
+                }
+                k_key_bounds<<<blocks(m1 + 1, 256), 256, 0, st>>>(ekeys2 + n, m1, C, 2 * C,
+                                                                  q_off);
+                count_launch();
+                ck(cudaMemcpyAsync(hq.data(), q_off, size_t(2 * C + 1) * 4,
+                                   cudaMemcpyDeviceToHost, st),
+                   "q_off");
+                ck(cudaStreamSynchronize(st), "layout");
+                make_jobs(1, hq, C, uint32_t(n));
+            }
             const uint32_t nj = uint32_t(jb[pass].size());
             if (nj == 0) continue;
+            CUtensorMap tq, tcm;
+            const bool maps =
+                fp8 ? make_fp8_map(&tq, qb8, ne, 128) && make_fp8_map(&tcm, xc8, n, 256)
+                    : make_bf16_map(&tq, qb, ne, 128) && make_bf16_map(&tcm, xc, n, 256);
+            if (!maps) throw DeviceError{"cuTensorMapEncodeTiled failed"};
             uint32_t* djb = c->get<uint32_t>(pass ? "job_b1" : "job_b0", nj);
             uint32_t* djq = c->get<uint32_t>(pass ? "job_q1" : "job_q0", nj);
             uint32_t* dje = c->get<uint32_t>(pass ? "job_e1" : "job_e0", nj);
@@ -937,7 +1145,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                 ck(cudaMemcpyAsync(djt, jt0.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st),
                    "jobs");
             } else {
-                k_job_tstart<<<blocks(nj, 256), 256, 0, st>>>(djb, djq, nj, ekeys, C, c_off,
+                k_job_tstart<<<blocks(nj, 256), 256, 0, st>>>(djb, djq, nj, ekeys2, C, c_off,
                                                               pair_off, djt);
                 count_launch();
             }
@@ -969,7 +1177,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             }
             if (pass == 0) {  // seed the other probes with the primary shortlist's R-th best
                 k_seed_thresholds<<<blocks(n, 256), 256, 0, st>>>(entry_of, n, P, sd, sn, Ssh, R0,
-                                                                  qthr);
+                                                                  cseed);
                 count_launch();
             }
             ck(cudaStreamSynchronize(st), "jobs");  // the host job arrays are reused
@@ -987,6 +1195,20 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                              h[IVF_T_ADMITS], h[IVF_T_WMBITS], h[IVF_T_SLOW_CYC]);
             }
         }
+        S_.shortlist[0] = tile_pairs;
+        S_.shortlist[1] = maxb;
+        S_.shortlist[2] = C;
+        S_.shortlist[3] = cells;
+        S_.shortlist[4] = pass_pairs[0];
+        S_.shortlist[5] = pass_pairs[1];
+        S_.shortlist[7] = pruned;
+        if (trace)
+            std::fprintf(stderr,
+                         "[chosen] %u buckets, largest %llu, %zu + %zu query tiles, %llu tile "
+                         "pairs, %llu of %llu other-probe entries dropped\n",
+                         C, (unsigned long long)maxb, jb[0].size(), jb[1].size(),
+                         (unsigned long long)tile_pairs, (unsigned long long)pruned,
+                         (unsigned long long)(ne - n));
     }
     int herr = 0;
     ck(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, st), "err");
