@@ -407,42 +407,57 @@ __global__ void k_bucket_scale(const unsigned* __restrict__ amax, uint32_t C,
 // E4M3 rows (128 one-byte columns, zero padded) of (row(src_i) - centre(c_i))
 // scaled by the row's own power-of-two scale (bucket_amax == null: queries;
 // inv_scale receives 1/scale) or its bucket's (candidates).  norm receives the
-// FP32 |dequantised row|^2, times `norm_mult`.
+// FP32 |dequantised row|^2, times `norm_mult`.  A half-warp per row (lane h:
+// columns 4h..4h+3, one 16-byte load of the row and of the centre; columns
+// 64..127 are zero), grid-stride over the rows; needs dp <= 64.
 __global__ void k_to_fp8(const float* __restrict__ X, int d, int dp,
                          const uint32_t* __restrict__ src, const uint32_t* __restrict__ cid,
                          const float* __restrict__ cent, size_t rows,
                          const unsigned* __restrict__ bucket_amax, uint32_t* __restrict__ out,
                          float* __restrict__ inv_scale, float* __restrict__ norm,
                          float norm_mult) {
-    const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (r >= rows) return;
-    const uint32_t i = src ? src[r] : uint32_t(r), c = cid[r];
-    float v[4];
-    float m = 0.f;
+    const int h = threadIdx.x & 15;
+    const unsigned hm = 0xFFFFu << (threadIdx.x & 16);  // this half-warp's lanes
+    const size_t nh = (size_t(gridDim.x) * blockDim.x) >> 4;
+    for (size_t r = (size_t(blockIdx.x) * blockDim.x + threadIdx.x) >> 4; r < rows; r += nh) {
+        const uint32_t i = src ? src[r] : uint32_t(r), c = cid[r];
+        float v[4] = {0.f, 0.f, 0.f, 0.f};
+        if (4 * h < dp) {
+            const float4 x4 = *reinterpret_cast<const float4*>(X + size_t(i) * dp + 4 * h);
+            const float4 c4 = *reinterpret_cast<const float4*>(cent + size_t(c) * dp + 4 * h);
+            v[0] = x4.x - c4.x;
+            v[1] = x4.y - c4.y;
+            v[2] = x4.z - c4.z;
+            v[3] = x4.w - c4.w;
+        }
+        float m = 0.f;
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const int j = 4 * lane + u;
-        v[u] = j < d ? X[size_t(i) * dp + j] - cent[size_t(c) * dp + j] : 0.f;
-        m = fmaxf(m, fabsf(v[u]));
-    }
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
-    const float sc = e4m3_scale(bucket_amax ? __uint_as_float(bucket_amax[c]) : m);
-    uint32_t word = 0;
-    float s = 0.f;
+        for (int u = 0; u < 4; ++u) {
+            if (4 * h + u >= d) v[u] = 0.f;
+            m = fmaxf(m, fabsf(v[u]));
+        }
 #pragma unroll
-    for (int u = 0; u < 4; ++u) {
-        const __nv_fp8_storage_t q = __nv_cvt_float_to_fp8(v[u] * sc, __NV_SATFINITE, __NV_E4M3);
-        const __half_raw hr = __nv_cvt_fp8_to_halfraw(q, __NV_E4M3);
-        const float deq = __half2float(__half(hr)) / sc;
-        s = fmaf(deq, deq, s);
-        word |= uint32_t(q) << (8 * u);
-    }
-    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xFFFFFFFFu, s, o);
-    out[r * 32 + lane] = word;
-    if (lane == 0) {
-        norm[r] = s * norm_mult;
-        if (inv_scale) inv_scale[r] = 1.0f / sc;
+        for (int o = 8; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(hm, m, o));
+        const float sc = e4m3_scale(bucket_amax ? __uint_as_float(bucket_amax[c]) : m);
+        uint32_t word = 0;
+        float s = 0.f;
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const __nv_fp8_storage_t q =
+                __nv_cvt_float_to_fp8(v[u] * sc, __NV_SATFINITE, __NV_E4M3);
+            const __half_raw hr = __nv_cvt_fp8_to_halfraw(q, __NV_E4M3);
+            const float deq = __half2float(__half(hr)) / sc;
+            s = fmaf(deq, deq, s);
+            word |= uint32_t(q) << (8 * u);
+        }
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(hm, s, o);
+        out[r * 32 + h] = word;
+        out[r * 32 + 16 + h] = 0u;
+        if (h == 0) {
+            norm[r] = s * norm_mult;
+            if (inv_scale) inv_scale[r] = 1.0f / sc;
+        }
     }
 }
 
@@ -962,7 +977,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         k_bucket_scale<<<blocks(C, 256), 256, 0, st>>>(amax, C, bscale); count_launch();
         xc8 = c->get<uint32_t>("xc_fp8", size_t(n) * 32);
         xch = c->get<float>("xc_half", n);
-        k_to_fp8<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax, xc8,
+        k_to_fp8<<<cvt_blocks(n), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax, xc8,
                                                 nullptr, xch, 0.5f); count_launch();
     }
     // query entries grouped by probe bucket (stable: cell order within a bucket);
@@ -998,7 +1013,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             k_to_bf16<<<cvt_blocks(m), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
                                                       1, qb + size_t(e0) * 64, qbn + e0);
         } else {
-            k_to_fp8<<<blocks(m, 8), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
+            k_to_fp8<<<cvt_blocks(m), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
                                                     nullptr, qb8 + size_t(e0) * 32,
                                                     qscale + e0, qbn + e0, 1.0f);
         }
