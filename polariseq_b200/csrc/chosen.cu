@@ -152,47 +152,49 @@ __global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_
 }
 
 // Exact FP32 squared distance of every cell to each of its P probe centroids
-// (d[i * P + r]), and each bucket's squared radius over its own cells
-// (rad2[b] = max over cells whose primary is b; non-negative floats order as
-// their bits).  One warp per cell, lane r < P.
-template <int DQ>  // row length in float4s (0: dp / 4 at run time)
+// (d[i * P + r]), each bucket's squared radius over its own cells (rad2[b] =
+// max over cells whose primary is b) and the largest |y - mean|^2 of its
+// cells (umax2[b], from un); non-negative floats order as their bits.  One
+// warp per cell: each half-warp takes every other probe, lane h holding
+// dimensions 4h..4h+3 (16-byte loads of the row and the centroid), the sum
+// reduced over the half-warp.  Needs dp <= 64.
 __global__ void k_probe_dist(const float* __restrict__ X, int d, int dp, uint32_t n,
                              const uint32_t* __restrict__ probes, int P,
                              const float* __restrict__ cent, const float* __restrict__ un,
                              float* __restrict__ dist, unsigned* __restrict__ rad2,
                              unsigned* __restrict__ umax2) {
     const uint32_t i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (i >= n || lane >= P) return;
-    const uint32_t c = probes[size_t(i) * P + lane];
-    const float* xi = X + size_t(i) * dp;
-    const float* cc = cent + size_t(c) * dp;
-    float s = 0.f;
-    if constexpr (DQ > 0) {
-        float4 xv[DQ], cv[DQ];
-#pragma unroll
-        for (int q = 0; q < DQ; ++q) {
-            xv[q] = reinterpret_cast<const float4*>(xi)[q];
-            cv[q] = reinterpret_cast<const float4*>(cc)[q];
-        }
-#pragma unroll
-        for (int q = 0; q < DQ; ++q) {
-            const float e[4] = {xv[q].x - cv[q].x, xv[q].y - cv[q].y, xv[q].z - cv[q].z,
-                                xv[q].w - cv[q].w};
+    if (i >= n) return;
+    const int lane = threadIdx.x & 31, h = lane & 15, half = lane >> 4;
+    const unsigned hm = 0xFFFFu << (lane & 16);
+    float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (4 * h < dp) x4 = reinterpret_cast<const float4*>(X + size_t(i) * dp)[h];
+    const float xs[4] = {x4.x, x4.y, x4.z, x4.w};
+    // both halves run the same number of rounds (the shuffles need their lanes)
+    for (int r0 = 0; r0 < P; r0 += 2) {
+        const int r = r0 + half;
+        const bool live = r < P;
+        const uint32_t c = live ? probes[size_t(i) * P + r] : 0u;
+        float s = 0.f;
+        if (live && 4 * h < dp) {
+            const float4 c4 = reinterpret_cast<const float4*>(cent + size_t(c) * dp)[h];
+            const float cs[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
             for (int u = 0; u < 4; ++u)
-                if (4 * q + u < d) s = fmaf(e[u], e[u], s);
+                if (4 * h + u < d) {
+                    const float df = xs[u] - cs[u];
+                    s = fmaf(df, df, s);
+                }
         }
-    } else {
-        for (int t = 0; t < d; ++t) {
-            const float df = xi[t] - cc[t];
-            s = fmaf(df, df, s);
+#pragma unroll
+        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(hm, s, o);
+        if (live && h == 0) {
+            dist[size_t(i) * P + r] = s;
+            if (r == 0) {
+                atomicMax(&rad2[c], __float_as_uint(s));
+                atomicMax(&umax2[c], __float_as_uint(un[i]));
+            }
         }
-    }
-    dist[size_t(i) * P + lane] = s;
-    if (lane == 0) {
-        atomicMax(&rad2[c], __float_as_uint(s));
-        atomicMax(&umax2[c], __float_as_uint(un[i]));
     }
 }
 
@@ -1029,12 +1031,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     unsigned* umax2 = rad2 + C;      // per bucket: max |y - mean|^2 of its cells
     unsigned* wmax2 = rad2 + 2 * C;  // max |c - mean|^2 over the centroids
     ck(cudaMemsetAsync(rad2, 0, (2 * size_t(C) + 1) * 4, st), "rad2");
-    if (dp == 52)
-        k_probe_dist<13><<<blocks(n, 8), 256, 0, st>>>(X, d, dp, n, probes, P, cent, qan, pdist,
-                                                        rad2, umax2);
-    else
-        k_probe_dist<0><<<blocks(n, 8), 256, 0, st>>>(X, d, dp, n, probes, P, cent, qan, pdist,
-                                                       rad2, umax2);
+    k_probe_dist<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, n, probes, P, cent, qan, pdist, rad2,
+                                                umax2);
     count_launch();
     k_max_nonneg<<<1, 256, 0, st>>>(cbn, C, wmax2); count_launch();
     float* cdist = c->get<float>("cent_dist", size_t(C) * C);
