@@ -67,7 +67,7 @@ __global__ void k_kmeans_accumulate(const float* __restrict__ xs, uint32_t ns, i
     for (int j = 0; j < d; ++j) atomicAdd(&sums[size_t(b) * dp + j], xs[size_t(i) * dp + j]);
 }
 
-// Query-entry keys and values (cell * P + rank) from the probes.  Primary
+// Query-entry keys and values (slot = position * P + rank) from the probes.  Primary
 // entries (rank 0) sort first, by (bucket, second-nearest centroid) exactly
 // as the candidates do, so that a primary job's own cells form its first
 // candidate tile; the others follow by (probe bucket, the cell's primary
@@ -75,9 +75,9 @@ __global__ void k_kmeans_accumulate(const float* __restrict__ xs, uint32_t ns, i
 // the candidates on that side of the probe bucket first.
 // Entry e = (candidate position p, probe rank r), p = e / P, of cell
 // perm[p]: key (primary entries) = the cell's candidate key, (others) =
-// (C + probe bucket) * C + primary bucket; value = cell * P + r.  Generated in
-// candidate order, so that after the stable sort the entries of one (probe,
-// primary) pair follow the primary bucket's candidate order.
+// (C + probe bucket) * C + primary bucket; value = its slot p * P + r (= e).
+// Generated in candidate order, so that after the stable sort the entries of
+// one (probe, primary) pair follow the primary bucket's candidate order.
 __global__ void k_entry_keys(const uint32_t* __restrict__ probes,
                              const uint32_t* __restrict__ perm, size_t ne, int P, uint32_t C,
                              uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
@@ -91,7 +91,7 @@ __global__ void k_entry_keys(const uint32_t* __restrict__ probes,
         keys[e] = a * C + (P > 1 ? probes[i * P + 1] : 0u);
     else
         keys[e] = (C + probes[i * P + r]) * C + a;
-    vals[e] = i * P + r;
+    vals[e] = e;
 }
 
 // The embedding rows in candidate order (xp[p] = X[perm[p]], dp floats each).
@@ -122,13 +122,14 @@ __global__ void k_job_tstart(const uint32_t* __restrict__ job_bucket,
 // Seed thresholds of the non-primary entries: the R-th best approximate
 // distance of the cell's primary shortlist (a candidate of another bucket can
 // only enter the cell's R best if it beats that); +inf when the primary
-// shortlist holds fewer than R.  sn holds the runs' live lengths, cell-major.
+// shortlist holds fewer than R.  Per candidate position p (the cell perm[p]);
+// entry_of and sn are indexed by slot p * P + rank.
 __global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_t n, int P,
                                   const float* __restrict__ sd, const uint8_t* __restrict__ sn,
                                   int S, int R, float* __restrict__ cseed) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
-    const uint32_t e0 = entry_of[size_t(i) * P];
+    const uint32_t e0 = entry_of[size_t(i) * P];  // i: the position
     // the R-th smallest of the entry's two ascending runs (live prefixes)
     const float* r0 = sd + size_t(e0) * 2 * S;
     const float* r1 = r0 + S;
@@ -151,24 +152,26 @@ __global__ void k_seed_thresholds(const uint32_t* __restrict__ entry_of, uint32_
     cseed[i] = t;
 }
 
-// Exact FP32 squared distance of every cell to each of its P probe centroids
-// (d[i * P + r]), each bucket's squared radius over its own cells (rad2[b] =
-// max over cells whose primary is b) and the largest |y - mean|^2 of its
-// cells (umax2[b], from un); non-negative floats order as their bits.  One
-// warp per cell: each half-warp takes every other probe, lane h holding
+// Exact FP32 squared distance of the cell at every candidate position p
+// (row xp[p], cell perm[p]) to each of its P probe centroids (d[p * P + r]),
+// each bucket's squared radius over its own cells (rad2[b] = max over cells
+// whose primary is b) and the largest |y - mean|^2 of its cells (umax2[b],
+// from un, per cell); non-negative floats order as their bits.  One warp per
+// position: each half-warp takes every other probe, lane h holding
 // dimensions 4h..4h+3 (16-byte loads of the row and the centroid), the sum
 // reduced over the half-warp.  Needs dp <= 64.
-__global__ void k_probe_dist(const float* __restrict__ X, int d, int dp, uint32_t n,
-                             const uint32_t* __restrict__ probes, int P,
+__global__ void k_probe_dist(const float* __restrict__ xp, const uint32_t* __restrict__ perm,
+                             int d, int dp, uint32_t n, const uint32_t* __restrict__ probes, int P,
                              const float* __restrict__ cent, const float* __restrict__ un,
                              float* __restrict__ dist, unsigned* __restrict__ rad2,
                              unsigned* __restrict__ umax2) {
-    const uint32_t i = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    if (i >= n) return;
+    const uint32_t p = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    if (p >= n) return;
+    const uint32_t i = perm[p];
     const int lane = threadIdx.x & 31, h = lane & 15, half = lane >> 4;
     const unsigned hm = 0xFFFFu << (lane & 16);
     float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (4 * h < dp) x4 = reinterpret_cast<const float4*>(X + size_t(i) * dp)[h];
+    if (4 * h < dp) x4 = reinterpret_cast<const float4*>(xp + size_t(p) * dp)[h];
     const float xs[4] = {x4.x, x4.y, x4.z, x4.w};
     // both halves run the same number of rounds (the shuffles need their lanes)
     for (int r0 = 0; r0 < P; r0 += 2) {
@@ -189,7 +192,7 @@ __global__ void k_probe_dist(const float* __restrict__ X, int d, int dp, uint32_
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(hm, s, o);
         if (live && h == 0) {
-            dist[size_t(i) * P + r] = s;
+            dist[size_t(p) * P + r] = s;
             if (r == 0) {
                 atomicMax(&rad2[c], __float_as_uint(s));
                 atomicMax(&umax2[c], __float_as_uint(un[i]));
@@ -236,7 +239,7 @@ __global__ void k_max_nonneg(const float* __restrict__ v, uint32_t m, unsigned* 
 // the split norm columns), and f grows with t where it is positive.  So an
 // entry with f(lb^2) >= seed (lb the larger bound) admits nothing and is
 // dropped: keep[j] = 0.  Entries j are the sorted other-probe entries (key =
-// (C + B) * C + A, value = cell * P + rank); distances are FP32 (their
+// (C + B) * C + A, value = slot p * P + rank); distances are FP32 (their
 // rounding is covered by the 2^-20 and 2^-18 terms).
 __global__ void k_prune_keep(const uint32_t* __restrict__ keys, const uint64_t* __restrict__ vals,
                              size_t m, int P, uint32_t C, const float* __restrict__ dist,
@@ -498,23 +501,19 @@ __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n, uin
 
 __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t* __restrict__ keys,
                                size_t ne, uint32_t e0, int P, uint32_t C,
-                               const uint32_t* __restrict__ probes,
-                               const uint32_t* __restrict__ pos_of, uint32_t* __restrict__ qpos,
-                               uint32_t* __restrict__ qbucket, uint32_t* __restrict__ qself,
-                               uint32_t* __restrict__ entry_of, uint32_t* __restrict__ slot) {
+                               uint32_t* __restrict__ qpos, uint32_t* __restrict__ qbucket,
+                               uint32_t* __restrict__ qself, uint32_t* __restrict__ entry_of,
+                               uint32_t* __restrict__ slot) {
     const size_t e = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (e >= ne) return;
-    const uint64_t v = vals[e];
-    const uint32_t i = uint32_t(v / P), r = uint32_t(v % P);
+    const uint64_t v = vals[e];  // slot: candidate position * P + probe rank
+    const uint32_t pos = uint32_t(v / P), r = uint32_t(v % P);
     const uint32_t kb = keys[e] / C;
-    const uint32_t b = kb >= C ? kb - C : kb;
-    const uint32_t pos = pos_of[i];
     qpos[e] = pos;
-    qbucket[e] = b;
-    qself[e] = b == probes[size_t(i) * P] ? pos : 0xFFFFFFFFu;
+    qbucket[e] = kb >= C ? kb - C : kb;
+    qself[e] = r == 0 ? pos : 0xFFFFFFFFu;  // rank 0 is the primary bucket
     entry_of[v] = e0 + uint32_t(e);
     slot[e] = uint32_t(v);
-    (void)r;
 }
 
 // Bitonic sort (ascending) of 64 keys held two per lane (element e of lane l
@@ -586,7 +585,7 @@ __global__ void __launch_bounds__(128) k_rerank(
     // 1. the R best approximate candidates of the shortlist runs (lane L <
     //    P * NR owns run L % NR of probe L / NR; runs are RS long (a multiple
     //    of 4), ascending, an entry's NR runs RS * NR apart, and the first
-    //    sn[cell * P * NR + L] entries of run L are its finite ones).  The
+    //    sn[position * P * NR + L] entries of run L are its finite ones).  The
     //    live prefixes are copied into shared memory (four entries per vector
     //    load, all issued at once) and sorted as (distance bits, position)
     //    keys — 64 at most, else the runs are merged head by head.
@@ -595,8 +594,8 @@ __global__ void __launch_bounds__(128) k_rerank(
     size_t base = 0;
     int fin = 0;
     if (owner) {
-        base = size_t(entry_of[size_t(i) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
-        fin = sn[size_t(i) * P * NR + lane];
+        base = size_t(entry_of[size_t(wg) * P + lane / NR]) * SO + size_t(lane % NR) * RS;
+        fin = sn[size_t(wg) * P * NR + lane];
     }
     uint32_t cand[2] = {0xFFFFFFFFu, 0xFFFFFFFFu};
     int off = fin;  // inclusive prefix sum of the live counts
@@ -991,7 +990,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* qbucket = c->get<uint32_t>("qbucket", ne);
     uint32_t* qself = c->get<uint32_t>("qself", ne);
     uint32_t* entry_of = c->get<uint32_t>("entry_of", ne);
-    uint32_t* eslot = c->get<uint32_t>("entry_slot", ne);  // entry -> cell * P + probe rank
+    uint32_t* eslot = c->get<uint32_t>("entry_slot", ne);  // entry -> position * P + probe rank
     uint32_t* q_off = c->get<uint32_t>("q_off", 2 * C + 1);
     __nv_bfloat16* qb = nullptr;
     uint32_t* qb8 = nullptr;
@@ -1007,9 +1006,9 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     // converted
     auto lay_entries = [&](const uint32_t* keys, const uint64_t* vals, uint32_t e0, size_t m) {
         if (m == 0) return;
-        k_entry_layout<<<blocks(m, 256), 256, 0, st>>>(vals, keys, m, e0, P, C, probes, pos_of,
-                                                       qpos + e0, qbucket + e0, qself + e0,
-                                                       entry_of, eslot + e0);
+        k_entry_layout<<<blocks(m, 256), 256, 0, st>>>(vals, keys, m, e0, P, C, qpos + e0,
+                                                       qbucket + e0, qself + e0, entry_of,
+                                                       eslot + e0);
         count_launch();
         if (!fp8) {
             k_to_bf16<<<cvt_blocks(m), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
@@ -1031,8 +1030,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     unsigned* umax2 = rad2 + C;      // per bucket: max |y - mean|^2 of its cells
     unsigned* wmax2 = rad2 + 2 * C;  // max |c - mean|^2 over the centroids
     ck(cudaMemsetAsync(rad2, 0, (2 * size_t(C) + 1) * 4, st), "rad2");
-    k_probe_dist<<<blocks(n, 8), 256, 0, st>>>(X, d, dp, n, probes, P, cent, qan, pdist, rad2,
-                                                umax2);
+    k_probe_dist<<<blocks(n, 8), 256, 0, st>>>(xp, perm, d, dp, n, probes, P, cent, qan, pdist,
+                                                rad2, umax2);
     count_launch();
     k_max_nonneg<<<1, 256, 0, st>>>(cbn, C, wmax2); count_launch();
     float* cdist = c->get<float>("cent_dist", size_t(C) * C);
@@ -1078,12 +1077,12 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (fp8 && Ssh > 16) throw DeviceError{"the E4M3 form supports k <= 15"};
     float* sd = c->get<float>("sl_d", ne * Sout);
     uint32_t* si = c->get<uint32_t>("sl_i", ne * Sout);
-    // live length of each run, cell-major: [cell * P + probe rank][run]; a
+    // live length of each run by slot: [position * P + probe rank][run]; a
     // dropped entry's runs stay empty
     uint8_t* sn = c->get<uint8_t>("sl_n", ne * ivf_groups());
     ck(cudaMemsetAsync(sn, 0, ne * ivf_groups(), st), "run lengths");
     float* qthr = c->get<float>("q_thr", ne);
-    float* cseed = c->get<float>("cell_seed", n);
+    float* cseed = c->get<float>("cell_seed", n);  // per candidate position
     {
         const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
         unsigned long long* tbuf = nullptr;
