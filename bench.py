@@ -212,10 +212,10 @@ def run_reference(args):
 
 # DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel:
 # an ncu capture of its two passes at 1M x 50 (profiles/k_ivf_tiles_1m.md) read
-# and wrote 0.547 GB over 184,443 tile pairs (primary pass) and 2.823 GB over
-# 1,258,551 (other probes), 2,336 bytes per pair over both; a launch's traffic
+# and wrote 0.537 GB over 184,331 tile pairs (primary pass) and 1.443 GB over
+# 806,044 (other probes), 1,999 bytes per pair over both; a launch's traffic
 # is taken to scale with the tile pairs it processes.
-TILE_DRAM_BYTES_PER_PAIR = 2336.0
+TILE_DRAM_BYTES_PER_PAIR = 1999.0
 
 
 def tiles_roofline(per, st, args, peaks):
