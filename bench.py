@@ -211,7 +211,7 @@ def run_reference(args):
 
 
 # DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel:
-# an ncu capture of its two passes at 1M x 50 (profiles/k_ivf_tiles_1m.md) read
+# an ncu capture (--set full) of its two passes at 1M x 50 read
 # and wrote 0.537 GB over 184,331 tile pairs (primary pass) and 1.443 GB over
 # 806,044 (other probes), 1,999 bytes per pair over both; a launch's traffic
 # is taken to scale with the tile pairs it processes.

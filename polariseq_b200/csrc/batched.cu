@@ -5,7 +5,7 @@
 // Semantics per sample (as knn_exact): every point's k nearest other points
 // of the same sample, exact, ties broken by index, ascending; indices are
 // local to the sample.  Distances are squared Euclidean sums of (q - x)^2 in
-// FP32 (FMA); the graph is judged against an FP64 brute force as exact sets.
+// FP32 (FMA); the graph is checked against an FP64 brute force as exact sets.
 //
 // Work items are (sample, block of NW*QW queries), ordered largest sample
 // first; persistent CTAs take the next item from a device counter.  A CTA

@@ -1,7 +1,7 @@
 """The tensor-core shortlist form (mode='bf16') on the GPU: graph structure,
 determinism and recall@k against the FP64 exact oracle.
 
-Its graph is not the reference's (a different search), so it is judged by
+Its graph is not the reference's (a different search), so it is checked by
 recall@k >= 0.99 against FP64 brute force with (distance, index) order and by
 its distances: every returned distance is the exact FP32 distance of its pair
 in the reference's summation order."""
