@@ -516,6 +516,21 @@ __global__ void k_entry_layout(const uint64_t* __restrict__ vals, const uint32_t
     slot[e] = uint32_t(v);
 }
 
+// Bitonic sort (ascending) of 32 keys held one per lane.
+__device__ __forceinline__ uint64_t warp_sort32(uint64_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+        for (int stride = size >> 1; stride > 0; stride >>= 1) {
+            const uint64_t o = __shfl_xor_sync(0xFFFFFFFFu, v, stride);
+            const bool lower = (lane & stride) == 0;
+            const bool up = (lane & size) == 0 || size == 32;
+            v = (lower == up) ? (o < v ? o : v) : (o > v ? o : v);
+        }
+    return v;
+}
+
 // Bitonic sort (ascending) of 64 keys held two per lane (element e of lane l
 // is index l + 32 e).
 __device__ __forceinline__ void warp_sort64(uint64_t (&v)[2]) {
@@ -678,7 +693,11 @@ __global__ void __launch_bounds__(128) k_rerank(
         }
     }
     // 3. sort by (distance, index): non-negative floats order as their bits
-    warp_sort64(key);
+    //    (R <= 32: one key per lane, the second places are empty)
+    if (R <= 32)
+        key[0] = warp_sort32(key[0]);
+    else
+        warp_sort64(key);
     // 4. FP64 band at the k-th boundary
     const uint64_t kk1 = __shfl_sync(0xFFFFFFFFu, (k - 1) >= 32 ? key[1] : key[0], (k - 1) & 31);
     const uint64_t kk =
