@@ -488,14 +488,13 @@ __global__ void k_key_bounds(const uint32_t* __restrict__ keys, size_t ne, uint3
     for (uint32_t v = lo; v <= hi; ++v) off[v] = uint32_t(e);
 }
 
+// Candidate position p -> its cell perm[p] and bucket cbucket[p].
 __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n, uint32_t C,
                               const uint32_t* __restrict__ keys, uint32_t* __restrict__ perm,
-                              uint32_t* __restrict__ pos_of, uint32_t* __restrict__ cbucket) {
+                              uint32_t* __restrict__ cbucket) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    const uint32_t i = uint32_t(vals[p]);
-    perm[p] = i;
-    pos_of[i] = p;
+    perm[p] = uint32_t(vals[p]);
     cbucket[p] = keys[p] / C;
 }
 
@@ -970,9 +969,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* pair_off = c->get<uint32_t>("pair_off", size_t(C) * C + 1);
     k_key_bounds<<<blocks(size_t(n) + 1, 256), 256, 0, st>>>(ckeys, n, 1, C * C, pair_off); count_launch();
     uint32_t* perm = c->get<uint32_t>("cperm", n);
-    uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
     uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
-    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, pos_of, cbucket); count_launch();
+    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, cbucket); count_launch();
     // the embedding in candidate order: the conversions below and the re-rank
     // read it in runs instead of gathering rows
     float* xp = c->get<float>("xp_f32", size_t(n) * dp);
