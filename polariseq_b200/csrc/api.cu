@@ -635,13 +635,16 @@ int pq_nndescent_into(pq_ctx* c, const float* data, uint64_t n, uint64_t d,
         uint32_t* dip = c->get<uint32_t>("out_indptr", n + 1);
         uint32_t* dix = c->get<uint32_t>("out_indices", cap);
         float* ddx = c->get<float>("out_dists", cap);
+        HostGraph hg{indptr, indices, dists, false};
         uint64_t nnz = o->mode == PQ_MODE_PLAIN
                            ? build_plain(c, data, true, n, d, *o, dip, dix, ddx, nullptr)
-                           : build_chosen(c, data, true, n, d, *o, dip, dix, ddx);
-        ck(cudaMemcpyAsync(indptr, dip, (n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
-        ck(cudaMemcpyAsync(indices, dix, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
-        ck(cudaMemcpyAsync(dists, ddx, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
-        ck(cudaStreamSynchronize(c->stream), "d2h");
+                           : build_chosen(c, data, true, n, d, *o, dip, dix, ddx, &hg);
+        if (!hg.copied) {
+            ck(cudaMemcpyAsync(indptr, dip, (n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
+            ck(cudaMemcpyAsync(indices, dix, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
+            ck(cudaMemcpyAsync(dists, ddx, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
+            ck(cudaStreamSynchronize(c->stream), "d2h");
+        }
         *nnz_out = nnz;
         return PQ_OK;
     });

@@ -488,13 +488,16 @@ __global__ void k_key_bounds(const uint32_t* __restrict__ keys, size_t ne, uint3
     for (uint32_t v = lo; v <= hi; ++v) off[v] = uint32_t(e);
 }
 
-// Candidate position p -> its cell perm[p] and bucket cbucket[p].
+// Candidate position p -> its cell perm[p] (and back: pos_of) and bucket
+// cbucket[p].
 __global__ void k_cand_layout(const uint64_t* __restrict__ vals, uint32_t n, uint32_t C,
                               const uint32_t* __restrict__ keys, uint32_t* __restrict__ perm,
-                              uint32_t* __restrict__ cbucket) {
+                              uint32_t* __restrict__ pos_of, uint32_t* __restrict__ cbucket) {
     const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n) return;
-    perm[p] = uint32_t(vals[p]);
+    const uint32_t i = uint32_t(vals[p]);
+    perm[p] = i;
+    pos_of[i] = p;
     cbucket[p] = keys[p] / C;
 }
 
@@ -586,16 +589,19 @@ __global__ void __launch_bounds__(128) k_rerank(
     int P, int SO, int RS, int R,
     const uint32_t* __restrict__ entry_of, const float* __restrict__ sd,
     const uint32_t* __restrict__ si, const uint8_t* __restrict__ sn,
-    const uint32_t* __restrict__ perm, uint32_t* __restrict__ out_idx,
-    float* __restrict__ out_dist, unsigned long long* boundary_fixes) {
+    const uint32_t* __restrict__ perm, const uint32_t* __restrict__ pos_of, uint32_t w0,
+    uint32_t* __restrict__ out_idx, float* __restrict__ out_dist,
+    unsigned long long* boundary_fixes) {
     __shared__ uint32_t band_i[4][64];
     __shared__ double band_d[4][64];
     __shared__ float band_f[4][64];
     __shared__ uint64_t band_key[4][64];
-    const uint32_t wg = blockIdx.x * 4 + (threadIdx.x >> 5);
+    // item it in [w0, n): a candidate position (pos_of null) or a cell
+    const uint32_t it = w0 + blockIdx.x * 4 + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (wg >= n) return;
-    const uint32_t i = perm[wg];
+    if (it >= n) return;
+    const uint32_t wg = pos_of ? pos_of[it] : it;  // the cell's candidate position
+    const uint32_t i = pos_of ? it : perm[wg];     // the cell
     // 1. the R best approximate candidates of the shortlist runs (lane L <
     //    P * NR owns run L % NR of probe L / NR; runs are RS long (a multiple
     //    of 4), ascending, an entry's NR runs RS * NR apart, and the first
@@ -782,6 +788,26 @@ __global__ void k_list_extract(const uint32_t* __restrict__ li, const float* __r
     }
 }
 
+// CSR rows [a, b) of full lists (k entries each, so row i starts at i * k):
+// Euclidean distances (sqrt).  A row with an empty place sets *short_rows
+// (the caller then lays the CSR out from the counts instead).
+__global__ void k_list_dense(const uint32_t* __restrict__ li, const float* __restrict__ ld,
+                             uint32_t a, uint32_t b, int k, uint32_t* __restrict__ indptr,
+                             uint32_t* __restrict__ indices, float* __restrict__ dists,
+                             unsigned* __restrict__ short_rows) {
+    const size_t e = size_t(a) * k + size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (e >= size_t(b) * k) return;
+    const size_t i = e / k;
+    const uint32_t v = li[e];
+    if (v == PQ_EMPTY) atomicOr(short_rows, 1u);
+    indices[e] = v;
+    dists[e] = __fsqrt_rn(ld[e]);
+    if (e - i * k == 0) {
+        indptr[i + 1] = uint32_t((i + 1) * k);
+        if (i == 0) indptr[0] = 0;
+    }
+}
+
 // Sorted (ascending) lists -> neighbour heaps: a descending array is a valid
 // max-heap; every entry starts new.
 __global__ void k_list_to_heap(const uint32_t* __restrict__ li, const float* __restrict__ ld,
@@ -806,7 +832,7 @@ using namespace pq;
 
 uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64, uint64_t d64,
                       const pq_nnd_opts& o, uint32_t* d_indptr, uint32_t* d_indices,
-                      float* d_dists) {
+                      float* d_dists, HostGraph* host) {
     cudaStream_t st = c->stream;
     const uint32_t n = uint32_t(n64);
     const int d = int(d64), dp = int((d64 + 3) / 4 * 4);
@@ -970,7 +996,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     k_key_bounds<<<blocks(size_t(n) + 1, 256), 256, 0, st>>>(ckeys, n, 1, C * C, pair_off); count_launch();
     uint32_t* perm = c->get<uint32_t>("cperm", n);
     uint32_t* cbucket = c->get<uint32_t>("cbucket", n);
-    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, cbucket); count_launch();
+    uint32_t* pos_of = c->get<uint32_t>("pos_of", n);
+    k_cand_layout<<<blocks(n, 256), 256, 0, st>>>(cvals, n, C, ckeys, perm, pos_of, cbucket); count_launch();
     // the embedding in candidate order: the conversions below and the re-rank
     // read it in runs instead of gathering rows
     float* xp = c->get<float>("xp_f32", size_t(n) * dp);
@@ -1254,22 +1281,65 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const int R = std::min(P * Sout, std::min(64, std::max(fp8 ? 4 * k : 2 * k, k + 1)));
     if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
     ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
-    {
-        KGScope kg(c, PQ_KG_RERANK);
+    // auto: no polish round for BF16; one for E4M3, whose shortlist misses more
+    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : (fp8 ? 1 : 0);
+    auto rerank = [&](const uint32_t* by_cell, uint32_t a, uint32_t b) {
         if (d == 50)
-            k_rerank<50><<<blocks(n, 4), 128, 0, st>>>(X, xp, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
-                                                       si, sn, perm, ridx, rdist, c->d_acc);
+            k_rerank<50><<<blocks(b - a, 4), 128, 0, st>>>(X, xp, d, dp, b, k, P, Sout, Ssh, R,
+                                                            entry_of, sd, si, sn, perm, by_cell, a,
+                                                            ridx, rdist, c->d_acc);
         else
-            k_rerank<0><<<blocks(n, 4), 128, 0, st>>>(X, xp, d, dp, n, k, P, Sout, Ssh, R, entry_of, sd,
-                                                      si, sn, perm, ridx, rdist, c->d_acc);
+            k_rerank<0><<<blocks(b - a, 4), 128, 0, st>>>(X, xp, d, dp, b, k, P, Sout, Ssh, R,
+                                                           entry_of, sd, si, sn, perm, by_cell, a,
+                                                           ridx, rdist, c->d_acc);
         count_launch();
+    };
+    // graph wanted in host memory and no polish: the cells are re-ranked in
+    // index order, a chunk at a time, and each chunk's CSR rows (full rows:
+    // row i at i * k) are copied to the host on the second stream while the
+    // next chunk is re-ranked
+    const bool overlap = host != nullptr && polish == 0 && n >= (1u << 20);
+    bool copied = false;
+    if (overlap) {
+        KGScope kg(c, PQ_KG_RERANK);
+        unsigned* short_rows = reinterpret_cast<unsigned*>(c->d_acc + 1);
+        const int NCH = 8;
+        cudaEvent_t evs[NCH];
+        for (int j = 0; j < NCH; ++j)
+            ck(cudaEventCreateWithFlags(&evs[j], cudaEventDisableTiming), "event");
+        for (int j = 0; j < NCH; ++j) {
+            const uint32_t a = uint32_t(uint64_t(n) * j / NCH), b = uint32_t(uint64_t(n) * (j + 1) / NCH);
+            if (b == a) continue;
+            rerank(pos_of, a, b);
+            k_list_dense<<<blocks(size_t(b - a) * k, 256), 256, 0, st>>>(ridx, rdist, a, b, k,
+                                                                          d_indptr, d_indices,
+                                                                          d_dists, short_rows);
+            count_launch();
+            ck(cudaEventRecord(evs[j], st), "event");
+            ck(cudaStreamWaitEvent(c->stream2, evs[j], 0), "event");
+            const size_t e0 = size_t(a) * k, ne_ = size_t(b - a) * k;
+            ck(cudaMemcpyAsync(host->indices + e0, d_indices + e0, ne_ * 4, cudaMemcpyDeviceToHost,
+                               c->stream2), "d2h");
+            ck(cudaMemcpyAsync(host->dists + e0, d_dists + e0, ne_ * 4, cudaMemcpyDeviceToHost,
+                               c->stream2), "d2h");
+            const uint32_t p0 = j == 0 ? 0u : a + 1;
+            ck(cudaMemcpyAsync(host->indptr + p0, d_indptr + p0, size_t(b + 1 - p0) * 4,
+                               cudaMemcpyDeviceToHost, c->stream2), "d2h");
+        }
+        unsigned hshort = 0;
+        ck(cudaMemcpyAsync(&hshort, short_rows, 4, cudaMemcpyDeviceToHost, st), "short rows");
+        ck(cudaStreamSynchronize(st), "re-rank");
+        ck(cudaStreamSynchronize(c->stream2), "d2h");
+        for (int j = 0; j < NCH; ++j) cudaEventDestroy(evs[j]);
+        copied = hshort == 0;  // else the CSR is laid out from the counts below
+    } else {
+        KGScope kg(c, PQ_KG_RERANK);
+        rerank(nullptr, 0, n);
     }
     unsigned long long fixes = 0;
     ck(cudaMemcpyAsync(&fixes, c->d_acc, 8, cudaMemcpyDeviceToHost, st), "fixes");
     // ── 5. NN-Descent rounds from the shortlist lists, then the extract ──
     const Resolved RR = resolve(n64, o);
-    // auto: no polish round for BF16; one for E4M3, whose shortlist misses more
-    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : (fp8 ? 1 : 0);
     int rounds = 0;
     uint32_t* ecnt = c->get<uint32_t>("ecnt", n);
     uint32_t* eoff = c->get<uint32_t>("eoff", n);
@@ -1284,7 +1354,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         launch_extract_count(hidx, n, k, ecnt, st);
         ck(scan_exclusive_u32(ecnt, eoff, n, stemp, c->d_u64, st), "scan extract");
         launch_extract(hidx, hdist, n, k, eoff, d_indptr, d_indices, d_dists, st);
-    } else {
+    } else if (!copied) {
         // the re-ranked lists are already ascending with their entries first
         KGScope kg(c, PQ_KG_EXTRACT);
         k_list_count<<<blocks(n, 256), 256, 0, st>>>(ridx, n, k, ecnt); count_launch();
@@ -1293,9 +1363,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                                                                     d_indptr, d_indices, d_dists);
         count_launch();
     }
-    uint64_t nnz = 0;
-    ck(cudaMemcpyAsync(&nnz, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "nnz");
+    uint64_t nnz = uint64_t(n) * k;
+    if (!copied) ck(cudaMemcpyAsync(&nnz, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "nnz");
     ck(cudaStreamSynchronize(st), "extract");
+    if (host) host->copied = copied;
     S_.ms_extract = tm.stop();
     S_.ms_total = tot.stop();
     S_.shortlist[6] = fixes;

@@ -193,9 +193,19 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
                       uint64_t seed, uint32_t* probes, double* ms_train, double* loss_first,
                       double* loss_last);
 
+// Host destinations of the graph: a build may copy its CSR there itself,
+// overlapping the copy with its last stage (copied = true), else the caller
+// copies the device arrays.
+struct HostGraph {
+    uint32_t* indptr;
+    uint32_t* indices;
+    float* dists;
+    bool copied;
+};
+
 // The chosen form (tensor-core shortlist), chosen.cu.
 uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64,
                       uint64_t d64, const pq_nnd_opts& o, uint32_t* d_indptr,
-                      uint32_t* d_indices, float* d_dists);
+                      uint32_t* d_indices, float* d_dists, HostGraph* host = nullptr);
 
 }  // namespace pqh

@@ -59,6 +59,25 @@ def test_bf16_form_is_deterministic():
     assert a["data"].tobytes() == b["data"].tobytes()
 
 
+def test_bf16_form_host_chunks_above_2_20_cells():
+    """Above 2^20 cells the host-buffer entry point re-ranks in cell-index
+    chunks and copies each chunk to the host while the next is re-ranked:
+    every chunk's rows must hold their own cell's neighbours (sorted, no self,
+    each distance the exact FP32 distance of its pair), at full recall."""
+    n = (1 << 20) + 4321
+    x = synth.mixture_lognormal(n, 50, 30, seed=9)
+    g = pq.nndescent_dense(x, 15, mode="bf16")
+    check_structure(g, n, 15)
+    ix = g["indices"].reshape(-1, 15)
+    dx = g["data"].reshape(-1, 15)
+    for i in np.linspace(0, n - 1, 64).astype(np.int64):  # rows of every chunk
+        for t in range(15):
+            want = np.sqrt(oracle.sq_dist(x[i], x[ix[i, t]]))
+            assert dx[i, t] == np.float32(want)
+    q = np.random.default_rng(3).choice(n, 300, replace=False).astype(np.uint32)
+    assert recall(g, x, 15, q) >= 0.99
+
+
 def test_bf16_form_k30_and_30_pcs():
     x = synth.mixture_lognormal(40_000, 30, 10, seed=3)
     g = pq.nndescent_dense(x, 30, mode="bf16")
