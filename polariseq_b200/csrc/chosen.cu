@@ -44,27 +44,47 @@ __global__ void k_sample_rows(const float* __restrict__ X, int dp, uint32_t n, u
 }
 
 // Column sums of padded rows (for the mean used as the centroid search's BF16 centre).
-__global__ void k_col_sum(const float* __restrict__ X, uint32_t n, int dp, float* sums) {
-    const int j = threadIdx.x;
-    if (j >= dp) return;
+// Column means of n rows: one 256-thread block per column, each thread
+// summing a fixed stride of rows, then a fixed tree (deterministic).
+__global__ void k_col_mean(const float* __restrict__ X, uint32_t n, int dp, float* mean) {
+    __shared__ float part[256];
+    const int j = blockIdx.x;
     float s = 0.f;
-    for (uint32_t i = blockIdx.x; i < n; i += gridDim.x) s += X[size_t(i) * dp + j];
-    atomicAdd(&sums[j], s);
-}
-__global__ void k_scale(float* v, int m, float f) {
-    if (int(threadIdx.x) < m) v[threadIdx.x] *= f;
+    for (uint32_t i = threadIdx.x; i < n; i += blockDim.x) s += X[size_t(i) * dp + j];
+    part[threadIdx.x] = s;
+    __syncthreads();
+    for (int o = 128; o > 0; o >>= 1) {
+        if (int(threadIdx.x) < o) part[threadIdx.x] += part[threadIdx.x + o];
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) mean[j] = part[0] / float(n);
 }
 
-// Lloyd update sums from the tensor-core nearest-centroid labels.
-__global__ void k_kmeans_accumulate(const float* __restrict__ xs, uint32_t ns, int d, int dp,
-                                    const uint32_t* __restrict__ lab, float* __restrict__ sums,
-                                    uint32_t* __restrict__ cnt) {
+// Lloyd update sums from the tensor-core nearest-centroid labels: keys =
+// label (C for none), values = sample index, to be sorted stably by label.
+__global__ void k_label_pairs(const uint32_t* __restrict__ lab, uint32_t ns, uint32_t C,
+                              uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
-    const uint32_t b = lab[i];
-    if (b == 0xFFFFFFFFu) return;
-    atomicAdd(&cnt[b], 1u);
-    for (int j = 0; j < d; ++j) atomicAdd(&sums[size_t(b) * dp + j], xs[size_t(i) * dp + j]);
+    keys[i] = lab[i] < C ? lab[i] : C;
+    vals[i] = i;
+}
+// Per centroid (one warp): its members' sums in sample order (deterministic)
+// and their count; off = the label bounds of the sorted pairs.
+__global__ void k_kmeans_sums(const float* __restrict__ xs, int d, int dp,
+                              const uint64_t* __restrict__ members,
+                              const uint32_t* __restrict__ off, uint32_t C,
+                              float* __restrict__ sums, uint32_t* __restrict__ cnt) {
+    const uint32_t b = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
+    const int lane = threadIdx.x & 31;
+    if (b >= C) return;
+    const uint32_t m0 = off[b], m1 = off[b + 1];
+    for (int j = lane; j < d; j += 32) {
+        float s = 0.f;
+        for (uint32_t m = m0; m < m1; ++m) s += xs[size_t(members[m]) * dp + j];
+        sums[size_t(b) * dp + j] = s;
+    }
+    if (lane == 0) cnt[b] = m1 - m0;
 }
 
 // Query-entry keys and values (slot = position * P + rank) from the probes.  Primary
@@ -874,9 +894,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     k_sample_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, n, ns, xs); count_launch();
     // the sample's mean: the BF16 centre of the centroid search
     float* mean = c->get<float>("mean", dp);
-    ck(cudaMemsetAsync(mean, 0, dp * 4, st), "mean");
-    k_col_sum<<<1024, 64 * ((dp + 63) / 64), 0, st>>>(xs, ns, dp, mean); count_launch();
-    k_scale<<<1, 128, 0, st>>>(mean, dp, 1.0f / float(ns)); count_launch();
+    k_col_mean<<<dp, 256, 0, st>>>(xs, ns, dp, mean); count_launch();
     k_sample_rows<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(xs, dp, ns, C, cent); count_launch();
     __nv_bfloat16* xsb = c->get<__nv_bfloat16>("km_sample_bf16", size_t(ns) * 64);
     float* xsn = c->get<float>("km_sample_norm", ns);
@@ -940,13 +958,21 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         }
     };
     ck(cudaMemsetAsync(c->d_err, 0, 4, st), "err");
+    // the Lloyd sums in a fixed order: members sorted by label
+    uint32_t* lk = c->get<uint32_t>("km_lk", ns);
+    uint64_t* lv = c->get<uint64_t>("km_lv", ns);
+    uint32_t* lk2 = c->get<uint32_t>("km_lk2", ns);
+    uint64_t* lv2 = c->get<uint64_t>("km_lv2", ns);
+    uint8_t* ltemp = c->get<uint8_t>("km_ltemp", radix_temp_bytes(ns));
+    uint32_t* loff = c->get<uint32_t>("km_loff", size_t(C) + 1);
     const int lloyd = 8;
     for (int it = 0; it < lloyd; ++it) {
         k_to_bf16<<<cvt_blocks(C), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
         centroid_search(xsb, xsn, ns, 1, lab_d, lab);
-        ck(cudaMemsetAsync(sums, 0, size_t(C) * dp * 4, st), "km");
-        ck(cudaMemsetAsync(cnt, 0, size_t(C) * 4, st), "km");
-        k_kmeans_accumulate<<<blocks(ns, 256), 256, 0, st>>>(xs, ns, d, dp, lab, sums, cnt); count_launch();
+        k_label_pairs<<<blocks(ns, 256), 256, 0, st>>>(lab, ns, C, lk, lv); count_launch();
+        ck(radix_sort_pairs(lk, lv, lk2, lv2, ns, key_bits(C), ltemp, st), "sort labels");
+        k_key_bounds<<<blocks(size_t(ns) + 1, 256), 256, 0, st>>>(lk, ns, 1, C, loff); count_launch();
+        k_kmeans_sums<<<blocks(C, 8), 256, 0, st>>>(xs, d, dp, lv, loff, C, sums, cnt); count_launch();
         k_kmeans_update<<<blocks(size_t(C) * dp, 256), 256, 0, st>>>(cent, sums, cnt, C, d, dp); count_launch();
     }
     k_to_bf16<<<cvt_blocks(C), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();

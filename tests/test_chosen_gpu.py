@@ -78,6 +78,29 @@ def test_bf16_form_host_chunks_above_2_20_cells():
     assert recall(g, x, 15, q) >= 0.99
 
 
+def test_bf16_form_host_and_device_entry_points_agree():
+    """The build is deterministic (fixed-order reductions throughout): the
+    host-buffer entry point, chunked above 2^20 cells, and the device entry
+    point give the same graph byte for byte."""
+    import torch
+
+    n = (1 << 20) + 4321
+    x = synth.mixture_lognormal(n, 50, 30, seed=9)
+    h = pq.nndescent_dense(x, 15, mode="bf16")
+    dev = torch.device("cuda", 0)
+    xd = torch.from_numpy(x).to(dev)
+    ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    ix = torch.empty(n * 15, dtype=torch.int32, device=dev)
+    dx = torch.empty(n * 15, dtype=torch.float32, device=dev)
+    opts = pq._opts(15, 0, 0, 0, 0, 0.001, mode=pq.MODES["bf16"])
+    nnz = pq.default_context(0).nndescent_device(xd, opts, ip, ix, dx)
+    torch.cuda.synchronize(dev)
+    assert nnz == len(h["indices"]) == n * 15
+    np.testing.assert_array_equal(ip.cpu().numpy().view(np.uint32), h["indptr"])
+    np.testing.assert_array_equal(ix.cpu().numpy().view(np.uint32), h["indices"])
+    assert dx.cpu().numpy().tobytes() == h["data"].tobytes()
+
+
 def test_bf16_form_k30_and_30_pcs():
     x = synth.mixture_lognormal(40_000, 30, 10, seed=3)
     g = pq.nndescent_dense(x, 30, mode="bf16")
