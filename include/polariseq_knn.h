@@ -130,6 +130,14 @@ int pq_ctx_stats(const pq_ctx* ctx, pq_nnd_stats* out);
  * CUDA events on the context's stream (pq_nnd_stats.kg_ms / kg_launches). */
 int pq_ctx_set_profiling(pq_ctx* ctx, int on);
 
+/* Test hook of the bounded device waits (no counterpart in the reference):
+ * with polls > 0, the next tensor-core build's shortlist tile kernels first
+ * wait `polls` polls on an mbarrier that nothing arrives at, before issuing
+ * any copy or MMA; the wait gives up, the kernels exit with nothing in
+ * flight and the build returns PQ_ETIMEOUT.  Applies to one build, after
+ * which the context is usable as before. */
+int pq_ctx_set_test_wait(pq_ctx* ctx, uint32_t polls);
+
 /* nndescent_into (nndescent.rs:688-707) with HOST buffers: data is n_obs x
  * n_dim row-major f32; indptr holds n_obs+1 entries; indices/dists hold at
  * least n_obs * effective_k(n_obs, k).  Writes the CSR graph (Euclidean

@@ -100,6 +100,8 @@ def lib():
         L.oracle_smooth_knn_dist.restype = None
         L.oracle_fuzzy.argtypes = [C.c_uint64, P, P, P, P, P, P, C.c_uint64]
         L.oracle_fuzzy.restype = C.c_uint64
+        L.oracle_knn_exact_batched.argtypes = [P, C.c_int, C.c_uint32, P, P, P]
+        L.oracle_knn_exact_batched.restype = None
         _lib = L
     return _lib
 
@@ -281,3 +283,23 @@ def fuzzy_connectivities(indptr, indices, data, n_obs: int) -> dict:
     ow = np.zeros(cap, np.float32)
     nnz = lib().oracle_fuzzy(n_obs, _ptr(ip), _ptr(ix), _ptr(dx), _ptr(oip), _ptr(oix), _ptr(ow), cap)
     return {"indptr": oip, "indices": oix[:nnz].copy(), "data": ow[:nnz].copy()}
+
+
+def knn_exact_batched(samples, ks) -> list:
+    """The reference's tiled exact per-sample kNN (doublets.rs:544-650,
+    restated in knn_exact_ref.cpp) over every sample, all threads: a list of
+    (n_s, k_s) u32 index arrays, itself excluded, (distance, index) order."""
+    L = lib()
+    d = samples[0].shape[1]
+    data = np.ascontiguousarray(np.concatenate(samples).astype(np.float32, copy=False))
+    offs = np.zeros(len(samples) + 1, np.uint64)
+    offs[1:] = np.cumsum([len(s) for s in samples])
+    kk = np.asarray(ks, np.uint32)
+    out = np.zeros(int(sum(len(s) * int(k) for s, k in zip(samples, ks))), np.uint32)
+    L.oracle_knn_exact_batched(_ptr(data), int(d), len(samples), _ptr(offs), _ptr(kk), _ptr(out))
+    res, o = [], 0
+    for s, k in zip(samples, ks):
+        m = len(s) * int(k)
+        res.append(out[o:o + m].reshape(len(s), int(k)))
+        o += m
+    return res

@@ -28,7 +28,7 @@ import numpy as np
 from . import _lib
 
 __all__ = [
-    "PanicException", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
+    "PanicException", "DeviceError", "DeviceTimeout", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
     "neighbors_dense", "knn_batched", "fuzzy_connectivities",
 ]
 
@@ -40,6 +40,11 @@ class PanicException(BaseException):
 
 class DeviceError(RuntimeError):
     pass
+
+
+class DeviceTimeout(DeviceError):
+    """A bounded device-side wait gave up (PQ_ETIMEOUT); the context stays
+    usable."""
 
 
 def effective_k(n_obs: int, k: int) -> int:
@@ -104,6 +109,8 @@ class Context:
             raise NotImplementedError(f"{what}: {msg}")
         if rc == _lib.PQ_ENOMEM:
             raise MemoryError(f"{what}: {msg}")
+        if rc == _lib.PQ_ETIMEOUT:
+            raise DeviceTimeout(f"{what}: {msg}")
         raise DeviceError(f"{what} failed (status {rc}): {msg}")
 
     def stats(self) -> dict:

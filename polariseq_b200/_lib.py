@@ -25,6 +25,7 @@ EXPORTS = (
     "pq_nndescent_probe", "pq_debug_tree", "pq_ctx_set_profiling", "pq_neighbors_into",
     "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc", "pq_knn_batched_into_device",
     "pq_mlp_params", "pq_mlp_grad", "pq_fuzzy_connectivities", "pq_fuzzy_connectivities_device",
+    "pq_ctx_set_test_wait",
 )
 
 
@@ -117,6 +118,8 @@ def load(build_if_missing: bool = False):
         L.pq_ctx_stats.restype = C.c_int
         L.pq_ctx_set_profiling.argtypes = [P, C.c_int]
         L.pq_ctx_set_profiling.restype = C.c_int
+        L.pq_ctx_set_test_wait.argtypes = [P, C.c_uint32]
+        L.pq_ctx_set_test_wait.restype = C.c_int
         L.pq_nndescent_into.argtypes = [P, P, U64, U64, C.POINTER(NndOpts), P, U64, P, U64, P,
                                         U64, C.POINTER(U64)]
         L.pq_nndescent_into.restype = C.c_int

@@ -46,6 +46,61 @@ __global__ void k_iota_trees(uint32_t* ids, uint32_t n, uint32_t T) {
     if (i < size_t(n) * T) ids[i] = uint32_t(i % n);
 }
 
+// Records of one round's join beyond which the round is replayed in
+// source-row chunks (a memory bound: 24 bytes of sort buffers per record).
+// POLARISEQ_JOIN_CHUNK overrides it (tests force many small chunks).
+uint64_t join_chunk_records() {
+    if (const char* e = std::getenv("POLARISEQ_JOIN_CHUNK")) {
+        const unsigned long long v = std::strtoull(e, nullptr, 10);
+        if (v >= 2) return v;
+    }
+    return uint64_t(1) << 30;
+}
+
+__global__ void k_widen_u32(const uint32_t* __restrict__ in, uint32_t n, uint64_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i];
+}
+__global__ void k_low_u32(const uint64_t* __restrict__ in, uint32_t n, uint32_t* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = uint32_t(in[i]);
+}
+// bnd[j] = the first row whose exclusive record prefix reaches j * half
+// (bnd[0] = 0, bnd[J] = n): every chunk holds less than half + one row's
+// records.
+__global__ void k_chunk_bounds(const uint64_t* __restrict__ pre, uint32_t n, uint64_t half,
+                               uint32_t J, uint32_t* __restrict__ bnd) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > J) return;
+    if (j == 0 || j == J) {
+        bnd[j] = j == 0 ? 0u : n;
+        return;
+    }
+    const uint64_t target = uint64_t(j) * half;
+    uint32_t lo = 0, hi = n;  // first i in [0, n) with pre[i] >= target, else n
+    while (lo < hi) {
+        const uint32_t mid = lo + (hi - lo) / 2;
+        if (pre[mid] >= target) hi = mid; else lo = mid + 1;
+    }
+    bnd[j] = lo;
+}
+// (chunk of row perm[t], perm[t]): sorted stably by chunk, the rows of each
+// chunk in perm order.
+__global__ void k_chunk_keys(const uint32_t* __restrict__ perm, uint32_t n,
+                             const uint32_t* __restrict__ bnd, uint32_t J,
+                             uint32_t* __restrict__ keys, uint64_t* __restrict__ vals) {
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const uint32_t i = perm ? perm[t] : t;
+    uint32_t lo = 0, hi = J;  // the last j with bnd[j] <= i
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) / 2;
+        if (bnd[mid] <= i) lo = mid; else hi = mid;
+    }
+    keys[t] = lo;
+    vals[t] = i;
+}
+
 // Host-side probe destinations.
 struct Probe {
     int32_t stop_after = -2;
@@ -91,6 +146,41 @@ float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, in
     pq::count_launch();
     ck(cudaGetLastError(), "pad embedding");
     return X;
+}
+
+// The records of source rows [a, b) (offsets row_off[a..b) local to the
+// chunk, `total` of them): written in generation order, sorted stably by
+// destination and replayed into the heaps.  `rows` lists the chunk's rows in
+// the order the CTAs take them.
+void replay_join_chunk(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m,
+                       const uint32_t* new_idx, const uint32_t* old_idx, const uint32_t* rows,
+                       const uint32_t* bits, int words, const uint32_t* row_cnt,
+                       const uint32_t* row_off, uint32_t a, uint32_t b, uint64_t total,
+                       uint32_t* dcnt, uint32_t* seg_off, void* stemp, uint32_t* hidx,
+                       float* hdist, uint8_t* hflag) {
+    using namespace pq;
+    cudaStream_t st = c->stream;
+    uint32_t* jk = c->get<uint32_t>("jkeys", total);
+    uint64_t* jv = c->get<uint64_t>("jvals", total);
+    uint32_t* jk2 = c->get<uint32_t>("jkeys2", total);
+    uint64_t* jv2 = c->get<uint64_t>("jvals2", total);
+    void* rtj = c->get<uint8_t>("radix_temp_j", radix_temp_bytes(total));
+    ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
+    {
+        KGScope kg(c, PQ_KG_JOIN_WRITE);
+        launch_join_write(X, d, dp, b - a, m, new_idx, old_idx, rows, bits, words, row_cnt,
+                          row_off, jk, jv, dcnt, st);
+    }
+    {
+        KGScope kg(c, PQ_KG_SORT);
+        ck(radix_sort_pairs(jk, jv, jk2, jv2, total, key_bits(n > 1 ? n - 1 : 1), rtj, st),
+           "sort join");
+        ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan replay");
+    }
+    {
+        KGScope kg(c, PQ_KG_REPLAY);
+        launch_replay(jk, jv, seg_off, dcnt, n, k, hidx, hdist, hflag, c->d_acc + 1, st);
+    }
 }
 
 int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m, uint64_t seed,
@@ -141,36 +231,60 @@ int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int 
         uint64_t total = 0;
         ck(cudaMemcpyAsync(&total, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "total");
         ck(cudaStreamSynchronize(st), "join count");
-        if (total >= 0xFFFFFFFFull) throw DeviceError{"join: more than 2^32 updates in a round"};
-        uint64_t changed = 0;
-        if (total > 0) {
-            uint32_t* jk = c->get<uint32_t>("jkeys", total);
-            uint64_t* jv = c->get<uint64_t>("jvals", total);
-            uint32_t* jk2 = c->get<uint32_t>("jkeys2", total);
-            uint64_t* jv2 = c->get<uint64_t>("jvals2", total);
-            void* rtj = c->get<uint8_t>("radix_temp_j", radix_temp_bytes(total));
-            ck(cudaMemsetAsync(dcnt, 0, size_t(n) * 4, st), "memset dcnt");
-            {
-                KGScope kg(c, PQ_KG_JOIN_WRITE);
-                launch_join_write(X, d, dp, n, m, new_idx, old_idx, perm, bits, words, row_cnt,
-                                  row_off, jk, jv, dcnt, st);
-            }
-            {
-                KGScope kg(c, PQ_KG_SORT);
-                ck(radix_sort_pairs(jk, jv, jk2, jv2, total, key_bits(n > 1 ? n - 1 : 1), rtj,
-                                    st),
-                   "sort join");
-                ck(scan_exclusive_u32(dcnt, seg_off, n, stemp, nullptr, st), "scan replay");
-            }
-            {
-                KGScope kg(c, PQ_KG_REPLAY);
-                launch_replay(jk, jv, seg_off, dcnt, n, k, hidx, hdist, hflag, c->d_acc + 1, st);
+        const uint64_t cap = join_chunk_records();
+        if (total > 0 && total <= cap) {
+            replay_join_chunk(c, X, d, dp, n, k, m, new_idx, old_idx, perm, bits, words, row_cnt,
+                              row_off, 0, n, total, dcnt, seg_off, stemp, hidx, hdist, hflag);
+        } else if (total > cap) {
+            // source-row chunks [b_j, b_j+1) in index order, each holding at
+            // most cap records: replaying them one after another keeps every
+            // destination's updates in generation order (the reference applies
+            // its 4096-row blocks the same way, nndescent.rs:916-969)
+            uint64_t* pre = c->get<uint64_t>("join_pre", size_t(n) + 1);
+            const uint64_t half = cap / 2;
+            const uint32_t J = uint32_t((total + half - 1) / half);
+            uint32_t* bnd = c->get<uint32_t>("join_bounds", size_t(J) + 1);
+            k_widen_u32<<<blocks(n, 256), 256, 0, st>>>(row_cnt, n, pre); count_launch();
+            ck(scan_exclusive_u64(pre, pre, n, c->get<uint8_t>("scan_temp64", scan_temp_bytes(n)),
+                                  nullptr, st),
+               "scan join 64");
+            k_chunk_bounds<<<blocks(size_t(J) + 1, 256), 256, 0, st>>>(pre, n, half, J, bnd);
+            count_launch();
+            std::vector<uint32_t> hb(size_t(J) + 1);
+            ck(cudaMemcpyAsync(hb.data(), bnd, (size_t(J) + 1) * 4, cudaMemcpyDeviceToHost, st),
+               "bounds");
+            // the join CTAs of each chunk keep the spatially coherent order:
+            // the rows in perm order, stably grouped by chunk
+            uint32_t* ck_k = c->get<uint32_t>("join_ck", n);
+            uint64_t* ck_v = c->get<uint64_t>("join_cv", n);
+            uint32_t* ck_k2 = c->get<uint32_t>("join_ck2", n);
+            uint64_t* ck_v2 = c->get<uint64_t>("join_cv2", n);
+            k_chunk_keys<<<blocks(n, 256), 256, 0, st>>>(perm, n, bnd, J, ck_k, ck_v);
+            count_launch();
+            ck(radix_sort_pairs(ck_k, ck_v, ck_k2, ck_v2, n, key_bits(J > 1 ? J - 1 : 1),
+                                c->get<uint8_t>("radix_temp_ck", radix_temp_bytes(n)), st),
+               "sort chunks");
+            uint32_t* cperm = c->get<uint32_t>("join_cperm", n);
+            k_low_u32<<<blocks(n, 256), 256, 0, st>>>(ck_v, n, cperm); count_launch();
+            ck(cudaStreamSynchronize(st), "bounds");
+            for (uint32_t j = 0; j < J; ++j) {
+                const uint32_t a = hb[j], b = hb[j + 1];
+                if (b <= a) continue;
+                ck(scan_exclusive_u32(row_cnt + a, row_off + a, b - a, stemp, c->d_u64, st),
+                   "scan chunk");
+                uint64_t tj = 0;
+                ck(cudaMemcpyAsync(&tj, c->d_u64, 8, cudaMemcpyDeviceToHost, st), "chunk total");
+                ck(cudaStreamSynchronize(st), "chunk total");
+                if (tj == 0) continue;  // (tj < cap / 2 + one row's records)
+                replay_join_chunk(c, X, d, dp, n, k, m, new_idx, old_idx, cperm + a, bits, words,
+                                  row_cnt, row_off, a, b, tj, dcnt, seg_off, stemp, hidx, hdist,
+                                  hflag);
             }
         }
         unsigned long long acc[2];
         ck(cudaMemcpyAsync(acc, c->d_acc, sizeof(acc), cudaMemcpyDeviceToHost, st), "acc");
         ck(cudaStreamSynchronize(st), "round");
-        changed = acc[1];
+        const uint64_t changed = acc[1];
         const uint64_t slot = stats_offset + iter;
         if (slot < 64) {
             S.changed[slot] = changed;
@@ -529,17 +643,25 @@ int check_neighbors(pq_ctx* c, uint64_t n, uint64_t d, uint64_t nn, int32_t metr
     return PQ_OK;
 }
 
+// Runs f, mapping its exceptions to status codes.  On an error both of the
+// context's streams are drained before returning, so no copy into the
+// caller's buffers is still in flight when the caller sees the status.
 template <class F>
 int guarded(pq_ctx* c, F&& f) {
+    auto drain = [c]() {
+        cudaStreamSynchronize(c->stream);
+        cudaStreamSynchronize(c->stream2);
+        cudaGetLastError();
+    };
     try {
         if (cudaSetDevice(c->device) != cudaSuccess)
             return fail(c, PQ_EDEVICE, "cudaSetDevice failed");
         return f();
     } catch (const DeviceError& e) {
-        cudaGetLastError();
-        return fail(c, PQ_EDEVICE, e.msg);
+        drain();
+        return fail(c, e.timeout ? PQ_ETIMEOUT : PQ_EDEVICE, e.msg);
     } catch (const std::string& s) {
-        cudaGetLastError();
+        drain();
         return fail(c, PQ_ENOMEM, s);
     }
 }
@@ -610,6 +732,12 @@ const char* pq_ctx_last_error(const pq_ctx* c) { return c ? c->err.c_str() : "nu
 int pq_ctx_set_profiling(pq_ctx* c, int on) {
     if (!c) return PQ_EINVAL;
     c->profile = on ? 1 : 0;
+    return PQ_OK;
+}
+
+int pq_ctx_set_test_wait(pq_ctx* c, uint32_t polls) {
+    if (!c) return PQ_EINVAL;
+    c->test_wait_polls = polls;
     return PQ_OK;
 }
 

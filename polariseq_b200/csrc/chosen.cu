@@ -12,8 +12,9 @@
 //   4. re-rank: per cell, the R best of its P*S shortlist by approximate
 //      distance get their exact FP32 squared distance in the reference's
 //      summation order (simd.rs:43-62), sorted by (distance, index); where the
-//      k-th and (k+1)-th differ by less than the FP32 error bound, the band is
-//      re-ordered by FP64 distances;
+//      k-th and (k+1)-th differ by less than the FP32 error bound, FP64
+//      distances choose which of the band's entries are kept, and the kept
+//      entries are written in ascending FP32 order;
 //   5. optional NN-Descent rounds (the plain form's round kernels) polish the
 //      lists; the extract writes the CSR graph.
 #include <cuda_bf16.h>
@@ -601,8 +602,8 @@ __device__ __forceinline__ double sq_dist_f64(const float* a, const float* b, in
 // the R best approximate candidates, give
 // them exact FP32 squared distances in the reference's summation order, sort
 // by (distance, index), and where the k-th and (k+1)-th differ by less than
-// the FP32 error bound re-order that band by FP64 distance.  Writes the k
-// nearest (ascending) per cell.
+// the FP32 error bound let FP64 distances choose which of that band's entries
+// are kept.  Writes the k nearest per cell, ascending by FP32 distance.
 template <int D>
 __global__ void __launch_bounds__(128) k_rerank(
     const float* __restrict__ X, const float* __restrict__ xp, int d, int dp, uint32_t n, int k,
@@ -758,6 +759,28 @@ __global__ void __launch_bounds__(128) k_rerank(
                 band_f[w][b + 1] = xf;
                 band_i[w][b + 1] = y;
             }
+            // FP64 decides which band entries fill places b0..k-1; they are
+            // written in ascending FP32 order (FP64, then index, on equal
+            // FP32 values), so every row stays ascending (nndescent.rs:989).
+            // Entries before b0 lie below the band's FP32 range.
+            for (int a = b0 + 1; a < k; ++a) {
+                const double x = band_d[w][a];
+                const float xf = band_f[w][a];
+                const uint32_t y = band_i[w][a];
+                int b = a - 1;
+                while (b >= b0 &&
+                       (band_f[w][b] > xf ||
+                        (band_f[w][b] == xf &&
+                         (band_d[w][b] > x || (band_d[w][b] == x && band_i[w][b] > y))))) {
+                    band_d[w][b + 1] = band_d[w][b];
+                    band_f[w][b + 1] = band_f[w][b];
+                    band_i[w][b + 1] = band_i[w][b];
+                    --b;
+                }
+                band_d[w][b + 1] = x;
+                band_f[w][b + 1] = xf;
+                band_i[w][b + 1] = y;
+            }
             atomicAdd(boundary_fixes, 1ull);
         }
         __syncwarp();
@@ -827,6 +850,30 @@ __global__ void k_list_dense(const uint32_t* __restrict__ li, const float* __res
         if (i == 0) indptr[0] = 0;
     }
 }
+
+// Sets *flag when a cell's shortlist runs hold fewer than k live entries in
+// all (the tile kernel never lists a cell itself and a candidate lies in one
+// bucket only, so the cell's row will have fewer than k neighbours).
+__global__ void k_short_rows(const uint8_t* __restrict__ sn, uint32_t n, int runs, int k,
+                             unsigned* __restrict__ flag) {
+    const uint32_t p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    int t = 0;
+    for (int l = 0; l < runs; ++l) t += sn[size_t(p) * runs + l];
+    if (t < k) atomicOr(flag, 1u);
+}
+
+// Events owned by one scope: destroyed on every exit, exceptions included.
+struct EventSet {
+    std::vector<cudaEvent_t> ev;
+    explicit EventSet(int count) : ev(count, nullptr) {
+        for (auto& e : ev) pqh::ck(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "event");
+    }
+    ~EventSet() {
+        for (auto e : ev)
+            if (e) cudaEventDestroy(e);
+    }
+};
 
 // Sorted (ascending) lists -> neighbour heaps: a descending array is a valid
 // max-heap; every entry starts new.
@@ -994,7 +1041,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     }
     int herr0 = 0;
     ck(cudaMemcpy(&herr0, c->d_err, 4, cudaMemcpyDeviceToHost), "err");
-    if (herr0) throw DeviceError{"centroid tiles: a bounded wait gave up"};
+    if (herr0) throw DeviceError{"centroid tiles: a bounded wait gave up", herr0 == 2};
     const size_t ne = size_t(n) * P;
     uint32_t* ekeys = c->get<uint32_t>("ekeys", ne);
     uint64_t* evals = c->get<uint64_t>("evals", ne);
@@ -1167,6 +1214,9 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         // (the E4M3 ranking error is larger: 2k places)
         const int R0 = std::min(Sout, fp8 ? 2 * k : k + 2);
         uint64_t pruned = 0;
+        // the timeout test hook applies to this build's two tile passes once
+        const uint32_t test_wait = c->test_wait_polls;
+        c->test_wait_polls = 0;
         for (int pass = 0; pass < 2; ++pass) {
             if (pass == 1) {
                 // the other-probe entries that can admit anything, compacted
@@ -1253,6 +1303,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.out_slot = eslot;
             a.err = c->d_err;
             a.trace = tbuf;
+            a.test_wait_polls = test_wait;
             {
                 KGScope kg(c, PQ_KG_TILES);
                 ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "ivf tiles");
@@ -1295,7 +1346,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     int herr = 0;
     ck(cudaMemcpyAsync(&herr, c->d_err, 4, cudaMemcpyDeviceToHost, st), "err");
     ck(cudaStreamSynchronize(st), "ivf tiles");
-    if (herr) throw DeviceError{"tensor-core tiles: a bounded wait gave up"};
+    if (herr) throw DeviceError{"tensor-core tiles: a bounded wait gave up", herr == 2};
     S_.ms_rounds = tm.stop();
 
     // ── 4. re-rank ──
@@ -1324,15 +1375,24 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     // index order, a chunk at a time, and each chunk's CSR rows (full rows:
     // row i at i * k) are copied to the host on the second stream while the
     // next chunk is re-ranked
-    const bool overlap = host != nullptr && polish == 0 && n >= (1u << 20);
+    // (only when no row can be short: a short row moves the CSR rows, and the
+    // host arrays past nnz must stay untouched)
+    bool overlap = host != nullptr && polish == 0 && n >= (1u << 20);
+    unsigned* short_rows = reinterpret_cast<unsigned*>(c->d_acc + 1);
+    if (overlap) {
+        unsigned hshort = 0;
+        k_short_rows<<<blocks(n, 256), 256, 0, st>>>(sn, n, P * ivf_groups(), k, short_rows);
+        count_launch();
+        ck(cudaMemcpyAsync(&hshort, short_rows, 4, cudaMemcpyDeviceToHost, st), "short rows");
+        ck(cudaStreamSynchronize(st), "short rows");
+        overlap = hshort == 0;
+    }
     bool copied = false;
     if (overlap) {
         KGScope kg(c, PQ_KG_RERANK);
-        unsigned* short_rows = reinterpret_cast<unsigned*>(c->d_acc + 1);
         const int NCH = 8;
-        cudaEvent_t evs[NCH];
-        for (int j = 0; j < NCH; ++j)
-            ck(cudaEventCreateWithFlags(&evs[j], cudaEventDisableTiming), "event");
+        EventSet es(NCH);
+        cudaEvent_t* evs = es.ev.data();
         for (int j = 0; j < NCH; ++j) {
             const uint32_t a = uint32_t(uint64_t(n) * j / NCH), b = uint32_t(uint64_t(n) * (j + 1) / NCH);
             if (b == a) continue;
@@ -1356,8 +1416,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         ck(cudaMemcpyAsync(&hshort, short_rows, 4, cudaMemcpyDeviceToHost, st), "short rows");
         ck(cudaStreamSynchronize(st), "re-rank");
         ck(cudaStreamSynchronize(c->stream2), "d2h");
-        for (int j = 0; j < NCH; ++j) cudaEventDestroy(evs[j]);
-        copied = hshort == 0;  // else the CSR is laid out from the counts below
+        copied = hshort == 0;  // (checked above; else laid out from the counts below)
     } else {
         KGScope kg(c, PQ_KG_RERANK);
         rerank(nullptr, 0, n);

@@ -26,6 +26,7 @@ struct Resolved {
 
 struct DeviceError {
     std::string msg;
+    bool timeout = false;  // a bounded device-side wait gave up (PQ_ETIMEOUT)
 };
 
 inline void ck(cudaError_t e, const char* where) {
@@ -106,6 +107,7 @@ struct pq_ctx {
     cudaStream_t stream2 = nullptr;  // the largest subtrees run here, concurrently
     cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     int profile = 0;
+    uint32_t test_wait_polls = 0;  // pq_ctx_set_test_wait: the next tile passes give up
     struct KGRec {
         cudaEvent_t a, b;
         int group;

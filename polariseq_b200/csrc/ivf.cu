@@ -69,6 +69,7 @@ struct __align__(8) IvfBars {
     uint64_t c_full[MAXCS], c_empty[MAXCS];
     uint64_t t_full[2], t_empty[2];
     uint64_t done;
+    uint64_t never;  // nothing arrives here: the target of the timeout test hook
     uint32_t tmem;
     int abort;
 };
@@ -162,8 +163,11 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             tc::mbar_init(&B.t_empty[s], NEPI / 32);
         }
         tc::mbar_init(&B.done, 1);
+        tc::mbar_init(&B.never, 1);
         tc::fence_barrier_init();
         B.abort = 0;
+        // the timeout test hook: a bounded wait that runs out before any work
+        if (a.test_wait_polls && !tc::mbar_wait(&B.never, 0, a.test_wait_polls)) B.abort = 1;
     }
     if (tid == NEPI) {
         tc::prefetch_tmap(&tmQ);

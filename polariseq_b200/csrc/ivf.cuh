@@ -44,6 +44,11 @@ struct IvfTileArgs {
     const uint32_t* out_slot;
     int* err;
     unsigned long long* trace;  // optional: block 0 cycle counters (IVF_T_*)
+    // test hook: when non-zero, thread 0 of every CTA first waits this many
+    // polls on a barrier that nothing arrives at, before any copy or MMA is
+    // issued; the wait gives up, every role skips its jobs and the kernel
+    // reports error 2 (a bounded wait gave up) with nothing in flight
+    uint32_t test_wait_polls;
 };
 
 enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT_C = 3,

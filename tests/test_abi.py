@@ -80,3 +80,67 @@ def test_null_context_and_args_are_rejected_without_a_device():
     assert L.pq_nndescent_into(None, None, 10, 3, C.byref(o), None, 11, None, 0, None, 0,
                                C.byref(nnz)) == _lib.PQ_EINVAL
     assert L.pq_ctx_last_error(None) == b"null context"
+
+
+# ── struct layouts: the header (compiled by a C compiler), the ctypes binding
+#    and the Rust binding documented in INTEGRATION.md must agree byte for byte
+
+def _c_layout(tmp_path, struct, fields):
+    """sizeof and every field's offset of `struct` as gcc lays it out from
+    include/polariseq_knn.h."""
+    import shutil
+    import subprocess
+
+    cc = shutil.which("gcc") or shutil.which("cc")
+    if cc is None:
+        pytest.skip("no C compiler")
+    lines = ['#include <stddef.h>', '#include <stdio.h>', '#include "polariseq_knn.h"',
+             'int main(void) {', f'  printf("%zu\\n", sizeof({struct}));']
+    lines += [f'  printf("%zu\\n", offsetof({struct}, {f}));' for f in fields]
+    lines += ['  return 0;', '}']
+    src = tmp_path / f"{struct}.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / struct
+    subprocess.run([cc, "-std=c99", "-I", os.path.dirname(HEADER), str(src), "-o", str(exe)],
+                   check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split()
+    return int(out[0]), [int(v) for v in out[1:]]
+
+
+@pytest.mark.parametrize("struct,cls", [("pq_nnd_opts", _lib.NndOpts),
+                                        ("pq_nnd_stats", _lib.NndStats)])
+def test_ctypes_structs_match_the_header_layout(tmp_path, struct, cls):
+    names = [f[0] for f in cls._fields_]
+    size, offs = _c_layout(tmp_path, struct, names)
+    assert C.sizeof(cls) == size, f"{struct}: ctypes {C.sizeof(cls)} bytes, C {size}"
+    assert [getattr(cls, f).offset for f in names] == offs
+
+
+def _rust_repr_c_layout(body):
+    """Size and field offsets of a #[repr(C)] Rust struct body with scalar
+    fields (the C layout rules: each field at the next multiple of its
+    alignment, the size rounded up to the largest alignment)."""
+    sizes = {"u64": 8, "i64": 8, "f64": 8, "u32": 4, "i32": 4, "f32": 4, "u8": 1, "i8": 1}
+    fields = re.findall(r"pub\s+(\w+)\s*:\s*(\w+)", body)
+    off, offs, align = 0, [], 1
+    for name, ty in fields:
+        s = sizes[ty]
+        off = (off + s - 1) // s * s
+        offs.append((name, off))
+        off += s
+        align = max(align, s)
+    return (off + align - 1) // align * align, offs
+
+
+def test_documented_rust_binding_matches_the_header(tmp_path):
+    """The PqNndOpts struct a maintainer would paste from INTEGRATION.md has
+    the header's field names, order, offsets and size."""
+    doc = open(os.path.join(os.path.dirname(HEADER), "..", "INTEGRATION.md")).read()
+    m = re.search(r"pub struct PqNndOpts\s*\{(.*?)\}", doc, flags=re.S)
+    assert m, "no PqNndOpts in INTEGRATION.md"
+    size, offs = _rust_repr_c_layout(m.group(1))
+    names = [f[0] for f in _lib.NndOpts._fields_]
+    assert [n for n, _ in offs] == names
+    c_size, c_offs = _c_layout(tmp_path, "pq_nnd_opts", names)
+    assert size == c_size
+    assert [o for _, o in offs] == c_offs

@@ -139,3 +139,64 @@ def test_fp8_form_rejects_large_k():
     x = synth.mixture_dirichlet(5000, 50, 5, seed=1)
     with pytest.raises(NotImplementedError):
         pq.nndescent_dense(x, 30, mode="fp8")
+
+
+def test_bf16_form_every_row_ascending_at_4m():
+    """At 4M cells thousands of cells go through the FP64 boundary step (the
+    k-th and (k+1)-th FP32 distances within the FP32 error bound).  FP64 only
+    chooses which entries are kept: every row of the whole graph is still
+    ascending, without self-loops or repeated neighbours."""
+    import torch
+
+    n, k = 4_000_000, 15
+    x = synth.mixture_lognormal(n, 50, 60, seed=1000)
+    dev = torch.device("cuda", 0)
+    xd = torch.from_numpy(x).to(dev)
+    ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    ix = torch.empty(n * k, dtype=torch.int32, device=dev)
+    dx = torch.empty(n * k, dtype=torch.float32, device=dev)
+    ctx = pq.default_context(0)
+    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES["bf16"])
+    nnz = ctx.nndescent_device(xd, opts, ip, ix, dx)
+    torch.cuda.synchronize(dev)
+    assert nnz == n * k
+    assert ctx.stats()["shortlist"][6] > 0, "no cell went through the FP64 boundary step"
+    rows = ix.view(n, k).long()
+    d = dx.view(n, k)
+    assert bool((d[:, 1:] >= d[:, :-1]).all()), "a row is not ascending"
+    assert not bool((rows == torch.arange(n, device=dev)[:, None]).any()), "self-loop"
+    srt = rows.sort(dim=1).values
+    assert bool((srt[:, 1:] != srt[:, :-1]).all()), "repeated neighbour"
+
+
+def test_a_bounded_wait_that_gives_up_returns_timeout_and_the_context_recovers():
+    """The tile kernel's bounded waits: the test hook makes every CTA wait on
+    an mbarrier that nothing arrives at, with a short poll limit, before it
+    issues any copy or MMA.  The wait runs out, the kernel exits with nothing
+    in flight, the build returns PQ_ETIMEOUT (DeviceTimeout), and the next
+    build on the same context gives the normal graph."""
+    import ctypes as C
+
+    from polariseq_b200 import _lib
+
+    n, k = 100_000, 15
+    x = synth.mixture_lognormal(n, 50, 20, seed=4)
+    ctx = pq.Context(0)
+    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES["bf16"])
+
+    def build():
+        ip = np.zeros(n + 1, np.uint32)
+        ix = np.zeros(n * k, np.uint32)
+        dx = np.zeros(n * k, np.float32)
+        nnz = ctx.nndescent_into(x, opts, ip, ix, dx)
+        return nnz, ip, ix, dx
+
+    want = build()
+    assert _lib.load().pq_ctx_set_test_wait(ctx._h, C.c_uint32(1000)) == _lib.PQ_OK
+    with pytest.raises(pq.DeviceTimeout):
+        build()
+    got = build()
+    assert got[0] == want[0]
+    for a, b in zip(got[1:], want[1:]):
+        assert a.tobytes() == b.tobytes()
+    ctx.close()

@@ -107,6 +107,22 @@ def test_c1_graph_is_bit_exact(c1):
     assert st["changed"] == rp["round_changed"].tolist()
 
 
+def test_join_in_small_source_row_chunks_is_bit_exact(c1, monkeypatch):
+    """A round whose join records exceed the chunk cap is replayed in
+    source-row chunks (index ranges, one after another).  Forcing a cap of
+    200,000 records splits every round at 20k x 50 into tens of chunks; the
+    graph and the per-round change counts stay those of the oracle."""
+    monkeypatch.setenv("POLARISEQ_JOIN_CHUNK", "200000")
+    g = pq.nndescent_dense(c1, 15, 0, 0)
+    st = pq.default_context(0).stats()
+    monkeypatch.delenv("POLARISEQ_JOIN_CHUNK")
+    r = oracle.nndescent(c1, 15, seed=0)
+    assert_graph_equal(g, r, "20k x 50 k=15, chunked join")
+    assert max(st["emitted"]) > 2 * 200_000, "the cap did not force several chunks"
+    rp = oracle.nndescent_probe(c1, 15, seed=0)
+    assert st["changed"] == rp["round_changed"].tolist()
+
+
 @pytest.mark.parametrize("n,d,k,seed,ncl", [
     (3000, 10, 12, 42, 7), (2000, 8, 10, 1, 5), (1500, 6, 9, 5, 4), (4000, 13, 30, 3, 6),
     (900, 50, 15, 9, 3), (64, 4, 15, 1, 2),

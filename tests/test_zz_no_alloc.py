@@ -87,11 +87,25 @@ def test_on_a_caller_stream():
 
 
 def test_rejects_beyond_its_limits():
+    """Each rejected call returns its code and leaves *nnz_out untouched."""
     torch = pytest.importorskip("torch")
     too_many = torch.zeros((262_145, 1), dtype=torch.float32, device="cuda")
-    assert _noalloc(torch, too_many, 2, "euclidean")[0] == _lib.PQ_ETOOBIG
     x = torch.zeros((10, 3), dtype=torch.float32, device="cuda")
-    assert _noalloc(torch, x, 0, "euclidean")[0] == _lib.PQ_EINVAL
-    assert _noalloc(torch, x[:0], 5, "euclidean")[0] == _lib.PQ_EINVAL
     wide = torch.zeros((10, 513), dtype=torch.float32, device="cuda")
-    assert _noalloc(torch, wide, 5, "euclidean")[0] == _lib.PQ_ENOTSUP
+    for data, k, want in ((too_many, 2, _lib.PQ_ETOOBIG), (x, 0, _lib.PQ_EINVAL),
+                          (x[:0], 5, _lib.PQ_EINVAL), (wide, 5, _lib.PQ_ENOTSUP)):
+        rc, nnz = _noalloc(torch, data, k, "euclidean")[:2]
+        assert rc == want
+        assert nnz == 0
+
+
+def test_accepts_exactly_its_row_limit():
+    """262,144 rows fill the fixed norm array to its last element: accepted,
+    and equal to the context path."""
+    torch = pytest.importorskip("torch")
+    g = np.random.default_rng(24)
+    x = torch.from_numpy(g.standard_normal((262_144, 2)).astype(np.float32)).cuda()
+    want = _with_context(torch, x, 3, "cosine")
+    rc, nnz, ip, ix, dx = _noalloc(torch, x, 3, "cosine")
+    assert rc == _lib.PQ_OK
+    _same((nnz, ip, ix, dx), want)
