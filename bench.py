@@ -10,10 +10,17 @@ data standing in for a PCA embedding; no dataset is needed or available).
          host->device copy and the graph's device->host copy are inside the
          timed region
   roofline  the dominant kernel's algorithmic work per launch (flops for the
-         tensor-core tiles, bytes for the plain form's join) over its CUDA-event
-         duration, against the measured peak (sustained BF16 GEMM, HBM copy)
+         tensor-core tiles, bytes for the plain form's subtrees) over its
+         CUDA-event duration, against the measured peak (sustained BF16 GEMM,
+         HBM copy)
   cpu_baseline  the C++ restatement of the reference's CPU NN-Descent (oracle/)
-         on a bounded sample of the same workload, all host threads
+         on the whole workload, all host threads; the same build checks the
+         plain form's graph byte for byte (plain_bit_exact)
+  forms  the plain form at the reference defaults and with the reference
+         options that reach recall@15 >= 0.99 (plain_r99), the BF16 and E4M3
+         shortlist forms; forms_k30 the same at k = 30
+  configs  1.3M x 50 (plain, plain_r99, BF16) and the batched doublet-scoring
+         workload (one persistent launch vs 64 launches, CPU knn_exact)
 
 Multi-GPU (torchrun): each rank builds the graph of its own embedding (replicas
 of the workload with different seeds); per-step time is the max over ranks.
@@ -55,8 +62,8 @@ def parse():
     ap.add_argument("--queries", type=int, default=20_000)
     ap.add_argument("--cpu-sample", type=int, default=262_144)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--form", default="bf16", choices=["plain", "bf16", "fp8"],
-                    help="the headline form (the other is measured too unless --skip-other)")
+    ap.add_argument("--form", default="bf16", choices=["plain", "plain_r99", "bf16", "fp8"],
+                    help="the headline form (the others are measured too unless --skip-other)")
     ap.add_argument("--skip-other", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="run W warm-up and K device-resident builds, print nothing else "
@@ -87,6 +94,7 @@ def config(args):
                         f"{args.comps}-component log-normal Gaussian mixture, 5% doublets",
             "n_cells": args.n, "n_pcs": args.d, "k": args.k,
             "form": {"plain": "plain (bit-exact)",
+                     "plain_r99": "plain (bit-exact) with options reaching recall@15 >= 0.99",
                      "bf16": "chosen: bf16 tensor-core shortlist + FP32 re-rank + FP64 boundary",
                      "fp8": "e4m3 tensor-core shortlist + FP32 re-rank + FP64 boundary"}[args.form],
             "l2": "inputs larger than L2 (embedding 800 MB, graph 480 MB)"}
@@ -158,9 +166,12 @@ def recall_fp64(torch, x_dev, indices, dists, k, nq, seed=7):
         xq = xd[qi]
         d2 = x2[qi][:, None] + x2[None, :] - 2.0 * (xq @ xd.T)
         d2[torch.arange(len(qi), device=d2.device), qi] = float("inf")
-        # (distance, index) order: stable sort of the k+8 best by distance
+        # (distance, index) order: the k+8 nearest, ties at equal FP64
+        # distance ordered by index, then the first k
         vals, idx = torch.topk(d2, k + 8, dim=1, largest=False, sorted=True)
-        exact = idx[:, :k].cpu().numpy()
+        vals, idx = vals.cpu().numpy(), idx.cpu().numpy()
+        order = np.lexsort((idx, vals), axis=1)
+        exact = np.take_along_axis(idx, order, axis=1)[:, :k]
         a = ind[q[s:s + 256]]
         for r in range(len(qi)):
             hits += len(set(exact[r].tolist()) & set(a[r].tolist()))
@@ -187,7 +198,8 @@ def cpu_baseline(args, x, threads=None):
     oracle.nndescent(sample, args.k, seed=0)
     dt = time.perf_counter() - t0
     return {"value": s / dt, "unit": UNIT, "cores": oracle.max_threads(), "kind": "port",
-            "sample": f"first {s} cells of the workload, one full build ({dt:.2f} s)"}
+            "sample": f"first {s} of the workload's {x.shape[0]} cells, one full build "
+                      f"({dt:.2f} s); per-cell cost grows with n, so the sample flatters the CPU"}
 
 
 def run_reference(args):
@@ -202,10 +214,15 @@ def run_reference(args):
     cb = dict(vals[-1])
     cb["value"] = v
     s = min(args.cpu_sample, args.n)
+    cfg = config(args)
+    cfg["reference_sample_cells"] = s
+    cfg["reference_sample"] = (f"each step builds the graph of the first {s} cells of the "
+                               f"{args.n}-cell workload (a full build of all cells takes "
+                               "about a minute on the host, too long for K steps)")
     line = {"metric": METRIC, "value": v, "unit": UNIT, "impl": "reference", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * s / v,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-            "data": "synthetic", "config": config(args), "cpu_baseline": cb,
+            "data": "synthetic", "config": cfg, "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -242,31 +259,50 @@ def tiles_roofline(per, st, args, peaks):
                             else "fallback")}
 
 
-def join_roofline(per, st, args, peaks):
-    """The plain form's join pass 1 against HBM: every non-empty candidate row
-    of every source row read once, the candidate ids and thresholds, and the
-    emit bits written, per launch over the launch's CUDA-event time."""
-    g = per.get("join_count")
+def seqtree_roofline(per, st, n, d, peaks):
+    """The plain form's dominant kernel group, the depth-first RP subtrees,
+    against HBM: each tree's rows read once below its parallel top levels
+    (trees x n x 4d bytes) over the group's CUDA-event time.  The kernel is
+    bound by its depth-first chain of dependent nodes, not by bandwidth, so
+    the fraction is small by nature."""
+    g = per.get("seqtree")
     if not g or g["launches_per_build"] == 0:
         return None
-    n, d = args.n, args.d
-    m = st["max_candidates"]
-    ab = n * (2 * m * 4 * d + 2 * m * 8 + (4 * m * m) // 8 + 4) * g["launches_per_build"]
-    L = g["launches_per_build"]
-    sec = g["ms_per_build"] / L / 1000.0
-    achieved = ab / L / sec / 1e9
+    ab = float(st["n_trees"]) * n * 4 * d
+    sec = g["ms_per_build"] / 1000.0
     hbm = peaks.get("hbm_gbs", 6650.0)
-    return {"bound": "hbm", "kernel": "k_join_count", "achieved": achieved, "peak": hbm,
+    achieved = ab / sec / 1e9
+    return {"bound": "hbm", "kernel": "k_seqtree", "achieved": achieved, "peak": hbm,
             "unit": "GB/s", "frac": achieved / hbm, "traffic": None,
+            "ms_per_build": g["ms_per_build"],
             "peak_source": "measured" if "hbm_gbs" in peaks else "fallback"}
 
 
-def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, world, k=None):
-    """W warm-up then K device-resident builds of one form, timed with CUDA
-    events on the launching stream (max over ranks), with per-group events."""
-    n, k = xd.shape[0], (k or args.k)
+# The reference's own NndescentOptions (nndescent.rs:42-76) under which the
+# bit-exact plain form reaches recall@15 >= 0.99 against FP64 on the 4M x 50
+# workload (a sweep of max_candidates, delta and leaf_size; the defaults give
+# 0.89): still the reference algorithm, graph for graph.
+PLAIN_R99 = {"max_candidates": 60, "delta": 0.0001, "max_iterations": 40}
+
+FORMS = {"plain": {"mode": "plain"}, "plain_r99": dict(mode="plain", **PLAIN_R99),
+         "bf16": {"mode": "bf16"}, "fp8": {"mode": "fp8"}}
+
+
+def form_opts(pq, name, k):
+    f = FORMS[name]
+    return pq._opts(k, f.get("max_iterations", 0), 0, f.get("max_candidates", 0), 0,
+                    f.get("delta", 0.001), f.get("leaf_size", 0), mode=pq.MODES[f["mode"]])
+
+
+def measure_form(torch, pq, _lib, ctx, name, xd, dev, stream, steps, warmup, barrier, world, k,
+                 queries, keep=False):
+    """`warmup` untimed then `steps` device-resident builds of one form, timed
+    with CUDA events on the launching stream (max over ranks), with
+    per-group events; recall@k against FP64 on `queries` cells and a check
+    that every row is ascending."""
+    n = xd.shape[0]
     cap = n * pq.effective_k(n, k)
-    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[form])
+    opts = form_opts(pq, name, k)
     ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
     ix = torch.empty(cap, dtype=torch.int32, device=dev)
     dx = torch.empty(cap, dtype=torch.float32, device=dev)
@@ -274,7 +310,7 @@ def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, wor
     def step():
         return ctx.nndescent_device(xd, opts, ip, ix, dx, stream=stream.cuda_stream)
 
-    for _ in range(max(3, args.warmup)):
+    for _ in range(max(3, warmup)):
         step()
     torch.cuda.synchronize(dev)
     _lib.load().pq_ctx_set_profiling(ctx._h, 1)
@@ -287,7 +323,7 @@ def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, wor
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    for _ in range(args.steps):
+    for _ in range(steps):
         nnz = step()
         stats.append(ctx.stats())
         s = _lib.NndStats()
@@ -299,17 +335,139 @@ def measure_form(torch, pq, _lib, ctx, form, xd, dev, stream, args, barrier, wor
     torch.cuda.synchronize(dev)
     barrier()
     _lib.load().pq_ctx_set_profiling(ctx._h, 0)
-    ms = max_over_ranks(torch, e0.elapsed_time(e1) / args.steps, dev, world)
+    ms = max_over_ranks(torch, e0.elapsed_time(e1) / steps, dev, world)
     names = _lib.KERNEL_GROUPS
-    per = {names[g]: {"ms_per_build": float(kg_ms[g] / args.steps),
-                      "launches_per_build": int(kg_l[g] // args.steps)}
+    per = {names[g]: {"ms_per_build": float(kg_ms[g] / steps),
+                      "launches_per_build": int(kg_l[g] // steps)}
            for g in range(len(names)) if kg_l[g] > 0}
-    rec, max_rel = recall_fp64(torch, xd, ix[:nnz].cpu().numpy().view(np.uint32),
-                               dx[:nnz].cpu().numpy(), k, args.queries)
+    kk = pq.effective_k(n, k)
+    full = nnz == n * kk
+    d2 = dx[:nnz].view(n, kk) if full else None
+    ascending = bool((d2[:, 1:] >= d2[:, :-1]).all()) if full else None
+    if full:
+        rec, max_rel = recall_fp64(torch, xd, ix[:nnz].cpu().numpy().view(np.uint32),
+                                   dx[:nnz].cpu().numpy(), kk, queries)
+    else:
+        rec, max_rel = None, None
     st = stats[-1]
-    return {"ms": ms, "value": world * n / (ms / 1000.0), "launches": launches // args.steps,
-            "launches_timed": int(launches), "groups": per, "stats": st,
-            "recall_at_k": rec, "max_rel_dist_err": max_rel, "rounds_run": st["rounds_run"]}
+    out = {"ms": ms, "value": world * n / (ms / 1000.0), "launches": launches // steps,
+           "launches_timed": int(launches), "groups": per, "stats": st, "steps": steps,
+           "recall_at_k": rec, "max_rel_dist_err": max_rel, "rounds_run": st["rounds_run"],
+           "rows_ascending": ascending}
+    if keep:
+        out["graph"] = {"indptr": ip.cpu().numpy().view(np.uint32),
+                        "indices": ix[:nnz].cpu().numpy().view(np.uint32),
+                        "data": dx[:nnz].cpu().numpy()}
+    return out
+
+
+def summary(f):
+    st = f["stats"]
+    return {"cells_per_s": f["value"], "ms_per_build": f["ms"], "steps": f["steps"],
+            "recall_at_k": f["recall_at_k"], "max_rel_dist_err": f["max_rel_dist_err"],
+            "rows_ascending": f["rows_ascending"], "rounds_run": f["rounds_run"],
+            "launches_per_build": f["launches"],
+            "phases_ms": {"init": st["ms_forest"], "layout_or_leaves": st["ms_leaves"],
+                          "search_or_rounds": st["ms_rounds"], "finish": st["ms_extract"]},
+            "kernel_groups": f["groups"]}
+
+
+def plain_bit_exact(x, k, graph):
+    """The oracle's graph of the same workload (reference defaults, seed 0),
+    timed on all host threads, compared byte for byte with the plain form's."""
+    import oracle
+
+    oracle.lib()
+    t0 = time.perf_counter()
+    r = oracle.nndescent(x, k, seed=0)
+    dt = time.perf_counter() - t0
+    same = (np.array_equal(r["indptr"], graph["indptr"])
+            and np.array_equal(r["indices"], graph["indices"])
+            and r["data"].tobytes() == graph["data"].tobytes())
+    return same, dt
+
+
+def bench_batched(torch, pq, ctx, dev, args, steps, warmup):
+    """The doublet-scoring workload: 64 samples, cell counts log-uniform in
+    [2,000, 60,000] plus 2x simulated doublets (30 PCs), k = round(0.5 sqrt(n))
+    per sample, exact kNN of every point within its sample.  One persistent,
+    work-queued, graph-captured launch for all samples against 64 launches of
+    one sample each; recall against FP64 on sampled points of the largest
+    sample; the reference's tiled knn_exact restated in C++ (all host
+    threads) on a bounded subset of the samples."""
+    from polariseq_b200 import synth
+
+    samples = synth.doublet_samples(64, 2000, 60000, seed=0, device=f"cuda:{dev.index}")
+    cells = [len(a) // 3 for a in samples]
+    ks = np.array([max(1, int(round(0.5 * np.sqrt(c)))) for c in cells], np.uint32)
+    sizes = np.array([len(a) for a in samples], np.uint64)
+    offs = np.concatenate([[0], np.cumsum(sizes)]).astype(np.uint64)
+    pts = int(sizes.sum())
+    total = int(np.sum(sizes * ks.astype(np.uint64)))
+    x = torch.from_numpy(np.concatenate(samples)).to(dev)
+    oi = torch.empty(total, dtype=torch.int32, device=dev)
+    od = torch.empty(total, dtype=torch.float32, device=dev)
+    stream = torch.cuda.current_stream(dev)
+    shape = ctx.knn_batched_device(x, offs, ks, oi, od, autotune=True, graph=True,
+                                   stream=stream.cuda_stream)
+    for _ in range(max(3, warmup)):
+        ctx.knn_batched_device(x, offs, ks, oi, od, graph=True, stream=stream.cuda_stream)
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        ctx.knn_batched_device(x, offs, ks, oi, od, graph=True, stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    one = e0.elapsed_time(e1) / steps
+    # 64 separate launches, one sample each (the same kernel)
+    out_off = np.concatenate([[0], np.cumsum(sizes * ks.astype(np.uint64))]).astype(np.int64)
+    e0.record(stream)
+    for s in range(len(samples)):
+        a, b = int(offs[s]), int(offs[s + 1])
+        o0, o1 = int(out_off[s]), int(out_off[s + 1])
+        ctx.knn_batched_device(x[a:b], np.array([0, b - a], np.uint64), ks[s:s + 1],
+                               oi[o0:o1], od[o0:o1], graph=False, stream=stream.cuda_stream)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    sep = e0.elapsed_time(e1)
+    # recall of the largest sample against FP64
+    big = int(np.argmax(sizes))
+    a, b = int(offs[big]), int(offs[big + 1])
+    o0, o1 = int(out_off[big]), int(out_off[big + 1])
+    kb = int(ks[big])
+    rec, max_rel = recall_fp64(torch, x[a:b], oi[o0:o1].cpu().numpy().view(np.uint32),
+                               od[o0:o1].cpu().numpy(), kb, 2000)
+    pairs = float(np.sum(sizes.astype(np.float64) ** 2))
+    out = {"workload": "64 samples, cells log-uniform in [2000, 60000] + 2x simulated doublets, "
+                       "30 PCs, k = round(0.5 sqrt(cells)) per sample",
+           "points": pts, "samples": len(samples), "k_range": [int(ks.min()), int(ks.max())],
+           "tile_shape": shape, "steps": steps,
+           "one_launch_ms": one, "points_per_s": pts / (one / 1000.0),
+           "separate_launches_ms": sep, "distance_pairs": pairs,
+           "pair_rate_tflops_fp32": 2.0 * pairs * 30 / (one / 1000.0) / 1e12,
+           "recall_at_k_largest_sample": rec, "max_rel_dist_err": max_rel}
+    if not args.no_cpu:
+        import oracle
+
+        oracle.lib()
+        # a bounded subset: the samples in order until ~5e10 point pairs
+        sub, acc = [], 0.0
+        for s in range(len(samples)):
+            if sub and acc + float(sizes[s]) ** 2 > 5e10:
+                break
+            sub.append(s)
+            acc += float(sizes[s]) ** 2
+        t0 = time.perf_counter()
+        oracle.knn_exact_batched([samples[s] for s in sub], [int(ks[s]) for s in sub])
+        dt = time.perf_counter() - t0
+        sp = int(sum(int(sizes[s]) for s in sub))
+        out["cpu_baseline"] = {"value": sp / dt, "unit": "points/s",
+                               "cores": oracle.max_threads(), "kind": "port",
+                               "sample": f"the first {len(sub)} samples ({sp} points), one "
+                                         f"call ({dt:.2f} s)"}
+    return out
 
 
 def main():
@@ -331,7 +489,7 @@ def main():
     dev = torch.device("cuda", local)
 
     import polariseq_b200 as pq
-    from polariseq_b200 import _lib
+    from polariseq_b200 import _lib, synth
 
     x = workload(args, rank)
     n, d, k = x.shape[0], x.shape[1], args.k
@@ -345,7 +503,7 @@ def main():
             dist.barrier()
 
     if args.profile_only:
-        opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES[args.form])
+        opts = form_opts(pq, args.form, k)
         ip = torch.empty(n + 1, dtype=torch.int32, device=dev)
         ix = torch.empty(cap, dtype=torch.int32, device=dev)
         dx = torch.empty(cap, dtype=torch.float32, device=dev)
@@ -363,23 +521,30 @@ def main():
         peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
     except OSError:
         pass
+    # secondary forms and configurations: fewer timed builds, one GPU only
+    sec = min(args.steps, 5)
+    others = world == 1 and not args.skip_other
 
     # ── device-resident timed region of the headline form (clocks sampled) ──
     clocks = Clocks(local)
     clocks.start()
-    head = measure_form(torch, pq, _lib, ctx, args.form, xd, dev, stream, args, barrier, world)
+    head = measure_form(torch, pq, _lib, ctx, args.form, xd, dev, stream, args.steps,
+                        args.warmup, barrier, world, k, args.queries)
     ck = clocks.stop()
     forms = {args.form: head}
     forms_k30 = {}
-    if not args.skip_other:
-        for other in ("plain", "bf16", "fp8"):
+    if others:
+        for other in ("plain", "plain_r99", "bf16", "fp8"):
             if other != args.form:
-                forms[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, args,
-                                            barrier, world)
-        # k = 30 (the E4M3 form supports k <= 15)
-        for other in ("bf16", "plain"):
-            forms_k30[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, args,
-                                            barrier, world, k=30)
+                forms[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, sec, 3,
+                                            barrier, world, k, args.queries,
+                                            keep=other == "plain")
+        for other in ("bf16", "fp8", "plain"):
+            try:
+                forms_k30[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream,
+                                                sec, 3, barrier, world, 30, args.queries)
+            except NotImplementedError as e:
+                forms_k30[other] = {"unsupported": str(e)}
 
     # ── end to end through the public API with pinned host buffers ──
     hx = torch.from_numpy(x).pin_memory()
@@ -391,39 +556,56 @@ def main():
     r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
     barrier()
     t0 = time.perf_counter()
-    e2e_steps = max(1, min(args.steps, 3))
-    for _ in range(e2e_steps):
+    for _ in range(args.steps):
         r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
-    e2e_ms = max_over_ranks(torch, (time.perf_counter() - t0) * 1000.0 / e2e_steps, dev, world)
+    e2e_ms = max_over_ranks(torch, (time.perf_counter() - t0) * 1000.0 / args.steps, dev, world)
     e2e = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(x.nbytes),
-           "d2h_bytes_per_step": int(4 * (n + 1) + 8 * r["nnz"]), "steps": e2e_steps}
+           "d2h_bytes_per_step": int(4 * (n + 1) + 8 * r["nnz"]), "steps": args.steps}
 
     roof = (tiles_roofline(head["groups"], head["stats"], args, peaks) if args.form != "plain"
-            else join_roofline(head["groups"], head["stats"], args, peaks))
+            else seqtree_roofline(head["groups"], head["stats"], n, d, peaks))
 
+    # ── the CPU baseline: the oracle on the whole workload (which also checks
+    #    the plain form's graph byte for byte), else on a bounded sample ──
     cpu = None
+    bit_exact = None
     if rank == 0 and not args.no_cpu:
         try:
-            cpu = cpu_baseline(args, x)
+            if "plain" in forms and "graph" in forms["plain"]:
+                bit_exact, dt = plain_bit_exact(x, k, forms["plain"].pop("graph"))
+                import oracle
+
+                cpu = {"value": n / dt, "unit": UNIT, "cores": oracle.max_threads(),
+                       "kind": "port", "sample": f"the whole workload ({n} cells), one build "
+                                                 f"({dt:.1f} s), also the bit-exact check"}
+            else:
+                cpu = cpu_baseline(args, x)
         except Exception as e:  # pragma: no cover
             cpu = {"error": str(e)}
 
-    def summary(f):
-        st = f["stats"]
-        out = {"cells_per_s": f["value"], "ms_per_build": f["ms"],
-               "recall_at_k": f["recall_at_k"], "max_rel_dist_err": f["max_rel_dist_err"],
-               "rounds_run": f["rounds_run"], "launches_per_build": f["launches"],
-               "phases_ms": {"init": st["ms_forest"], "layout_or_leaves": st["ms_leaves"],
-                             "search_or_rounds": st["ms_rounds"], "finish": st["ms_extract"]},
-               "kernel_groups": f["groups"]}
-        return out
+    # ── the other configurations ──
+    configs = {}
+    if others:
+        del xd
+        x2 = synth.mixture_lognormal(1_300_000, d, 40, seed=2000)
+        xd2 = torch.from_numpy(x2).to(dev)
+        c2 = {}
+        for f in ("plain", "plain_r99", "bf16"):
+            c2[f] = summary(measure_form(torch, pq, _lib, ctx, f, xd2, dev, stream, sec, 3,
+                                         barrier, world, k, args.queries))
+        configs["c2_1.3M"] = {"workload": "1,300,000 cells x 50 PCs f32, k=15, 40-component "
+                                          "log-normal Gaussian mixture, 5% doublets",
+                              "forms": c2}
+        del xd2
+        configs["c4_batched"] = bench_batched(torch, pq, ctx, dev, args, sec, 3)
 
     forms_out = {f: summary(v) for f, v in forms.items()}
-    forms_k30_out = {f: summary(v) for f, v in forms_k30.items()}
+    forms_k30_out = {f: (summary(v) if "stats" in v else v) for f, v in forms_k30.items()}
     if "plain" in forms:
-        forms_out["plain"]["roofline"] = join_roofline(forms["plain"]["groups"],
-                                                       forms["plain"]["stats"], args, peaks)
+        forms_out["plain"]["roofline"] = seqtree_roofline(forms["plain"]["groups"],
+                                                          forms["plain"]["stats"], n, d, peaks)
+        forms_out["plain"]["bit_exact_vs_oracle"] = bit_exact
     line = {"metric": METRIC, "value": head["value"], "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": max(3, args.warmup), "ms_per_step": head["ms"],
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -432,8 +614,10 @@ def main():
             "roofline": roof, "cpu_baseline": cpu, "clocks": ck,
             "quality": {"recall_at_k": head["recall_at_k"],
                         "max_rel_dist_err": head["max_rel_dist_err"],
+                        "rows_ascending": head["rows_ascending"],
                         "queries": min(args.queries, n), "oracle": "FP64 brute force"},
-            "forms": forms_out, "forms_k30": forms_k30_out}
+            "plain_bit_exact": bit_exact, "plain_r99_options": PLAIN_R99,
+            "forms": forms_out, "forms_k30": forms_k30_out, "configs": configs}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -44,8 +44,20 @@ enum { PQ_METRIC_EUCLIDEAN = 0, PQ_METRIC_COSINE = 1 };
  * and per-bucket candidate power-of-two scales, k <= 15). */
 enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
 /* Initial neighbour lists: the reference's RP-tree forest, or learned buckets
- * (tensor-core forms, n_obs >= 65,536: an MLP trained on a subsample's plain
- * graph routes each cell to the buckets its neighbours live in). */
+ * (n_obs >= 65,536, n_dim <= 62, k <= 31): an MLP trained on a subsample's
+ * plain graph routes each cell to the buckets its neighbours live in.
+ *   - with PQ_MODE_BF16 / PQ_MODE_FP8 the router chooses the buckets each
+ *     cell's shortlist searches;
+ *   - with PQ_MODE_PLAIN it is the learned-init NN-Descent: each cell's
+ *     initial list is its k nearest within its `probes` (default 4) most
+ *     likely buckets (BF16 tensor-core tiles, exact FP32 re-rank), in place
+ *     of the RP forest + random fill (nndescent.rs:768-845); the reference's
+ *     rounds (max_iterations, delta, max_candidates) then run to
+ *     convergence.  Its recall is estimated on 1,024 sampled cells against
+ *     their exact FP32 neighbours; below 0.99 the RP-initialised build runs
+ *     too (the fallback) and the graph with the higher estimate is kept
+ *     (pq_nnd_stats.fell_back / est_recall*).  Not bit-exact with the
+ *     RP-initialised graph. */
 enum { PQ_INIT_RP = 0, PQ_INIT_LEARNED = 1 };
 
 /* Mirrors NndescentOptions (nndescent.rs:42-76): zero = auto for the sized
@@ -92,6 +104,13 @@ typedef struct pq_nnd_stats {
      * (the untrained router is the nearest-centroid prior), and the time of
      * the subsample graph + training, and of routing every cell, in ms. */
     double learn_loss_first, learn_loss_last, ms_learn_train, ms_learn_route;
+    /* Learned-init NN-Descent (PQ_MODE_PLAIN + PQ_INIT_LEARNED): recall@k
+     * estimated on sampled cells for the returned graph, for the learned-init
+     * graph and for the RP-initialised fallback (0 when it did not run);
+     * fell_back = 1 when the fallback ran, 2 when its graph was kept. */
+    double est_recall, est_recall_learned, est_recall_rp;
+    int32_t fell_back;
+    int32_t learned_rounds;  /* rounds the learned-init build ran */
 } pq_nnd_stats;
 
 /* Kernel groups timed by the profiling mode. */

@@ -125,7 +125,9 @@ class Context:
             "ms_rounds": s.ms_rounds, "ms_extract": s.ms_extract, "ms_total": s.ms_total,
             "shortlist": list(s.shortlist), "learn_loss_first": s.learn_loss_first,
             "learn_loss_last": s.learn_loss_last, "ms_learn_train": s.ms_learn_train,
-            "ms_learn_route": s.ms_learn_route,
+            "ms_learn_route": s.ms_learn_route, "est_recall": s.est_recall,
+            "est_recall_learned": s.est_recall_learned, "est_recall_rp": s.est_recall_rp,
+            "fell_back": s.fell_back, "learned_rounds": s.learned_rounds,
         }
 
     # -- host-buffer build (the drop-in) ------------------------------------

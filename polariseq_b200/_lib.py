@@ -74,6 +74,11 @@ class NndStats(C.Structure):
         ("learn_loss_last", C.c_double),
         ("ms_learn_train", C.c_double),
         ("ms_learn_route", C.c_double),
+        ("est_recall", C.c_double),
+        ("est_recall_learned", C.c_double),
+        ("est_recall_rp", C.c_double),
+        ("fell_back", C.c_int32),
+        ("learned_rounds", C.c_int32),
     ]
 
 

@@ -582,6 +582,67 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
     return nnz;
 }
 
+// Learned-init NN-Descent: the initial lists from the learned buckets, the
+// reference's rounds to convergence (build_chosen with PQ_MODE_PLAIN), then
+// the recall estimate on sampled cells; below the target the RP-initialised
+// build runs too and the graph with the higher estimate is kept.
+// POLARISEQ_LEARNED_MIN_RECALL overrides the 0.99 target (tests force the
+// fallback with a target above 1).
+uint64_t build_learned_nnd(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64,
+                           uint64_t d64, const pq_nnd_opts& o, uint32_t* d_indptr,
+                           uint32_t* d_indices, float* d_dists) {
+    cudaStream_t st = c->stream;
+    const uint32_t n = uint32_t(n64);
+    const int d = int(d64), dp = int((d64 + 3) / 4 * 4);
+    const int k = int(effective_k(n64, o.k));
+    double target = 0.99;
+    if (const char* e = std::getenv("POLARISEQ_LEARNED_MIN_RECALL")) target = std::atof(e);
+    const uint32_t Q = 1024;
+    uint64_t nnz = build_chosen(c, data, data_on_host, n64, d64, o, d_indptr, d_indices, d_dists);
+    const float* X = c->get<float>("X", size_t(n) * dp);  // the padded rows of this build
+    const double rl = pq::sampled_recall(c, X, d, dp, n, k, d_indptr, d_indices, Q, o.seed);
+    pq_nnd_stats learned = c->stats;
+    learned.est_recall = learned.est_recall_learned = rl;
+    learned.learned_rounds = learned.rounds_run;
+    if (rl >= target) {
+        c->stats = learned;
+        return nnz;
+    }
+    // the fallback: keep the learned graph aside, build with the RP forest
+    uint32_t* sip = c->get<uint32_t>("lf_ip", n64 + 1);
+    uint32_t* six = c->get<uint32_t>("lf_ix", std::max<uint64_t>(nnz, 1));
+    float* sdx = c->get<float>("lf_dx", std::max<uint64_t>(nnz, 1));
+    ck(cudaMemcpyAsync(sip, d_indptr, (n64 + 1) * 4, cudaMemcpyDeviceToDevice, st), "keep");
+    ck(cudaMemcpyAsync(six, d_indices, nnz * 4, cudaMemcpyDeviceToDevice, st), "keep");
+    ck(cudaMemcpyAsync(sdx, d_dists, nnz * 4, cudaMemcpyDeviceToDevice, st), "keep");
+    pq_nnd_opts po = o;
+    po.init = PQ_INIT_RP;
+    const uint64_t nnz_rp =
+        build_plain(c, data, data_on_host, n64, d64, po, d_indptr, d_indices, d_dists, nullptr);
+    const float* X2 = c->get<float>("X", size_t(n) * dp);
+    const double rr = pq::sampled_recall(c, X2, d, dp, n, k, d_indptr, d_indices, Q, o.seed);
+    pq_nnd_stats& S = c->stats;  // the RP build's statistics
+    const double ms_rp = S.ms_total;
+    if (rr >= rl) {
+        S.est_recall = rr;
+        S.fell_back = 2;
+        nnz = nnz_rp;
+    } else {
+        ck(cudaMemcpyAsync(d_indptr, sip, (n64 + 1) * 4, cudaMemcpyDeviceToDevice, st), "back");
+        ck(cudaMemcpyAsync(d_indices, six, nnz * 4, cudaMemcpyDeviceToDevice, st), "back");
+        ck(cudaMemcpyAsync(d_dists, sdx, nnz * 4, cudaMemcpyDeviceToDevice, st), "back");
+        ck(cudaStreamSynchronize(st), "back");
+        S = learned;
+        S.est_recall = rl;
+        S.fell_back = 1;
+        S.ms_total += ms_rp;
+    }
+    S.est_recall_learned = rl;
+    S.est_recall_rp = rr;
+    S.learned_rounds = learned.rounds_run;
+    return nnz;
+}
+
 int fail(pq_ctx* c, int code, const std::string& msg) {
     if (c) c->err = msg;
     return code;
@@ -610,13 +671,12 @@ int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
         return fail(c, PQ_ENOTSUP, "the E4M3 form supports k <= 15");
     if (o->init != PQ_INIT_RP && o->init != PQ_INIT_LEARNED)
         return fail(c, PQ_ENOTSUP, "init not available in this build");
-    if (o->init == PQ_INIT_LEARNED && (o->mode == PQ_MODE_PLAIN || n < 65536))
-        return fail(c, PQ_ENOTSUP,
-                    "learned probes need a tensor-core form and at least 65,536 cells");
-    if (o->mode != PQ_MODE_PLAIN && d > 62)
-        return fail(c, PQ_ENOTSUP, "the tensor-core form supports n_dim <= 62");
-    if (o->mode != PQ_MODE_PLAIN && R.k > 31)
-        return fail(c, PQ_ENOTSUP, "the tensor-core form supports k <= 31");
+    if (o->init == PQ_INIT_LEARNED && n < 65536)
+        return fail(c, PQ_ENOTSUP, "learned buckets need at least 65,536 cells");
+    const bool tiles = o->mode != PQ_MODE_PLAIN || o->init == PQ_INIT_LEARNED;
+    if (tiles && d > 62)
+        return fail(c, PQ_ENOTSUP, "the tensor-core tiles support n_dim <= 62");
+    if (tiles && R.k > 31) return fail(c, PQ_ENOTSUP, "the tensor-core tiles support k <= 31");
     return PQ_OK;
 }
 
@@ -764,9 +824,11 @@ int pq_nndescent_into(pq_ctx* c, const float* data, uint64_t n, uint64_t d,
         uint32_t* dix = c->get<uint32_t>("out_indices", cap);
         float* ddx = c->get<float>("out_dists", cap);
         HostGraph hg{indptr, indices, dists, false};
-        uint64_t nnz = o->mode == PQ_MODE_PLAIN
-                           ? build_plain(c, data, true, n, d, *o, dip, dix, ddx, nullptr)
-                           : build_chosen(c, data, true, n, d, *o, dip, dix, ddx, &hg);
+        uint64_t nnz = o->mode != PQ_MODE_PLAIN
+                           ? build_chosen(c, data, true, n, d, *o, dip, dix, ddx, &hg)
+                       : o->init == PQ_INIT_LEARNED
+                           ? build_learned_nnd(c, data, true, n, d, *o, dip, dix, ddx)
+                           : build_plain(c, data, true, n, d, *o, dip, dix, ddx, nullptr);
         if (!hg.copied) {
             ck(cudaMemcpyAsync(indptr, dip, (n + 1) * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
             ck(cudaMemcpyAsync(indices, dix, nnz * 4, cudaMemcpyDeviceToHost, c->stream), "d2h");
@@ -792,9 +854,11 @@ int pq_nndescent_into_device(pq_ctx* c, const float* d_data, uint64_t n, uint64_
         ck(cudaEventRecord(ev, user), "event");
         ck(cudaStreamWaitEvent(c->stream, ev, 0), "event");
         uint64_t nnz =
-            o->mode == PQ_MODE_PLAIN
-                ? build_plain(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists, nullptr)
-                : build_chosen(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists);
+            o->mode != PQ_MODE_PLAIN
+                ? build_chosen(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists)
+            : o->init == PQ_INIT_LEARNED
+                ? build_learned_nnd(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists)
+                : build_plain(c, d_data, false, n, d, *o, d_indptr, d_indices, d_dists, nullptr);
         ck(cudaEventRecord(ev, c->stream), "event");
         ck(cudaStreamWaitEvent(user, ev, 0), "event");
         cudaEventDestroy(ev);
@@ -1073,7 +1137,11 @@ int pq_mlp_grad(pq_ctx* c, uint64_t d, const float* params, const float* X, uint
     return guarded(c, [&]() -> int {
         cudaStream_t st = c->stream;
         const size_t np = pq::mlp_params(int(d));
-        pq::MlpView net{int(d), c->get<float>("mg_w", np), c->get<__nv_bfloat16>("mg_wb", np)};
+        ck(cudaMemsetAsync(c->d_err, 0, sizeof(int), st), "err");
+        pq::MlpView net{int(d), c->get<float>("mg_w", np),
+                        c->get<__nv_bfloat16>("mg_wt", pq::mlp_wt_elems()), c->d_err};
+        const pq::MlpBufs b16 = pq::mlp_bufs(
+            c->get<uint8_t>("mg_b16", pq::mlp_bufs_bytes(int(rows), true)), int(rows), true);
         float* dx = c->get<float>("mg_x", rows * d);
         uint32_t* dtb = c->get<uint32_t>("mg_tb", rows * T);
         float* dtw = c->get<float>("mg_tw", rows * T);
@@ -1090,16 +1158,19 @@ int pq_mlp_grad(pq_ctx* c, uint64_t d, const float* params, const float* X, uint
         ck(cudaMemcpyAsync(dtb, tb, rows * T * 4, cudaMemcpyHostToDevice, st), "h2d");
         ck(cudaMemcpyAsync(dtw, tw, rows * T * 4, cudaMemcpyHostToDevice, st), "h2d");
         pq::mlp_sync_bf16(net, st);
-        pq::mlp_forward(net, dx, int(rows), h1, h2, z, st);
+        ck(pq::mlp_forward(net, dx, int(rows), h1, h2, z, b16, true, st), "mlp forward");
         if (logits_out)
             ck(cudaMemcpyAsync(logits_out, z, rows * pq::MLP_OUT * 4, cudaMemcpyDeviceToHost, st),
                "d2h");
-        pq::mlp_backward(net, dx, int(rows), h1, h2, z, dtb, dtw, int(T), loss, dh1, dh2, g,
-                         scratch, st);
-        ck(cudaGetLastError(), "mlp");
+        ck(pq::mlp_backward(net, int(rows), h1, h2, z, b16, dtb, dtw, int(T), loss, dh1, dh2, g,
+                            scratch, st),
+           "mlp backward");
         ck(cudaMemcpyAsync(grad_out, g, np * 4, cudaMemcpyDeviceToHost, st), "d2h");
         ck(cudaMemcpyAsync(loss_out, loss, rows * 4, cudaMemcpyDeviceToHost, st), "d2h");
+        int herr = 0;
+        ck(cudaMemcpyAsync(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost, st), "err");
         ck(cudaStreamSynchronize(st), "mlp");
+        if (herr) throw DeviceError{"mlp tensor-core products: a bounded wait gave up", herr == 2};
         return PQ_OK;
     });
 }

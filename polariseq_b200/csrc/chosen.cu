@@ -918,11 +918,15 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     std::optional<KGScope> kg_sec;
     kg_sec.emplace(c, PQ_KG_BUCKETS);
     const bool learned = o.init == PQ_INIT_LEARNED;
+    // PQ_MODE_PLAIN here is the learned-init NN-Descent: BF16 tiles over the
+    // router's top buckets give the initial lists, the rounds run to
+    // convergence
+    const bool nnd = o.mode == PQ_MODE_PLAIN;
     // learned probes: the MLP's 1024 buckets; else about 4096 cells per bucket
     const uint32_t C = learned ? 1024u
                        : o.buckets > 0 ? std::min<uint32_t>(uint32_t(o.buckets), n)
                                        : std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
-    const uint32_t P_auto = learned ? 6u : 14u;
+    const uint32_t P_auto = nnd ? 4u : learned ? 6u : 14u;
     const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : P_auto, std::min(C, 16u)));
     const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
     if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};
@@ -1359,7 +1363,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
     ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
     // auto: no polish round for BF16; one for E4M3, whose shortlist misses more
-    const uint64_t polish = o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : (fp8 ? 1 : 0);
+    const uint64_t polish = nnd ? resolve(n64, o).n_iters
+                            : o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : (fp8 ? 1 : 0);
     auto rerank = [&](const uint32_t* by_cell, uint32_t a, uint32_t b) {
         if (d == 50)
             k_rerank<50><<<blocks(b - a, 4), 128, 0, st>>>(X, xp, d, dp, b, k, P, Sout, Ssh, R,

@@ -205,6 +205,18 @@ struct HostGraph {
     bool copied;
 };
 
+}  // namespace pqh
+
+namespace pq {
+// recall@k of the graph (device CSR) on Q seeded sampled cells against their
+// exact FP32 k nearest (recall.cu).
+double sampled_recall(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k,
+                      const uint32_t* d_indptr, const uint32_t* d_indices, uint32_t Q,
+                      uint64_t seed);
+}  // namespace pq
+
+namespace pqh {
+
 // The chosen form (tensor-core shortlist), chosen.cu.
 uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t n64,
                       uint64_t d64, const pq_nnd_opts& o, uint32_t* d_indptr,

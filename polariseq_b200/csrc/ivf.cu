@@ -570,6 +570,20 @@ bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t b
     return r == CUDA_SUCCESS;
 }
 
+bool make_bf16_map_ld(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
+                      uint64_t ld, uint32_t box_rows) {
+    EncodeTiledFn fn = encode_fn();
+    if (!fn || (ld * 2) % 16 != 0 || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+    cuuint64_t dims[2] = {cols, rows};
+    cuuint64_t strides[1] = {ld * 2};
+    cuuint32_t box[2] = {64, box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims,
+                    strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                    CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS;
+}
+
 bool make_fp8_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows) {
     EncodeTiledFn fn = encode_fn();
     if (!fn) return false;

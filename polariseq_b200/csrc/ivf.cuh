@@ -57,6 +57,11 @@ enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT
        IVF_T_SLOW_CYC = 12, IVF_TRACE_N = 16 };
 
 bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
+// A [rows x cols] BF16 matrix with leading dimension ld (elements, a multiple
+// of 8; base 16-byte aligned) as 128-byte-swizzled boxes of box_rows x 64;
+// reads beyond rows or cols fill zeros.
+bool make_bf16_map_ld(CUtensorMap* map, const void* base, uint64_t rows, uint64_t cols,
+                      uint64_t ld, uint32_t box_rows);
 // A [rows x 128] one-byte (E4M3) matrix as 128-byte-swizzled boxes of box_rows x 128.
 bool make_fp8_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
 // Runs of one entry's output row.

@@ -207,7 +207,9 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     k_targets<<<blocks(ns, 256), 256, 0, st>>>(gip, gix, ns, n, primary, tb, tw); count_launch();
     // ── 3. training ──
     const size_t np = mlp_params(d);
-    MlpView net{d, c->get<float>("ml_w", np), c->get<__nv_bfloat16>("ml_wb", np)};
+    ck(cudaMemsetAsync(c->d_err, 0, sizeof(int), st), "err");
+    MlpView net{d, c->get<float>("ml_w", np), c->get<__nv_bfloat16>("ml_wt", mlp_wt_elems()),
+                c->d_err};
     float* am = c->get<float>("ml_m", np);
     float* av = c->get<float>("ml_v", np);
     float* grad = c->get<float>("ml_g", np);
@@ -226,6 +228,7 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     float* dh2 = c->get<float>("ml_dh2", size_t(B) * MLP_H);
     float* loss = c->get<float>("ml_loss", B);
     float* scratch = c->get<float>("ml_scratch", mlp_scratch_floats());
+    const MlpBufs tb16 = mlp_bufs(c->get<uint8_t>("ml_b16", mlp_bufs_bytes(B, true)), B, true);
     uint32_t* dperm = c->get<uint32_t>("ml_perm", ns);
     std::vector<uint32_t> perm(ns);
     std::iota(perm.begin(), perm.end(), 0u);
@@ -242,9 +245,10 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
             k_gather_batch<<<blocks(size_t(rows) * std::max(d, T_MAX), 256), 256, 0, st>>>(
                 xs, d, dperm + b0, rows, tb, tw, xb, bb, bw);
             count_launch();
-            mlp_forward(net, xb, int(rows), h1, h2, z, st, &prior);
-            mlp_backward(net, xb, int(rows), h1, h2, z, bb, bw, T_MAX, loss, dh1, dh2, grad,
-                         scratch, st);
+            ck(mlp_forward(net, xb, int(rows), h1, h2, z, tb16, true, st, &prior), "mlp forward");
+            ck(mlp_backward(net, int(rows), h1, h2, z, tb16, bb, bw, T_MAX, loss, dh1, dh2, grad,
+                            scratch, st),
+               "mlp backward");
             mlp_adam(net, am, av, grad, ++step, 1e-3f, st);
             k_sum_f32<<<8, 256, 0, st>>>(loss, rows, eloss + ep); count_launch();
             erows[ep] += rows;
@@ -266,16 +270,20 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     float* ih2 = c->get<float>("ml_ih2", size_t(R) * MLP_H);
     float* iz = c->get<float>("ml_iz", size_t(R) * MLP_OUT);
     uint32_t* top = c->get<uint32_t>("ml_top", size_t(R) * std::max(P - 1, 1));
+    const MlpBufs ib16 = mlp_bufs(c->get<uint8_t>("ml_i16", mlp_bufs_bytes(R, false)), R, false);
     for (uint64_t r0 = 0; r0 < n; r0 += R) {
         const uint32_t rows = uint32_t(std::min<uint64_t>(R, n - r0));
         k_rows_of<<<blocks(size_t(rows) * d, 256), 256, 0, st>>>(X, d, dp, r0, rows, xr); count_launch();
-        mlp_forward(net, xr, int(rows), ih1, ih2, iz, st, &prior);
+        ck(mlp_forward(net, xr, int(rows), ih1, ih2, iz, ib16, false, st, &prior), "mlp routing");
         if (P > 1) mlp_topp(iz, int(rows), P - 1, primary + r0, top, st);
         k_assemble_probes<<<blocks(size_t(rows) * P, 256), 256, 0, st>>>(primary, top, r0, rows, P,
                                                                         probes);
         count_launch();
     }
     ck(cudaStreamSynchronize(st), "learned probes");
+    int herr = 0;
+    ck(cudaMemcpy(&herr, c->d_err, sizeof(int), cudaMemcpyDeviceToHost), "err");
+    if (herr) throw DeviceError{"mlp tensor-core products: a bounded wait gave up", herr == 2};
     return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t1).count();
 }
 

@@ -1,20 +1,25 @@
 // Learned bucket routing: a small MLP d -> 256 -> 256 -> 1024 (ReLU) maps a
 // cell's embedding to logits over the 1024 k-means buckets; trained so that
 // a cell puts its probability where its neighbours (in a plain NN-Descent
-// graph of a subsample) live.  Its top buckets replace the nearest-centroid
-// probes of the tensor-core form.
+// graph of a subsample) live.
 //
-// Hand-written kernels, no library calls: a tiled GEMM (64 x 64 output tile
-// per 256-thread block, 4 x 4 per thread, 16-deep K steps through shared
-// memory) with BF16 weights and FP32 activations / accumulation, used for the
-// forward pass and both backward products; a softmax cross-entropy against
-// sparse soft targets; column sums for the bias gradients; ReLU masks; Adam
-// on FP32 master weights that refreshes the BF16 copies; and a per-row top-P
-// of the logits.
+// Hand-written kernels, no library calls.  Every product of the forward and
+// backward pass runs on the tcgen05 tensor cores: one 128 x 256 output tile
+// per CTA, BF16 operands staged K-major in shared memory by TMA (128-byte
+// swizzle, four stages), FP32 accumulation in TMEM, and an epilogue that adds
+// the bias, applies ReLU or the ReLU-backward mask and writes FP32 and BF16
+// (row-major and transposed) copies, so that each product's output is the
+// next one's operand without another pass.  Weights are BF16 copies of FP32
+// master weights (both orientations); activations and output gradients are
+// rounded to BF16 where they feed a product.  The nearest-centroid prior of
+// the routing logits (K = d, FP32) stays a CUDA-core GEMM; so do the softmax
+// cross-entropy, the bias-gradient column sums, Adam and the per-row top-P.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
+#include "ivf.cuh"
 #include "mlp.cuh"
+#include "tc.cuh"
 
 namespace pq {
 namespace {
@@ -23,9 +28,6 @@ constexpr int GT = 64;   // output tile (rows and columns)
 constexpr int GK = 16;   // K step
 
 __device__ __forceinline__ float ld(const float* p, size_t i) { return p[i]; }
-__device__ __forceinline__ float ld(const __nv_bfloat16* p, size_t i) {
-    return __bfloat162float(p[i]);
-}
 
 // C[M x N] (= or +=) op(A)[M x K] . op(B)[K x N] (+ bias[n]) (ReLU).  A is
 // M x K row-major (lda) or, transposed, K x M; B is K x N row-major (ldb) or,
@@ -97,6 +99,270 @@ void gemm(int M, int N, int K, const TA* A, int lda, const TB* B, int ldb, float
     count_launch();
 }
 
+// ── tensor-core GEMM: C[M x N] = A[M x K] . B[N x K]^T ─────────────────────
+constexpr int TM = 128;   // output rows per CTA (TMEM lanes)
+constexpr int TN = 256;   // output columns per CTA (TMEM columns)
+constexpr int GS = 4;     // pipeline stages
+constexpr int G_THREADS = 192;  // TMA warp, MMA warp, four epilogue warps
+constexpr uint32_t G_WAIT = 1u << 24;
+constexpr int A_BYTES = TM * 128, B_BYTES = TN * 128;  // one 64-deep K block
+
+struct TcOut {
+    const float* bias;    // [N] or null
+    int relu;             // max(0, .)
+    const float* mask;    // optional ReLU-backward mask: out *= (mask[m][n] > 0)
+    int ldm;
+    float* C;             // optional FP32 [M x N], ldc
+    int ldc;
+    __nv_bfloat16* Cb;    // optional BF16 row-major, ldcb
+    int ldcb;
+    __nv_bfloat16* Ct;    // optional BF16 transposed: Ct[n * ldct + m]
+    int ldct;
+    int M, N, K;
+    int* err;
+};
+
+struct __align__(8) GemmBars {
+    uint64_t full[GS], empty[GS], done;
+    uint32_t tmem;
+    int abort;
+};
+
+__global__ void __launch_bounds__(G_THREADS, 1) k_tc_gemm(const __grid_constant__ CUtensorMap tA,
+                                                          const __grid_constant__ CUtensorMap tB,
+                                                          TcOut o) {
+    extern __shared__ __align__(1024) uint8_t graw[];
+    uint8_t* smem = graw + ((1024u - (tc::smem_u32(graw) & 1023u)) & 1023u);
+    uint8_t* sA = smem;
+    uint8_t* sB = smem + GS * A_BYTES;
+    __shared__ GemmBars Bb;
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    volatile int* abort_flag = &Bb.abort;
+    if (w == 0) {
+        tc::tmem_alloc(&Bb.tmem, TN);
+        tc::tmem_relinquish();
+    }
+    if (tid == 32) {
+        for (int s = 0; s < GS; ++s) {
+            tc::mbar_init(&Bb.full[s], 1);
+            tc::mbar_init(&Bb.empty[s], 1);
+        }
+        tc::mbar_init(&Bb.done, 1);
+        tc::fence_barrier_init();
+        Bb.abort = 0;
+        tc::prefetch_tmap(&tA);
+        tc::prefetch_tmap(&tB);
+    }
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t taddr = Bb.tmem;
+    const int m0 = blockIdx.y * TM, n0 = blockIdx.x * TN;
+    const int nk = (o.K + 63) / 64;
+    if (w == 0) {
+        // ── TMA producer ──
+        if (lane == 0) {
+            int issued = 0;
+            for (int kb = 0; kb < nk && !*abort_flag; ++kb) {
+                const int s = kb % GS;
+                if (!tc::mbar_wait(&Bb.empty[s], ((kb / GS) & 1) ^ 1, G_WAIT)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                tc::mbar_expect_tx(&Bb.full[s], A_BYTES + B_BYTES);
+                tc::tma_load_2d(sA + s * A_BYTES, &tA, &Bb.full[s], kb * 64, m0);
+                tc::tma_load_2d(sB + s * B_BYTES, &tB, &Bb.full[s], kb * 64, n0);
+                ++issued;
+            }
+            // every issued copy has landed before the CTA may exit
+            for (int s = 0; s < GS; ++s) {
+                const int uses = issued / GS + (s < issued % GS ? 1 : 0);
+                if (uses > 0 && !tc::mbar_wait(&Bb.full[s], (uses - 1) & 1, G_WAIT))
+                    *abort_flag = 1;
+            }
+        }
+        __syncwarp();
+    } else if (w == 1) {
+        // ── MMA issuer ──
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16_f32(TM, TN);
+            for (int kb = 0; kb < nk && !*abort_flag; ++kb) {
+                const int s = kb % GS;
+                if (!tc::mbar_wait(&Bb.full[s], (kb / GS) & 1, G_WAIT)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                tc::tc_fence_after();
+                const uint64_t dA = tc::desc_k_sw128(tc::smem_u32(sA + s * A_BYTES));
+                const uint64_t dB = tc::desc_k_sw128(tc::smem_u32(sB + s * B_BYTES));
+#pragma unroll
+                for (int kk = 0; kk < 4; ++kk)  // K = 64 as four K = 16 steps (32 B each)
+                    tc::umma_f16(taddr, dA + uint64_t(2 * kk), dB + uint64_t(2 * kk), idesc,
+                                 (kb | kk) > 0 ? 1u : 0u);
+                tc::umma_commit(&Bb.empty[s]);
+            }
+            // every issued MMA has completed before the epilogue reads TMEM
+            tc::umma_commit(&Bb.done);
+        }
+        __syncwarp();
+    } else {
+        // ── epilogue: warp w reads TMEM lanes 32 (w % 4) .. + 32 ──
+        const int quarter = w & 3;
+        const int m = m0 + quarter * 32 + lane;
+        const uint32_t lane_base = uint32_t(quarter * 32) << 16;
+        const bool ok = __all_sync(0xFFFFFFFFu, tc::mbar_wait(&Bb.done, 0, G_WAIT));
+        if (!ok) {
+            if (lane == 0) *abort_flag = 1;
+        } else {
+            tc::tc_fence_after();
+            for (int c = 0; c < TN / 32; ++c) {
+                uint32_t r[32];
+                tc::tmem_ld32(taddr + lane_base + uint32_t(c * 32), r);
+                tc::tmem_ld_wait();
+                const int nb = n0 + c * 32;
+                if (nb >= o.N) break;
+                float v[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    float x = __uint_as_float(r[j]);
+                    if (o.bias) x += o.bias[nb + j];
+                    if (o.relu) x = fmaxf(x, 0.f);
+                    v[j] = x;
+                }
+                if (m < o.M) {
+                    if (o.mask) {
+                        const float4* mk = reinterpret_cast<const float4*>(o.mask + size_t(m) * o.ldm + nb);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q) {
+                            const float4 t = mk[q];
+                            v[4 * q] = t.x > 0.f ? v[4 * q] : 0.f;
+                            v[4 * q + 1] = t.y > 0.f ? v[4 * q + 1] : 0.f;
+                            v[4 * q + 2] = t.z > 0.f ? v[4 * q + 2] : 0.f;
+                            v[4 * q + 3] = t.w > 0.f ? v[4 * q + 3] : 0.f;
+                        }
+                    }
+                    if (o.C) {
+                        float4* cp = reinterpret_cast<float4*>(o.C + size_t(m) * o.ldc + nb);
+#pragma unroll
+                        for (int q = 0; q < 8; ++q)
+                            cp[q] = make_float4(v[4 * q], v[4 * q + 1], v[4 * q + 2], v[4 * q + 3]);
+                    }
+                    if (o.Cb) {
+                        uint4* bp = reinterpret_cast<uint4*>(o.Cb + size_t(m) * o.ldcb + nb);
+#pragma unroll
+                        for (int q = 0; q < 4; ++q) {
+                            uint32_t pk[4];
+#pragma unroll
+                            for (int h = 0; h < 4; ++h) {
+                                const __nv_bfloat162 b2 =
+                                    __floats2bfloat162_rn(v[8 * q + 2 * h], v[8 * q + 2 * h + 1]);
+                                pk[h] = *reinterpret_cast<const uint32_t*>(&b2);
+                            }
+                            bp[q] = make_uint4(pk[0], pk[1], pk[2], pk[3]);
+                        }
+                    }
+                    if (o.Ct) {
+#pragma unroll
+                        for (int j = 0; j < 32; ++j)
+                            o.Ct[size_t(nb + j) * o.ldct + m] = __float2bfloat16_rn(v[j]);
+                    }
+                }
+            }
+        }
+    }
+    __syncthreads();
+    if (*abort_flag && tid == 0 && o.err) atomicExch(o.err, 2);
+    tc::tc_fence_after();
+    if (w == 0) tc::tmem_dealloc(taddr, TN);
+}
+
+size_t tc_gemm_smem() { return 1024 + size_t(GS) * (A_BYTES + B_BYTES); }
+
+// out = A[M x K] . B[N x K]^T (A, B BF16 with leading dimensions lda, ldb;
+// K need not be a multiple of 64: reads past K are zeros).
+bool tc_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, const TcOut& o,
+             cudaStream_t st) {
+    CUtensorMap ta, tb;
+    if (!make_bf16_map_ld(&ta, A, uint64_t(o.M), uint64_t(o.K), uint64_t(lda), TM) ||
+        !make_bf16_map_ld(&tb, B, uint64_t(o.N), uint64_t(o.K), uint64_t(ldb), TN))
+        return false;
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(tc_gemm_smem()));
+        attr = true;
+    }
+    dim3 grid((o.N + TN - 1) / TN, (o.M + TM - 1) / TM);
+    k_tc_gemm<<<grid, G_THREADS, tc_gemm_smem(), st>>>(ta, tb, o);
+    count_launch();
+    return true;
+}
+
+TcOut tc_out(int M, int N, int K, int* err) {
+    TcOut o{};
+    o.M = M;
+    o.N = N;
+    o.K = K;
+    o.err = err;
+    return o;
+}
+
+// X [rows x d] FP32 -> BF16 rows padded to 64 columns (zeros) and the
+// transposed copy [64 x ldt] (rows d..63 zero).
+__global__ void k_x_bf16(const float* __restrict__ X, int rows, int d, __nv_bfloat16* __restrict__ xb,
+                         __nv_bfloat16* __restrict__ xt, int ldt) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(rows) * 64) return;
+    const int r = int(t / 64), c = int(t % 64);
+    const __nv_bfloat16 v = __float2bfloat16_rn(c < d ? X[size_t(r) * d + c] : 0.f);
+    xb[t] = v;
+    if (xt) xt[size_t(c) * ldt + r] = v;
+}
+
+// Y [rows x N] FP32 -> BF16 row-major (may be null) and transposed [N x ldt],
+// through 32 x 32 shared-memory tiles.
+__global__ void k_bf16_both(const float* __restrict__ Y, int rows, int N,
+                            __nv_bfloat16* __restrict__ yb, __nv_bfloat16* __restrict__ yt,
+                            int ldt) {
+    __shared__ float tile[32][33];
+    const int c0 = blockIdx.x * 32, r0 = blockIdx.y * 32;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;  // 256 threads: 8 rows a pass
+    for (int i = ty; i < 32; i += 8) {
+        const int r = r0 + i, c = c0 + tx;
+        float v = 0.f;
+        if (r < rows && c < N) {
+            v = Y[size_t(r) * N + c];
+            if (yb) yb[size_t(r) * N + c] = __float2bfloat16_rn(v);
+        }
+        tile[i][tx] = v;
+    }
+    __syncthreads();
+    for (int i = ty; i < 32; i += 8) {
+        const int c = c0 + i, r = r0 + tx;
+        if (c < N && r < rows) yt[size_t(c) * ldt + r] = __float2bfloat16_rn(tile[tx][i]);
+    }
+}
+
+// BF16 transposed weights: W1t [256 x 64] (columns >= d zero), W2t [256 x 256],
+// W3t [1024 x 256], from the FP32 masters W1 [d x 256], W2 [256 x 256],
+// W3 [256 x 1024].
+__global__ void k_w_transpose(const float* __restrict__ w, MlpLayout L, int d,
+                              __nv_bfloat16* __restrict__ wt) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t n1 = size_t(MLP_H) * 64, n2 = size_t(MLP_H) * MLP_H, n3 = size_t(MLP_OUT) * MLP_H;
+    if (t < n1) {
+        const int n = int(t / 64), k = int(t % 64);
+        wt[t] = __float2bfloat16_rn(k < d ? w[L.w1 + size_t(k) * MLP_H + n] : 0.f);
+    } else if (t < n1 + n2) {
+        const size_t u = t - n1;
+        const int n = int(u / MLP_H), k = int(u % MLP_H);
+        wt[t] = __float2bfloat16_rn(w[L.w2 + size_t(k) * MLP_H + n]);
+    } else if (t < n1 + n2 + n3) {
+        const size_t u = t - n1 - n2;
+        const int n = int(u / MLP_H), k = int(u % MLP_H);
+        wt[t] = __float2bfloat16_rn(w[L.w3 + size_t(k) * MLP_OUT + n]);
+    }
+}
+
 // Softmax cross-entropy of each row's logits against its sparse soft target
 // (T (bucket, weight) pairs, bucket ~0 = unused; weights sum to 1): writes
 // the loss per row and dlogits = (softmax - target) / rows.  One warp per row.
@@ -131,11 +397,6 @@ __global__ void k_softmax_xent(float* __restrict__ Z, int rows, int N,
     if (lane == 0) loss[r] = lse - tl;
 }
 
-// dH *= (H > 0)
-__global__ void k_relu_back(float* __restrict__ dH, const float* __restrict__ H, size_t n) {
-    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n && !(H[i] > 0.f)) dH[i] = 0.f;
-}
 
 // Column sums in two deterministic stages: part[c][n] = sum of rows
 // c*chunk.. of column n, then db[n] = sum over c of part[c][n].
@@ -161,7 +422,7 @@ __global__ void k_col_final(const float* __restrict__ part, int N, float* __rest
 
 __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __restrict__ v,
                        const float* __restrict__ g, size_t n, float lr, float b1, float b2,
-                       float c1, float c2, float eps, __nv_bfloat16* __restrict__ wb) {
+                       float c1, float c2, float eps) {
     const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float gi = g[i];
@@ -171,13 +432,8 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
     v[i] = vi;
     const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
     w[i] = wi;
-    if (wb) wb[i] = __float2bfloat16_rn(wi);
 }
 
-__global__ void k_f32_to_bf16(const float* __restrict__ a, size_t n, __nv_bfloat16* __restrict__ b) {
-    const size_t i = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (i < n) b[i] = __float2bfloat16_rn(a[i]);
-}
 
 // The P largest logits of each row (ties by index), descending, skipping the
 // bucket `skip[r]` (the row's own primary, probed anyway).  One warp per row.
@@ -239,49 +495,175 @@ MlpLayout mlp_layout(int d) {
     return L;
 }
 
-void mlp_forward(const MlpView& net, const float* X, int rows, float* H1, float* H2, float* Z,
-                 cudaStream_t st, const MlpPrior* prior) {
+size_t mlp_wt_elems() {
+    return size_t(MLP_H) * 64 + 2 * size_t(MLP_H) * MLP_H + 2 * size_t(MLP_OUT) * MLP_H;
+}
+
+namespace {
+// Offsets (elements) of the BF16 weight copies in `wt`; all 256-byte aligned.
+struct WtLayout {
+    size_t w1t, w2t, w3t, w2, w3;
+};
+WtLayout wt_layout() {
+    WtLayout L;
+    L.w1t = 0;
+    L.w2t = L.w1t + size_t(MLP_H) * 64;
+    L.w3t = L.w2t + size_t(MLP_H) * MLP_H;
+    L.w2 = L.w3t + size_t(MLP_OUT) * MLP_H;
+    L.w3 = L.w2 + size_t(MLP_H) * MLP_H;
+    return L;
+}
+
+// Row-major BF16 copies of W2 [256 x 256] and W3 [256 x 1024] (the B operands
+// of the backward products).
+__global__ void k_w_rowmajor(const float* __restrict__ w, MlpLayout L,
+                             __nv_bfloat16* __restrict__ w2, __nv_bfloat16* __restrict__ w3) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    const size_t n2 = size_t(MLP_H) * MLP_H, n3 = size_t(MLP_H) * MLP_OUT;
+    if (t < n2) w2[t] = __float2bfloat16_rn(w[L.w2 + t]);
+    else if (t < n2 + n3) w3[t - n2] = __float2bfloat16_rn(w[L.w3 + (t - n2)]);
+}
+
+void refresh_wt(const MlpView& net, cudaStream_t st) {
     const MlpLayout L = mlp_layout(net.d);
-    gemm<float, __nv_bfloat16, false, false>(rows, MLP_H, net.d, X, net.d, net.wb + L.w1, MLP_H,
-                                             H1, MLP_H, net.w + L.b1, true, false, st);
-    gemm<float, __nv_bfloat16, false, false>(rows, MLP_H, MLP_H, H1, MLP_H, net.wb + L.w2, MLP_H,
-                                             H2, MLP_H, net.w + L.b2, true, false, st);
-    gemm<float, __nv_bfloat16, false, false>(rows, MLP_OUT, MLP_H, H2, MLP_H, net.wb + L.w3,
-                                             MLP_OUT, Z, MLP_OUT, net.w + L.b3, false, false, st);
+    const WtLayout W = wt_layout();
+    const size_t nt = size_t(MLP_H) * 64 + size_t(MLP_H) * MLP_H + size_t(MLP_OUT) * MLP_H;
+    k_w_transpose<<<unsigned((nt + 255) / 256), 256, 0, st>>>(net.w, L, net.d, net.wt);
+    count_launch();
+    const size_t nr = size_t(MLP_H) * MLP_H + size_t(MLP_H) * MLP_OUT;
+    k_w_rowmajor<<<unsigned((nr + 255) / 256), 256, 0, st>>>(net.w, L, net.wt + W.w2,
+                                                             net.wt + W.w3);
+    count_launch();
+}
+
+size_t up64(size_t x) { return (x + 63) / 64 * 64; }
+}  // namespace
+
+size_t mlp_bufs_bytes(int rows, bool train) {
+    const size_t R = up64(size_t(rows));
+    size_t e = R * (64 + 2 * MLP_H);                              // xb, h1b, h2b
+    if (train) e += R * (MLP_OUT + MLP_H) + R * (64 + 4 * MLP_H + MLP_OUT);  // dzb, dh2b; transposes
+    return e * sizeof(__nv_bfloat16) + 16 * 256;
+}
+
+MlpBufs mlp_bufs(void* base, int rows, bool train) {
+    MlpBufs b{};
+    const size_t R = up64(size_t(rows));
+    b.ldt = int(R);
+    __nv_bfloat16* p = static_cast<__nv_bfloat16*>(base);
+    auto take = [&](size_t elems) {
+        __nv_bfloat16* q = p;
+        p += (elems + 127) / 128 * 128;  // 256-byte aligned pieces
+        return q;
+    };
+    b.xb = take(R * 64);
+    b.h1b = take(R * MLP_H);
+    b.h2b = take(R * MLP_H);
+    if (train) {
+        b.dzb = take(R * MLP_OUT);
+        b.dh2b = take(R * MLP_H);
+        b.xt = take(R * 64);
+        b.h1t = take(R * MLP_H);
+        b.h2t = take(R * MLP_H);
+        b.dzt = take(R * MLP_OUT);
+        b.dh2t = take(R * MLP_H);
+        b.dh1t = take(R * MLP_H);
+    }
+    return b;
+}
+
+cudaError_t mlp_forward(const MlpView& net, const float* X, int rows, float* H1, float* H2,
+                        float* Z, const MlpBufs& b, bool train, cudaStream_t st,
+                        const MlpPrior* prior) {
+    const MlpLayout L = mlp_layout(net.d);
+    const WtLayout W = wt_layout();
+    k_x_bf16<<<unsigned((size_t(rows) * 64 + 255) / 256), 256, 0, st>>>(
+        X, rows, net.d, b.xb, train ? b.xt : nullptr, b.ldt);
+    count_launch();
+    TcOut o = tc_out(rows, MLP_H, 64, net.err);
+    o.bias = net.w + L.b1;
+    o.relu = 1;
+    o.C = H1;
+    o.ldc = MLP_H;
+    o.Cb = b.h1b;
+    o.ldcb = MLP_H;
+    if (train) {
+        o.Ct = b.h1t;
+        o.ldct = b.ldt;
+    }
+    if (!tc_gemm(b.xb, 64, net.wt + W.w1t, 64, o, st)) return cudaErrorInvalidValue;
+    o = tc_out(rows, MLP_H, MLP_H, net.err);
+    o.bias = net.w + L.b2;
+    o.relu = 1;
+    o.C = H2;
+    o.ldc = MLP_H;
+    o.Cb = b.h2b;
+    o.ldcb = MLP_H;
+    if (train) {
+        o.Ct = b.h2t;
+        o.ldct = b.ldt;
+    }
+    if (!tc_gemm(b.h1b, MLP_H, net.wt + W.w2t, MLP_H, o, st)) return cudaErrorInvalidValue;
+    o = tc_out(rows, MLP_OUT, MLP_H, net.err);
+    o.bias = net.w + L.b3;
+    o.C = Z;
+    o.ldc = MLP_OUT;
+    if (!tc_gemm(b.h2b, MLP_H, net.wt + W.w3t, MLP_H, o, st)) return cudaErrorInvalidValue;
     if (prior && prior->cs)
         gemm<float, float, false, true>(rows, MLP_OUT, net.d, X, net.d, prior->cs, prior->ld, Z,
                                         MLP_OUT, prior->cb, false, true, st);
+    return cudaGetLastError();
 }
 
-void mlp_backward(const MlpView& net, const float* X, int rows, float* H1, float* H2, float* Z,
-                  const uint32_t* tb, const float* tw, int T, float* loss, float* dH1,
-                  float* dH2, float* grad, float* scratch, cudaStream_t st) {
+cudaError_t mlp_backward(const MlpView& net, int rows, float* H1, float* H2, float* Z,
+                         const MlpBufs& b, const uint32_t* tb, const float* tw, int T,
+                         float* loss, float* dH1, float* dH2, float* grad, float* scratch,
+                         cudaStream_t st) {
     const MlpLayout L = mlp_layout(net.d);
-    // Z becomes dZ
+    const WtLayout W = wt_layout();
+    // Z becomes dZ, and its BF16 copies
     k_softmax_xent<<<(rows + 7) / 8, 256, 0, st>>>(Z, rows, MLP_OUT, tb, tw, T, loss);
     count_launch();
-    // layer 3: dW3 = H2^T dZ, db3, dH2 = dZ W3^T, masked by ReLU
-    gemm<float, float, true, false>(MLP_H, MLP_OUT, rows, H2, MLP_H, Z, MLP_OUT, grad + L.w3,
-                                    MLP_OUT, nullptr, false, false, st);
+    k_bf16_both<<<dim3(MLP_OUT / 32, (rows + 31) / 32), 256, 0, st>>>(Z, rows, MLP_OUT, b.dzb,
+                                                                      b.dzt, b.ldt);
+    count_launch();
+    // layer 3: dW3 = H2^T dZ, db3, dH2 = (dZ W3^T) * (H2 > 0)
+    TcOut o = tc_out(MLP_H, MLP_OUT, rows, net.err);
+    o.C = grad + L.w3;
+    o.ldc = MLP_OUT;
+    if (!tc_gemm(b.h2t, b.ldt, b.dzt, b.ldt, o, st)) return cudaErrorInvalidValue;
     col_sums(Z, rows, MLP_OUT, scratch, grad + L.b3, st);
-    gemm<float, __nv_bfloat16, false, true>(rows, MLP_H, MLP_OUT, Z, MLP_OUT, net.wb + L.w3,
-                                            MLP_OUT, dH2, MLP_H, nullptr, false, false, st);
-    k_relu_back<<<unsigned((size_t(rows) * MLP_H + 255) / 256), 256, 0, st>>>(dH2, H2,
-                                                                            size_t(rows) * MLP_H);
-    count_launch();
-    // layer 2
-    gemm<float, float, true, false>(MLP_H, MLP_H, rows, H1, MLP_H, dH2, MLP_H, grad + L.w2, MLP_H,
-                                    nullptr, false, false, st);
+    o = tc_out(rows, MLP_H, MLP_OUT, net.err);
+    o.mask = H2;
+    o.ldm = MLP_H;
+    o.C = dH2;
+    o.ldc = MLP_H;
+    o.Cb = b.dh2b;
+    o.ldcb = MLP_H;
+    o.Ct = b.dh2t;
+    o.ldct = b.ldt;
+    if (!tc_gemm(b.dzb, MLP_OUT, net.wt + W.w3, MLP_OUT, o, st)) return cudaErrorInvalidValue;
+    // layer 2: dW2 = H1^T dH2, db2, dH1 = (dH2 W2^T) * (H1 > 0)
+    o = tc_out(MLP_H, MLP_H, rows, net.err);
+    o.C = grad + L.w2;
+    o.ldc = MLP_H;
+    if (!tc_gemm(b.h1t, b.ldt, b.dh2t, b.ldt, o, st)) return cudaErrorInvalidValue;
     col_sums(dH2, rows, MLP_H, scratch, grad + L.b2, st);
-    gemm<float, __nv_bfloat16, false, true>(rows, MLP_H, MLP_H, dH2, MLP_H, net.wb + L.w2, MLP_H,
-                                            dH1, MLP_H, nullptr, false, false, st);
-    k_relu_back<<<unsigned((size_t(rows) * MLP_H + 255) / 256), 256, 0, st>>>(dH1, H1,
-                                                                            size_t(rows) * MLP_H);
-    count_launch();
-    // layer 1
-    gemm<float, float, true, false>(net.d, MLP_H, rows, X, net.d, dH1, MLP_H, grad + L.w1, MLP_H,
-                                    nullptr, false, false, st);
+    o = tc_out(rows, MLP_H, MLP_H, net.err);
+    o.mask = H1;
+    o.ldm = MLP_H;
+    o.C = dH1;
+    o.ldc = MLP_H;
+    o.Ct = b.dh1t;
+    o.ldct = b.ldt;
+    if (!tc_gemm(b.dh2b, MLP_H, net.wt + W.w2, MLP_H, o, st)) return cudaErrorInvalidValue;
+    // layer 1: dW1 = X^T dH1, db1
+    o = tc_out(net.d, MLP_H, rows, net.err);
+    o.C = grad + L.w1;
+    o.ldc = MLP_H;
+    if (!tc_gemm(b.xt, b.ldt, b.dh1t, b.ldt, o, st)) return cudaErrorInvalidValue;
     col_sums(dH1, rows, MLP_H, scratch, grad + L.b1, st);
+    return cudaGetLastError();
 }
 
 void mlp_adam(MlpView& net, float* m, float* v, const float* grad, int step, float lr,
@@ -290,15 +672,12 @@ void mlp_adam(MlpView& net, float* m, float* v, const float* grad, int step, flo
     const float b1 = 0.9f, b2 = 0.999f;
     const float c1 = 1.f - powf(b1, float(step)), c2 = 1.f - powf(b2, float(step));
     k_adam<<<unsigned((np + 255) / 256), 256, 0, st>>>(net.w, m, v, grad, np, lr, b1, b2, c1, c2,
-                                                       1e-8f, net.wb);
+                                                       1e-8f);
     count_launch();
+    refresh_wt(net, st);
 }
 
-void mlp_sync_bf16(MlpView& net, cudaStream_t st) {
-    const size_t np = mlp_params(net.d);
-    k_f32_to_bf16<<<unsigned((np + 255) / 256), 256, 0, st>>>(net.w, np, net.wb);
-    count_launch();
-}
+void mlp_sync_bf16(MlpView& net, cudaStream_t st) { refresh_wt(net, st); }
 
 void mlp_topp(const float* Z, int rows, int P, const uint32_t* skip, uint32_t* out,
               cudaStream_t st) {

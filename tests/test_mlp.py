@@ -60,12 +60,17 @@ def test_cuda_gradients_match_oracle():
     rc = L.pq_mlp_grad(ctx._h, d, params.ctypes.data, X.ctypes.data, rows, tb.ctypes.data,
                        tw.ctypes.data, T, g.ctypes.data, loss.ctypes.data, z.ctypes.data)
     assert rc == 0
-    # FP32 accumulation against FP64: relative error per parameter block
-    np.testing.assert_allclose(z, ref_z, rtol=1e-4, atol=1e-4)
-    np.testing.assert_allclose(loss, ref_loss, rtol=1e-5, atol=1e-5)
+    # tensor-core products (BF16 operands, FP32 accumulation) against the FP64
+    # oracle that rounds the same operands to BF16: what remains is the FP32
+    # accumulation and the odd operand that rounds to the other BF16
+    # neighbour (its FP32 and FP64 values straddle a rounding boundary).
+    # Tolerances: logits 2e-3 (relative and absolute), per-row loss 1e-3, each
+    # parameter block's gradient 5e-3 of its largest entry.
+    np.testing.assert_allclose(z, ref_z, rtol=2e-3, atol=2e-3)
+    np.testing.assert_allclose(loss, ref_loss, rtol=1e-3, atol=1e-3)
     for (a, e) in mlp_ref.layout(d):
         err = np.max(np.abs(g[a:e] - ref_g[a:e])) / (np.max(np.abs(ref_g[a:e])) + 1e-30)
-        assert err < 1e-3, (a, e, err)
+        assert err < 5e-3, (a, e, err)
 
 
 @pytest.mark.gpu
@@ -96,3 +101,61 @@ def test_learned_router_training_and_recall():
     learned, st = run("learned")
     assert st["learn_loss_last"] < st["learn_loss_first"] - 0.01, st
     assert learned > base - 0.01, (learned, base)
+
+
+@pytest.mark.gpu
+def test_learned_init_nndescent_gains_over_rp_init():
+    """The learned-init NN-Descent against the method without it, the
+    reference's RP-forest initialisation, under the same NN-Descent options:
+    the router's top-4 buckets give initial lists (exact within those buckets)
+    from which the reference's rounds converge in fewer rounds, to a higher
+    recall@15 against FP64, without the fallback."""
+    import torch
+
+    import polariseq_b200 as pq
+    from bench import recall_fp64
+    from polariseq_b200 import synth
+
+    n, k = 300_000, 15
+    x = synth.mixture_lognormal(n, 50, 40, seed=23)
+    xd = torch.from_numpy(x).cuda()
+    ctx = pq.default_context(0)
+
+    def run(init):
+        g = pq.nndescent_dense(x, k, init=init)
+        return recall_fp64(torch, xd, g["indices"], g["data"], k, 4000)[0], ctx.stats()
+
+    rec_rp, st_rp = run("rp")
+    rec_l, st_l = run("learned")
+    assert st_l["fell_back"] == 0, st_l
+    assert st_l["learned_rounds"] < st_rp["rounds_run"], (st_l["learned_rounds"],
+                                                          st_rp["rounds_run"])
+    assert rec_l >= 0.99 and rec_l > rec_rp, (rec_l, rec_rp)
+    # the sampled estimate the fallback decision uses agrees with FP64
+    assert abs(st_l["est_recall"] - rec_l) < 0.01, (st_l["est_recall"], rec_l)
+
+
+@pytest.mark.gpu
+def test_learned_init_falls_back_to_rp_init(monkeypatch):
+    """Below the recall target (forced here above 1) the RP-initialised build
+    runs too, and the graph with the higher sampled recall is kept: the
+    result is byte for byte one of the two builds, the one its statistics
+    name."""
+    import polariseq_b200 as pq
+    from polariseq_b200 import synth
+
+    n, k = 100_000, 15
+    x = synth.mixture_lognormal(n, 50, 20, seed=29)
+    ctx = pq.default_context(0)
+    rp = pq.nndescent_dense(x, k, max_iterations=2)
+    learned = pq.nndescent_dense(x, k, max_iterations=2, init="learned")
+    monkeypatch.setenv("POLARISEQ_LEARNED_MIN_RECALL", "2")
+    got = pq.nndescent_dense(x, k, max_iterations=2, init="learned")
+    st = ctx.stats()
+    assert st["fell_back"] in (1, 2)
+    assert st["est_recall_rp"] > 0
+    want = rp if st["fell_back"] == 2 else learned
+    assert st["est_recall"] == max(st["est_recall_rp"], st["est_recall_learned"])
+    np.testing.assert_array_equal(got["indptr"], want["indptr"])
+    np.testing.assert_array_equal(got["indices"], want["indices"])
+    assert got["data"].tobytes() == want["data"].tobytes()
