@@ -62,9 +62,14 @@ def parse():
     ap.add_argument("--queries", type=int, default=20_000)
     ap.add_argument("--cpu-sample", type=int, default=262_144)
     ap.add_argument("--no-cpu", action="store_true")
-    ap.add_argument("--form", default="bf16", choices=["plain", "plain_r99", "bf16", "fp8"],
+    ap.add_argument("--form", default="bf16",
+                    choices=["plain", "plain_r99", "bf16", "fp8", "learned"],
                     help="the headline form (the others are measured too unless --skip-other)")
+    ap.add_argument("--others", default="plain,plain_r99,bf16,fp8",
+                    help="comma-separated forms measured besides the headline")
     ap.add_argument("--skip-other", action="store_true")
+    ap.add_argument("--skip-k30", action="store_true")
+    ap.add_argument("--skip-configs", action="store_true")
     ap.add_argument("--profile-only", action="store_true",
                     help="run W warm-up and K device-resident builds, print nothing else "
                          "(for ncu launch lists)")
@@ -285,13 +290,17 @@ def seqtree_roofline(per, st, n, d, peaks):
 PLAIN_R99 = {"max_candidates": 60, "delta": 0.0001, "max_iterations": 40}
 
 FORMS = {"plain": {"mode": "plain"}, "plain_r99": dict(mode="plain", **PLAIN_R99),
-         "bf16": {"mode": "bf16"}, "fp8": {"mode": "fp8"}}
+         "bf16": {"mode": "bf16"}, "fp8": {"mode": "fp8"},
+         # learned-init NN-Descent: the router's top-4 buckets seed the lists,
+         # the reference's rounds (default options) run to convergence
+         "learned": {"mode": "plain", "init": "learned"}}
 
 
 def form_opts(pq, name, k):
     f = FORMS[name]
     return pq._opts(k, f.get("max_iterations", 0), 0, f.get("max_candidates", 0), 0,
-                    f.get("delta", 0.001), f.get("leaf_size", 0), mode=pq.MODES[f["mode"]])
+                    f.get("delta", 0.001), f.get("leaf_size", 0), mode=pq.MODES[f["mode"]],
+                    init=pq.INITS[f.get("init", "rp")])
 
 
 def measure_form(torch, pq, _lib, ctx, name, xd, dev, stream, steps, warmup, barrier, world, k,
@@ -369,7 +378,12 @@ def summary(f):
             "launches_per_build": f["launches"],
             "phases_ms": {"init": st["ms_forest"], "layout_or_leaves": st["ms_leaves"],
                           "search_or_rounds": st["ms_rounds"], "finish": st["ms_extract"]},
-            "kernel_groups": f["groups"]}
+            "kernel_groups": f["groups"],
+            **({"learned": {k: st[k] for k in ("est_recall", "est_recall_learned",
+                                               "est_recall_rp", "fell_back", "learned_rounds",
+                                               "ms_learn_train", "ms_learn_route",
+                                               "learn_loss_first", "learn_loss_last")}}
+               if st.get("ms_learn_train") else {})}
 
 
 def plain_bit_exact(x, k, graph):
@@ -534,12 +548,12 @@ def main():
     forms = {args.form: head}
     forms_k30 = {}
     if others:
-        for other in ("plain", "plain_r99", "bf16", "fp8"):
+        for other in [f for f in args.others.split(",") if f]:
             if other != args.form:
                 forms[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream, sec, 3,
                                             barrier, world, k, args.queries,
                                             keep=other == "plain")
-        for other in ("bf16", "fp8", "plain"):
+        for other in ([] if args.skip_k30 else ["bf16", "fp8", "plain"]):
             try:
                 forms_k30[other] = measure_form(torch, pq, _lib, ctx, other, xd, dev, stream,
                                                 sec, 3, barrier, world, 30, args.queries)
@@ -553,11 +567,19 @@ def main():
     hdx = torch.empty(cap, dtype=torch.float32).pin_memory()
     hxn, hipn = hx.numpy(), hip.numpy().view(np.uint32)
     hixn, hdxn = hix.numpy().view(np.uint32), hdx.numpy()
-    r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
+    hf = FORMS[args.form]
+
+    def e2e_build():
+        return pq.nndescent_dense(hxn, k, hf.get("max_iterations", 0), 0,
+                                  hf.get("max_candidates", 0), 0, hf.get("delta", 0.001),
+                                  out=(hipn, hixn, hdxn), device=local, mode=hf["mode"],
+                                  init=hf.get("init", "rp"))
+
+    r = e2e_build()
     barrier()
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        r = pq.nndescent_dense(hxn, k, out=(hipn, hixn, hdxn), device=local, mode=args.form)
+        r = e2e_build()
     e2e_ms = max_over_ranks(torch, (time.perf_counter() - t0) * 1000.0 / args.steps, dev, world)
     e2e = {"value": world * n / (e2e_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": int(x.nbytes),
@@ -586,7 +608,7 @@ def main():
 
     # ── the other configurations ──
     configs = {}
-    if others:
+    if others and not args.skip_configs:
         del xd
         x2 = synth.mixture_lognormal(1_300_000, d, 40, seed=2000)
         xd2 = torch.from_numpy(x2).to(dev)

@@ -143,6 +143,32 @@ def test_graph_matches_committed_golden_fixtures():
         assert_graph_equal(g, h, name)
 
 
+def test_graph_matches_the_literal_restatement_on_reference_test_inputs():
+    """The goldens written by the second, independent restatement
+    (oracle/nndescent_literal.py) on the reference unit tests' own inputs
+    (ChaCha8 make_clustered_data, nndescent.rs:1012-1022): the CUDA graph and
+    its per-round change counts are the same, byte for byte."""
+    z = np.load(os.path.join(GOLDEN, "reference_inputs_golden.npz"))
+    ctx = pq.default_context(0)
+    for name in sorted({f.split("__")[0] for f in z.files}):
+        n, d, ncl, ds, k, seed = (int(v) for v in z[name + "__cfg"])
+        g = pq.nndescent(z[name + "__data"], k, seed=seed)
+        h = {"indptr": z[name + "__indptr"], "indices": z[name + "__indices"],
+             "data": z[name + "__dists"]}
+        assert_graph_equal(g, h, name)
+        assert ctx.stats()["changed"] == z[name + "__changed"].tolist(), name
+
+
+def test_graph_is_bit_exact_at_262k_cells():
+    """A whole graph above the sizes of the reference's tests: 262,144 cells x
+    50 PCs of the benchmark's generator (the forest's parallel levels, every
+    round), byte for byte against the oracle."""
+    x = synth.mixture_lognormal(262_144, 50, 40, seed=31)
+    g = pq.nndescent_dense(x, 15, 0, 0)
+    r = oracle.nndescent(x, 15, seed=0)
+    assert_graph_equal(g, r, "262144 x 50 k=15")
+
+
 @pytest.mark.parametrize("n", [1, 2, 3, 5, 17])
 def test_tiny_inputs_match(n):
     x = synth.blobs_rust_tests(n, 3, 2, 0)
