@@ -697,16 +697,21 @@ __global__ void k_leaf_scatter(const uint8_t* f, const uint32_t* pre, uint32_t n
 // position receives every other member of its leaf in leaf order, which is
 // the order the reference's (i<j, p-then-q) generation addresses it.
 //
-// A CTA takes LPB consecutive leaves: it stages their ids, rows and heap
-// roots in shared memory once, computes each pair's distance once into a
-// per-position table, and then each thread replays its own member's pushes.
-// A push whose distance is not below the row's root (its current worst) is
-// rejected unchanged (nndescent.rs:176), so the heap row in HBM is touched
-// only when a mate beats the root.  Tiles whose span exceeds LCAP or whose
-// leaves exceed LMAX members take the direct path.
+// A CTA takes LPB consecutive leaves: it stages their ids, rows and their
+// members' heap rows in shared memory once (the heap rows column-major, one
+// column per position, so that the pushes of a warp hit distinct banks),
+// computes each pair's distance once into a per-position table, and then each
+// thread replays its own member's pushes on the staged row and writes the row
+// back if it changed.  A push whose distance is not below the row's root (its
+// current worst) is rejected unchanged (nndescent.rs:176).  Tiles whose span
+// exceeds LCAP or whose leaves exceed LMAX members take the direct path.
 constexpr int LPB = 8;      // leaves per CTA
 constexpr int LCAP = 128;   // staged positions per CTA (= threads)
 constexpr int LMAXC = 32;   // largest leaf of the staged path
+
+size_t leaf_pairs_smem(int dp, int lmax, int k) {
+    return size_t(LCAP) * dp * 4 + size_t(LCAP) * lmax * 4 + size_t(LCAP) * k * 9;
+}
 
 template <int D>
 __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
@@ -718,8 +723,10 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
     __shared__ int staged;
     float* R = lsm;                               // LCAP * dp
     float* Dt = lsm + size_t(LCAP) * dp;          // LCAP * LMAX (LMAX: 16 or 32)
+    uint32_t* hI = reinterpret_cast<uint32_t*>(Dt + size_t(LCAP) * LMAX);  // k x LCAP
+    float* hD = reinterpret_cast<float*>(hI + size_t(k) * LCAP);           // k x LCAP
+    uint8_t* hF = reinterpret_cast<uint8_t*>(hD + size_t(k) * LCAP);       // k x LCAP
     __shared__ uint32_t sid[LCAP];
-    __shared__ float sroot[LCAP];
     __shared__ uint16_t sl0[LCAP], sl1[LCAP];     // leaf bounds of each staged position
     const uint32_t L0 = blockIdx.x * LPB;
     const uint32_t L1 = min(nleaves, L0 + LPB);
@@ -753,23 +760,33 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
         }
         return;
     }
-    if (uint32_t(tid) < span) {
-        const uint32_t p = ids[P0 + tid];
+    const bool own = uint32_t(tid) < span;
+    uint32_t p = 0;
+    if (own) {
+        p = ids[P0 + tid];
         sid[tid] = p;
-        sroot[tid] = hdist[size_t(p) * k];
         uint32_t l = 0;
         while (sls[l + 1] <= P0 + tid) ++l;
         sl0[tid] = uint16_t(sls[l] - P0);
         sl1[tid] = uint16_t(sls[l + 1] - P0);
     }
     __syncthreads();
+    // rows and heap rows, all loads in flight together
     const int q4 = dp / 4;
     for (uint32_t t = tid; t < span * q4; t += LCAP) {
         const uint32_t r = t / q4, j = t - r * q4;
         reinterpret_cast<float4*>(R)[t] = reinterpret_cast<const float4*>(X + size_t(sid[r]) * dp)[j];
     }
+    if (own) {
+        const size_t hb = size_t(p) * k;
+        for (int s = 0; s < k; ++s) {
+            hI[s * LCAP + tid] = hidx[hb + s];
+            hD[s * LCAP + tid] = hdist[hb + s];
+            hF[s * LCAP + tid] = hflag[hb + s];
+        }
+    }
     __syncthreads();
-    if (uint32_t(tid) < span) {  // each pair once: this position with its later mates
+    if (own) {  // each pair once: this position with its later mates
         const uint32_t l0 = sl0[tid], l1 = sl1[tid];
         for (uint32_t j = tid + 1; j < l1; ++j) {
             const float dd = sq_dist_exact_t<D>(R + size_t(tid) * dp, R + size_t(j) * dp, d);
@@ -778,19 +795,25 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
         }
     }
     __syncthreads();
-    if (uint32_t(tid) < span) {
+    if (own) {
         const uint32_t l0 = sl0[tid], l1 = sl1[tid];
-        const uint32_t p = sid[tid];
-        float root = sroot[tid];
-        uint32_t* ri = hidx + size_t(p) * k;
-        float* rd = hdist + size_t(p) * k;
-        uint8_t* rf = hflag + size_t(p) * k;
+        uint32_t* ri = hI + tid;
+        float* rd = hD + tid;
+        uint8_t* rf = hF + tid;
+        bool changed = false;
         for (uint32_t j = l0; j < l1; ++j) {
             if (j == uint32_t(tid)) continue;
             const float dd = Dt[size_t(tid) * LMAX + (j - l0)];
-            if (dd >= root) continue;  // heap_push would reject it unchanged
-            heap_push(ri, rd, rf, k, sid[j], dd, 1);
-            root = rd[0];
+            if (dd >= rd[0]) continue;  // heap_push would reject it unchanged
+            changed |= heap_push_strided(ri, rd, rf, k, LCAP, sid[j], dd, 1);
+        }
+        if (changed) {
+            const size_t hb = size_t(p) * k;
+            for (int s = 0; s < k; ++s) {
+                hidx[hb + s] = ri[s * LCAP];
+                hdist[hb + s] = rd[s * LCAP];
+                hflag[hb + s] = rf[s * LCAP];
+            }
         }
     }
 }
@@ -877,8 +900,12 @@ void launch_leaf_pairs(const float* X, int d, int dp, const uint32_t* ids_t,
     if (nleaves == 0) return;
     // leaves never exceed leaf_size (or come from depth > 100); a 16-wide mate
     // table covers the default leaf size 15 and keeps more CTAs resident
-    const int lmax = leaf_cap <= 16 ? 16 : LMAXC;
-    const size_t sm = (size_t(LCAP) * dp + size_t(LCAP) * lmax) * sizeof(float);
+    int lmax = leaf_cap <= 16 ? 16 : LMAXC;
+    size_t sm = leaf_pairs_smem(dp, lmax, k);
+    if (sm > 200 * 1024) {  // wide rows or large k: every tile takes the direct path
+        lmax = 0;
+        sm = 0;
+    }
     const unsigned grid = (nleaves + LPB - 1) / LPB;
     if (d == 50) {
         if (sm > 40 * 1024)

@@ -285,12 +285,9 @@ bool tc_gemm(const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb, c
     if (!make_bf16_map_ld(&ta, A, uint64_t(o.M), uint64_t(o.K), uint64_t(lda), TM) ||
         !make_bf16_map_ld(&tb, B, uint64_t(o.N), uint64_t(o.K), uint64_t(ldb), TN))
         return false;
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(tc_gemm_smem()));
-        attr = true;
-    }
+    if (cudaFuncSetAttribute(k_tc_gemm, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(tc_gemm_smem())) != cudaSuccess)
+        return false;
     dim3 grid((o.N + TN - 1) / TN, (o.M + TM - 1) / TM);
     k_tc_gemm<<<grid, G_THREADS, tc_gemm_smem(), st>>>(ta, tb, o);
     count_launch();
