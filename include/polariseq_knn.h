@@ -40,8 +40,8 @@ typedef enum pq_status {
 enum { PQ_METRIC_EUCLIDEAN = 0, PQ_METRIC_COSINE = 1 };
 
 /* Search form.  PLAIN reproduces the reference graph bit for bit; BF16 and
- * FP8 are the tensor-core shortlist forms (FP8: E4M3 tiles with per-row query
- * and per-bucket candidate power-of-two scales, k <= 15). */
+ * FP8 are the tensor-core shortlist forms (FP8: E4M3 tiles, every query and
+ * candidate row with its own power-of-two scale); both take k <= 31. */
 enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
 /* Initial neighbour lists: the reference's RP-tree forest, or learned buckets
  * (n_obs >= 65,536, n_dim <= 62, k <= 31): an MLP trained on a subsample's

@@ -667,8 +667,6 @@ int check_args(pq_ctx* c, uint64_t n, uint64_t d, const pq_nnd_opts* o) {
                     "max_candidates <= 200)");
     if (o->mode != PQ_MODE_PLAIN && o->mode != PQ_MODE_BF16 && o->mode != PQ_MODE_FP8)
         return fail(c, PQ_ENOTSUP, "mode not available in this build");
-    if (o->mode == PQ_MODE_FP8 && R.k > 15)
-        return fail(c, PQ_ENOTSUP, "the E4M3 form supports k <= 15");
     if (o->init != PQ_INIT_RP && o->init != PQ_INIT_LEARNED)
         return fail(c, PQ_ENOTSUP, "init not available in this build");
     if (o->init == PQ_INIT_LEARNED && n < 65536)

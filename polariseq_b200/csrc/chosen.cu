@@ -400,46 +400,22 @@ __global__ void k_merge_runs(const float* __restrict__ rd, const uint32_t* __res
     }
 }
 
-// Largest |x - centre| over each bucket's candidate rows (non-negative floats
-// order as their bits).
-__global__ void k_bucket_absmax(const float* __restrict__ X, int d, int dp,
-                                const uint32_t* __restrict__ perm,
-                                const uint32_t* __restrict__ cbucket,
-                                const float* __restrict__ cent, uint32_t n,
-                                unsigned* __restrict__ amax) {
-    const size_t r = size_t(blockIdx.x) * (blockDim.x / 32) + (threadIdx.x >> 5);
-    const int lane = threadIdx.x & 31;
-    if (r >= n) return;
-    const uint32_t i = perm ? perm[r] : uint32_t(r), b = cbucket[r];
-    float m = 0.f;
-    for (int j = lane; j < d; j += 32)
-        m = fmaxf(m, fabsf(X[size_t(i) * dp + j] - cent[size_t(b) * dp + j]));
-    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
-    if (lane == 0) atomicMax(&amax[b], __float_as_uint(m));
-}
-
 // Power-of-two E4M3 scale 2^floor(log2(448 / absmax)) (exact in FP32), 1 for
-// an all-zero row or bucket.
+// an all-zero row.
 __device__ __forceinline__ float e4m3_scale(float amax) {
     return amax > 0.f ? exp2f(floorf(log2f(448.0f / amax))) : 1.0f;
 }
 
-__global__ void k_bucket_scale(const unsigned* __restrict__ amax, uint32_t C,
-                               float* __restrict__ bscale) {
-    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
-    if (b < C) bscale[b] = 1.0f / e4m3_scale(__uint_as_float(amax[b]));
-}
-
 // E4M3 rows (128 one-byte columns, zero padded) of (row(src_i) - centre(c_i))
-// scaled by the row's own power-of-two scale (bucket_amax == null: queries;
-// inv_scale receives 1/scale) or its bucket's (candidates).  norm receives the
-// FP32 |dequantised row|^2, times `norm_mult`.  A half-warp per row (lane h:
-// columns 4h..4h+3, one 16-byte load of the row and of the centre; columns
-// 64..127 are zero), grid-stride over the rows; needs dp <= 64.
+// scaled by the row's own power-of-two scale; inv_scale (may be null)
+// receives 1/scale, norm the FP32 |dequantised row|^2 times `norm_mult`.  A
+// half-warp per row (lane h: columns 4h..4h+3, one 16-byte load of the row
+// and of the centre; columns 64..127 are zero), grid-stride over the rows;
+// needs dp <= 64.
 __global__ void k_to_fp8(const float* __restrict__ X, int d, int dp,
                          const uint32_t* __restrict__ src, const uint32_t* __restrict__ cid,
                          const float* __restrict__ cent, size_t rows,
-                         const unsigned* __restrict__ bucket_amax, uint32_t* __restrict__ out,
+                         uint32_t* __restrict__ out,
                          float* __restrict__ inv_scale, float* __restrict__ norm,
                          float norm_mult) {
     const int h = threadIdx.x & 15;
@@ -464,7 +440,7 @@ __global__ void k_to_fp8(const float* __restrict__ X, int d, int dp,
         }
 #pragma unroll
         for (int o = 8; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(hm, m, o));
-        const float sc = e4m3_scale(bucket_amax ? __uint_as_float(bucket_amax[c]) : m);
+        const float sc = e4m3_scale(m);
         uint32_t word = 0;
         float s = 0.f;
 #pragma unroll
@@ -1085,22 +1061,19 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const bool fp8 = o.mode == PQ_MODE_FP8;
     __nv_bfloat16* xc = nullptr;
     uint32_t* xc8 = nullptr;
-    float* xch = nullptr;    // E4M3: |x~|^2 / 2 per candidate
-    float* bscale = nullptr;  // E4M3: 1 / the bucket's scale
+    float* xch = nullptr;     // E4M3: |x~|^2 / 2 per candidate
+    float* cscale = nullptr;  // E4M3: 1 / the candidate row's own scale
     if (!fp8) {
         xc = c->get<__nv_bfloat16>("xc_bf16", size_t(n) * 64);
         float* xcn = c->get<float>("xc_norm", n);
         k_to_bf16<<<cvt_blocks(n), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, 2, xc, xcn); count_launch();
     } else {
-        unsigned* amax = c->get<unsigned>("bucket_amax", C);
-        ck(cudaMemsetAsync(amax, 0, size_t(C) * 4, st), "amax");
-        k_bucket_absmax<<<blocks(n, 8), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax); count_launch();
-        bscale = c->get<float>("bucket_scale", C);
-        k_bucket_scale<<<blocks(C, 256), 256, 0, st>>>(amax, C, bscale); count_launch();
+        // every candidate row with its own power-of-two scale (its absmax)
         xc8 = c->get<uint32_t>("xc_fp8", size_t(n) * 32);
         xch = c->get<float>("xc_half", n);
-        k_to_fp8<<<cvt_blocks(n), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, amax, xc8,
-                                                nullptr, xch, 0.5f); count_launch();
+        cscale = c->get<float>("xc_scale", n);
+        k_to_fp8<<<cvt_blocks(n), 256, 0, st>>>(xp, d, dp, nullptr, cbucket, cent, n, xc8, cscale,
+                                                xch, 0.5f); count_launch();
     }
     // query entries grouped by probe bucket (stable: cell order within a bucket);
     // the n primary entries (keys below C * C) come first, in candidate order
@@ -1136,8 +1109,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                                                       1, qb + size_t(e0) * 64, qbn + e0);
         } else {
             k_to_fp8<<<cvt_blocks(m), 256, 0, st>>>(xp, d, dp, qpos + e0, qbucket + e0, cent, m,
-                                                    nullptr, qb8 + size_t(e0) * 32,
-                                                    qscale + e0, qbn + e0, 1.0f);
+                                                    qb8 + size_t(e0) * 32, qscale + e0,
+                                                    qbn + e0, 1.0f);
         }
         count_launch();
     };
@@ -1195,7 +1168,6 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const int Ssh = ivf_shortlist(k + 1);        // per entry and column half
     const int Sout = ivf_groups() * Ssh;         // per entry: ivf_groups() ascending runs
     if (Ssh == 0) throw DeviceError{"the tensor-core form supports k <= 31"};
-    if (fp8 && Ssh > 16) throw DeviceError{"the E4M3 form supports k <= 15"};
     float* sd = c->get<float>("sl_d", ne * Sout);
     uint32_t* si = c->get<uint32_t>("sl_i", ne * Sout);
     // live length of each run by slot: [position * P + probe rank][run]; a
@@ -1295,7 +1267,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.qnorm = qbn;
             a.fp8 = fp8 ? 1 : 0;
             a.qscale = qscale;
-            a.bscale = bscale;
+            a.cscale = cscale;
             a.chalf = xch;
             a.qthr = pass ? qthr : nullptr;
             a.qself = qself;

@@ -138,9 +138,11 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     uint8_t* sC = sQ + QST * TQ * ROWB;                          // NCS x 32 KB
     float* bdall = reinterpret_cast<float*>(sC + NCS * TCN * ROWB);        // NG x BUF x TQ
     uint32_t* biall = reinterpret_cast<uint32_t*>(bdall + NG * BUF * TQ);  // NG x BUF x TQ
-    // E4M3 only: |x~|^2 / 2 of the tile's columns, per TMEM buffer parity and
-    // column half (the four warps of a half write the same values)
+    // E4M3 only: |x~|^2 / 2 and the inverse scale of the tile's columns, per
+    // TMEM buffer parity and column half (the four warps of a half write the
+    // same values)
     float* hsall = reinterpret_cast<float*>(biall + NG * BUF * TQ);        // 2 x NG x CPG
+    float* hkall = hsall + 2 * NG * CPG;                                   // 2 x NG x CPG
     __shared__ IvfBars B;
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     volatile int* abort_flag = &B.abort;
@@ -331,8 +333,9 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             const uint32_t slot = (valid && a.out_slot) ? a.out_slot[entry] : entry;
             float thr = thr0;
             float ath = (qn - thr) * 0.5f;
-            // E4M3: the accumulator's scale back to the dot product of the rows
-            const float rq = F8 && valid ? a.qscale[entry] * a.bscale[b] : 1.0f;
+            // E4M3: the query row's part of the accumulator's scale back to
+            // the dot product (the candidate's part is per column)
+            const float rq = F8 && valid ? a.qscale[entry] : 1.0f;
             // the shortlist: S ascending (distance, candidate) pairs in registers
             float sv[S];
             uint32_t sx[S];
@@ -369,11 +372,13 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                 const uint32_t cbase = cs + tt * TCN + g * CPG;
                 long long c1 = t0 ? clock64() : 0;
                 float* hs = hsall + (tb * NG + g) * CPG;
+                float* hk = hkall + (tb * NG + g) * CPG;
                 if constexpr (F8) {
 #pragma unroll
                     for (int i = 0; i < CPG / 32; ++i) {
                         const int col = i * 32 + lane;
                         hs[col] = col < lim ? a.chalf[cbase + col] : 0.0f;
+                        hk[col] = col < lim ? a.cscale[cbase + col] : 0.0f;
                     }
                     __syncwarp();
                 }
@@ -389,10 +394,11 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
 #pragma unroll
                         for (int j = 0; j < 32; j += 4) {
                             const float4 h4 = *reinterpret_cast<const float4*>(hs + q * 32 + j);
-                            v[j] = fmaf(__uint_as_float(r[j]), rq, -h4.x);
-                            v[j + 1] = fmaf(__uint_as_float(r[j + 1]), rq, -h4.y);
-                            v[j + 2] = fmaf(__uint_as_float(r[j + 2]), rq, -h4.z);
-                            v[j + 3] = fmaf(__uint_as_float(r[j + 3]), rq, -h4.w);
+                            const float4 k4 = *reinterpret_cast<const float4*>(hk + q * 32 + j);
+                            v[j] = fmaf(__uint_as_float(r[j]) * k4.x, rq, -h4.x);
+                            v[j + 1] = fmaf(__uint_as_float(r[j + 1]) * k4.y, rq, -h4.y);
+                            v[j + 2] = fmaf(__uint_as_float(r[j + 2]) * k4.z, rq, -h4.z);
+                            v[j + 3] = fmaf(__uint_as_float(r[j + 3]) * k4.w, rq, -h4.w);
                         }
                     } else {
 #pragma unroll
@@ -431,7 +437,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                             const int j = __ffs(lm) - 1;
                             lm &= lm - 1;
                             float vj = __uint_as_float(select32(r, j));
-                            if constexpr (F8) vj = fmaf(vj, rq, -hs[q * 32 + j]);
+                            if constexpr (F8) vj = fmaf(vj * hk[q * 32 + j], rq, -hs[q * 32 + j]);
                             const float dj = fmaf(-2.0f, vj, qn);
                             if (dj < thr && cb0 + j != qself) {
                                 if (buffered) {
@@ -539,7 +545,7 @@ EncodeTiledFn encode_fn() {
 template <int S, bool F8>
 size_t tiles_smem() {
     return 1024 + size_t(QST) * TQ * ROWB + size_t(cand_stages(S, F8)) * TCN * ROWB +
-           size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * NG * CPG * 4 : 0);
+           size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * 2 * NG * CPG * 4 : 0);
 }
 
 template <int S, bool F8>

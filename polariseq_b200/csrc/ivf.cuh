@@ -29,11 +29,12 @@ struct IvfTileArgs {
     // inserted at once, tightening the bound (launches that start unbounded)
     int buffered;
     // E4M3 tiles (the maps hold 128 one-byte columns per row, no norm
-    // columns): the accumulator times qscale[entry] * bscale[bucket] is the
-    // dot product, and chalf[candidate] = |x~|^2 / 2 is subtracted in FP32
+    // columns): the accumulator times qscale[entry] * cscale[candidate] (each
+    // row's own inverse scale) is the dot product, and chalf[candidate] =
+    // |x~|^2 / 2 is subtracted in FP32
     int fp8;
     const float* qscale;
-    const float* bscale;
+    const float* cscale;
     const float* chalf;
     float* out_d;            // entries x (ivf_groups() x S): ascending runs of S
     uint32_t* out_i;         // the candidate positions (~0 = none)

@@ -118,7 +118,7 @@ def test_bf16_form_small_inputs_are_exact():
 
 
 def test_fp8_form_recall_and_exact_distances():
-    """E4M3 tiles (per-row query scales, per-bucket candidate scales) with the
+    """E4M3 tiles (every query and candidate row with its own scale) with the
     exact FP32 re-rank and its default polish round: recall against FP64 and
     exact returned distances."""
     n, k = 120_000, 15
@@ -135,10 +135,14 @@ def test_fp8_form_recall_and_exact_distances():
         np.testing.assert_array_equal(g["data"][ip[i]:ip[i + 1]], want)
 
 
-def test_fp8_form_rejects_large_k():
-    x = synth.mixture_dirichlet(5000, 50, 5, seed=1)
-    with pytest.raises(NotImplementedError):
-        pq.nndescent_dense(x, 30, mode="fp8")
+def test_fp8_form_k30_recall_and_structure():
+    """E4M3 tiles at k = 30 (32-entry shortlists per column half)."""
+    n, k = 60_000, 30
+    x = synth.mixture_lognormal(n, 50, 20, seed=13)
+    g = pq.nndescent_dense(x, k, mode="fp8")
+    check_structure(g, n, k)
+    q = np.random.default_rng(4).choice(n, 1000, replace=False).astype(np.uint32)
+    assert recall(g, x, k, q) >= 0.99
 
 
 def test_bf16_form_every_row_ascending_at_4m():
