@@ -18,6 +18,8 @@
 // position of the j-th left point in [nL, size) counted from the top, and c
 // the number of right points in [0, nL).
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -263,10 +265,17 @@ __global__ void k_degenerate(ForestArgs a, PNode* nodes, uint32_t nn) {
 // with ballots, without block barriers.  The largest subtrees (their
 // depth-first chains are the critical path) run with NT = 512.
 constexpr int SCAP = 128;   // staged capacity (points): 4 per lane of warp 0
+// A subtree of at most `mcap` points (a launch parameter) is finished in mid
+// mode: its ids, sides and partition tables live in shared memory for the
+// whole subtree (the rows stay in HBM / L2), so a node costs two memory round
+// trips (the hyperplane rows, the margin rows) instead of the global mode's
+// seven; the split steps are the same code on shared-memory arrays.
 
 struct SeqShared {
     uint32_t stS[STK], stN[STK];
     uint16_t stD[STK];
+    uint32_t mS[STK], mN[STK];  // the depth-first stack inside a mid subtree
+    uint16_t mD[STK];
     uint32_t lS[STK], lN[STK];
     uint16_t lD[STK];
     uint32_t sid[SCAP], sslot[SCAP], sid2[SCAP], sslot2[SCAP];
@@ -275,7 +284,7 @@ struct SeqShared {
     uint32_t ws[32];
     uint64_t rng;
     uint32_t cntL, sc;
-    int sp, anytie;
+    int sp, msp, anytie;
 };
 
 // Draws of random_hyperplane (nndescent.rs:369-375) as positions: ids within
@@ -443,15 +452,231 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
     }
 }
 
+// One node split (random_hyperplane, margins with tie draws in position
+// order, the two-pointer partition in its closed form, random_split when the
+// hyperplane separates nothing) of positions [st, st + sz) of `ids`, with the
+// scratch arrays tmp / side / tabA / tabB at the same positions: the per-tree
+// arrays in HBM (global mode) or a mid subtree's shared-memory arrays.
+// Every thread holds the same Rng.  Returns the split point.
 template <int NT, int D>
-__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax) {
+__device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t* tmp,
+                               uint8_t* side, uint32_t* tabA, uint32_t* tabB, uint32_t st,
+                               uint32_t sz, Rng& rng, float* nv, float* xab, bool tb0,
+                               long long& tclk) {
     constexpr int PERT = 8;  // positions per thread per partition tile
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int d = a.d, dp = a.dp;
+    unsigned long long* tr = a.trace;
+    if (tr && tid == 0) {
+        atomicAdd(&tr[SEQ_T_GLOBAL_NODES], 1ull);
+        atomicAdd(&tr[SEQ_T_GLOBAL_POINTS], (unsigned long long)sz);
+    }
+    uint32_t pa, pb;
+    draw_pair(rng, sz, pa, pb);
+    {
+        const uint32_t A = ids[st + pa], B = ids[st + pb];
+        for (int j = tid; j < 2 * dp; j += NT)
+            xab[j] = j < dp ? a.X[size_t(A) * dp + j] : a.X[size_t(B) * dp + (j - dp)];
+    }
+    if (tid == 0) {
+        S.anytie = 0;
+        S.cntL = 0;
+        S.sc = 0;
+    }
+    __syncthreads();
+    for (int j = tid; j < dp; j += NT) nv[j] = j < d ? __fsub_rn(xab[j], xab[dp + j]) : 0.0f;
+    const float off = hyper_offset_t<D>(xab, xab + dp, d);
+    __syncthreads();
+    if (tb0) {
+        long long t1 = clock64();
+        tr[SEQ_T_CYC_DRAW] += t1 - tclk;
+        tclk = t1;
+    }
+    uint32_t cnt = 0;
+    bool tie = false;
+    constexpr int U = NT >= 512 ? 2 : 4;  // rows in flight per thread
+    for (uint32_t p0 = tid; p0 < sz; p0 += U * NT) {
+        uint32_t id[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t p = p0 + u * NT;
+            id[u] = ids[st + (p < sz ? p : p0)];
+        }
+        float m[U];
+#pragma unroll
+        for (int u = 0; u < U; ++u)
+            m[u] = __fadd_rn(dot_exact_t<D>(nv, a.X + size_t(id[u]) * dp, d), off);
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const uint32_t p = p0 + u * NT;
+            if (p < sz) {
+                const uint8_t c = fabsf(m[u]) < 1e-8f ? 2 : (m[u] > 0.0f ? 1 : 0);
+                side[st + p] = c;
+                tie |= c == 2;
+                cnt += c == 1;
+            }
+        }
+    }
+    if (tie) S.anytie = 1;
+    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+    if (lane == 0) atomicAdd(&S.cntL, cnt);
+    __syncthreads();
+    if (tb0) {
+        long long t1 = clock64();
+        tr[SEQ_T_CYC_MARGIN] += t1 - tclk;
+        tclk = t1;
+    }
+    if (S.anytie) {
+        if (tr && tid == 0) atomicAdd(&tr[SEQ_T_TIES], 1ull);
+        // every thread replays the tie draws; thread 0 writes the sides
+        uint32_t add = 0;
+        for (uint32_t p = 0; p < sz; ++p)
+            if (side[st + p] == 2) {
+                uint8_t v = (rng.next_u64() & 1ull) == 0 ? 1 : 0;
+                add += v;
+                __syncthreads();
+                if (tid == 0) side[st + p] = v;
+                __syncthreads();
+            }
+        if (tid == 0) S.cntL += add;
+        __syncthreads();
+    }
+    const uint32_t nL = S.cntL;
+    uint32_t carry = 0;
+    for (uint32_t t0 = 0; t0 < sz; t0 += NT * PERT) {
+        uint8_t sd[PERT];
+        uint32_t c2 = 0;
+#pragma unroll
+        for (int j = 0; j < PERT; ++j) {
+            uint32_t p = t0 + tid * PERT + j;
+            sd[j] = p < sz ? side[st + p] : 0;
+            c2 += sd[j];
+        }
+        uint32_t tt;
+        uint32_t lp = carry + bscan(c2, S.ws, &tt);
+#pragma unroll
+        for (int j = 0; j < PERT; ++j) {
+            uint32_t p = t0 + tid * PERT + j;
+            if (p < sz) {
+                if (sd[j]) {
+                    if (p >= nL) tabB[st + (nL - lp) - 1] = p;
+                } else if (p < nL) {
+                    tabA[st + (p - lp)] = p;
+                }
+                if (p == nL) S.sc = nL - lp;
+                lp += sd[j];
+            }
+        }
+        carry += tt;
+    }
+    __syncthreads();
+    const uint32_t c = S.sc;
+    carry = 0;
+    for (uint32_t t0 = 0; t0 < sz; t0 += NT * PERT) {
+        uint8_t sd[PERT];
+        uint32_t c2 = 0;
+#pragma unroll
+        for (int j = 0; j < PERT; ++j) {
+            uint32_t p = t0 + tid * PERT + j;
+            sd[j] = p < sz ? side[st + p] : 0;
+            c2 += sd[j];
+        }
+        uint32_t tt;
+        uint32_t lp = carry + bscan(c2, S.ws, &tt);
+#pragma unroll
+        for (int j = 0; j < PERT; ++j) {
+            uint32_t p = t0 + tid * PERT + j;
+            if (p < sz) {
+                uint32_t dst;
+                if (sd[j]) {
+                    dst = p < nL ? p : tabA[st + (nL - lp) - 1];
+                } else if (p < nL) {
+                    uint32_t rr = p - lp + 1;
+                    dst = (rr == 1 ? sz : tabB[st + rr - 2]) - 1;
+                } else if (p > nL) {
+                    dst = p - 1;
+                } else {
+                    dst = (c == 0 ? sz : tabB[st + c - 1]) - 1;
+                }
+                tmp[st + dst] = ids[st + p];
+                lp += sd[j];
+            }
+        }
+        carry += tt;
+    }
+    __syncthreads();
+    for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = tmp[st + p];
+    __syncthreads();
+    uint32_t split = nL;
+    if (nL == 0 || nL == sz) {
+        if (tr && tid == 0) atomicAdd(&tr[SEQ_T_DEGENERATE], 1ull);
+        for (uint32_t i = sz - 1; i >= 1; --i) {
+            uint32_t j = uint32_t(rng.below(uint64_t(i) + 1));
+            if (tid == 0) {
+                uint32_t t = ids[st + i];
+                ids[st + i] = ids[st + j];
+                ids[st + j] = t;
+            }
+            __syncthreads();
+        }
+        split = sz / 2;
+    }
+    if (tb0) {
+        long long t1 = clock64();
+        tr[SEQ_T_CYC_PART] += t1 - tclk;
+        tclk = t1;
+    }
+    return split;
+}
+
+// A staged subtree of at most smax points: ids[0, sz) (from HBM or from a mid
+// subtree's shared memory) with their rows in shared memory, finished by warp
+// 0; the ids come back in tree order.  `gpos` is its first position in the
+// tree (for the leaf flags).
+template <int NT, int D>
+__device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t gpos,
+                               uint32_t sz, uint32_t dep, Rng& rng, float* rows, float* nv,
+                               uint8_t* leaf) {
+    const int tid = threadIdx.x;
+    const int dp = a.dp;
+    for (uint32_t p = tid; p < sz; p += NT) {
+        S.sid[p] = ids[p];
+        S.sslot[p] = p;
+    }
+    __syncthreads();
+    const int q4 = dp / 4;
+    for (uint32_t t = tid; t < sz * q4; t += NT) {
+        uint32_t r = t / q4, j = t - r * q4;
+        reinterpret_cast<float4*>(rows)[t] =
+            reinterpret_cast<const float4*>(a.X + size_t(S.sid[r]) * dp)[j];
+    }
+    __syncthreads();
+    if (tid < 32) {
+        warp_subtree<D>(a, S, rows, nv, gpos, sz, dep, rng, leaf);
+        if (tid == 0) S.rng = rng.s;
+    }
+    __syncthreads();
+    rng.s = S.rng;  // the other warps adopt warp 0's Rng state
+    for (uint32_t p = tid; p < sz; p += NT) ids[p] = S.sid[p];
+    __syncthreads();
+    if (a.trace && tid == 0) atomicAdd(&a.trace[SEQ_T_STAGED_TREES], 1ull);
+}
+
+template <int NT, int D>
+__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax,
+                                                int mcap) {
     extern __shared__ __align__(16) float dyn[];
     __shared__ SeqShared S;
     float* nv = dyn;                 // dp
-    float* xab = dyn + a.dp;         // 2 * dp: the two hyperplane rows (global mode)
+    float* xab = dyn + a.dp;         // 2 * dp: the two hyperplane rows
     float* rows = dyn + 3 * a.dp;    // smax * dp
-    const int tid = threadIdx.x, lane = tid & 31;
+    // mid-subtree arrays (mcap entries each)
+    uint32_t* m_ids = reinterpret_cast<uint32_t*>(rows + size_t(smax) * a.dp);
+    uint32_t* m_tmp = m_ids + mcap;
+    uint32_t* m_tabA = m_tmp + mcap;
+    uint32_t* m_tabB = m_tabA + mcap;
+    uint8_t* m_side = reinterpret_cast<uint8_t*>(m_tabB + mcap);
+    const int tid = threadIdx.x;
     const SRoot rt = roots[blockIdx.x];
     const size_t tb = size_t(rt.tree) * a.n;
     uint32_t* ids = a.ids + tb;
@@ -460,7 +685,6 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
     uint32_t* tabA = a.tabA + tb;
     uint32_t* tabB = a.tabB + tb;
     uint8_t* leaf = a.leafflag + tb;
-    const int d = a.d, dp = a.dp;
     Rng rng{rt.seed};  // every thread holds the same state
     unsigned long long* tr = a.trace;
     const bool tb0 = tr && rt.size == tr[SEQ_T_ROOT0] && tid == 0;
@@ -483,185 +707,62 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
         }
         if (sz <= uint32_t(smax)) {
             if (tb0) tclk = clock64();
-            for (uint32_t p = tid; p < sz; p += NT) {
-                S.sid[p] = ids[st + p];
-                S.sslot[p] = p;
-            }
-            __syncthreads();
-            const int q4 = dp / 4;
-            for (uint32_t t = tid; t < sz * q4; t += NT) {
-                uint32_t r = t / q4, j = t - r * q4;
-                reinterpret_cast<float4*>(rows)[t] =
-                    reinterpret_cast<const float4*>(a.X + size_t(S.sid[r]) * dp)[j];
-            }
-            __syncthreads();
-            if (tid < 32) {
-                warp_subtree<D>(a, S, rows, nv, st, sz, dep, rng, leaf);
-                if (tid == 0) S.rng = rng.s;
-            }
-            __syncthreads();
-            rng.s = S.rng;  // the other warps adopt warp 0's Rng state
-            for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = S.sid[p];
-            __syncthreads();
+            staged_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf);
             if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
-            if (tr && tid == 0) atomicAdd(&tr[SEQ_T_STAGED_TREES], 1ull);
+            continue;
+        }
+        if (sz <= uint32_t(mcap)) {
+            // ── mid mode: the subtree's ids in shared memory until it is done ──
+            for (uint32_t p = tid; p < sz; p += NT) m_ids[p] = ids[st + p];
+            if (tid == 0) {
+                S.msp = 1;
+                S.mS[0] = 0;
+                S.mN[0] = sz;
+                S.mD[0] = uint16_t(dep);
+            }
+            __syncthreads();
+            while (S.msp > 0) {
+                const uint32_t ls = S.mS[S.msp - 1], ln = S.mN[S.msp - 1], ld = S.mD[S.msp - 1];
+                __syncthreads();
+                if (tid == 0) S.msp -= 1;
+                if (ln <= a.leaf_size || ld > 100) {
+                    if (tid == 0) leaf[st + ls] = 1;
+                    __syncthreads();
+                    continue;
+                }
+                if (ln <= uint32_t(smax)) {
+                    if (tb0) tclk = clock64();
+                    staged_subtree<NT, D>(a, S, m_ids + ls, st + ls, ln, ld, rng, rows, nv, leaf);
+                    if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
+                    continue;
+                }
+                if (tb0) tclk = clock64();
+                const uint32_t split = split_node<NT, D>(a, S, m_ids, m_tmp, m_side, m_tabA,
+                                                         m_tabB, ls, ln, rng, nv, xab, tb0, tclk);
+                if (tid == 0) {
+                    if (S.msp + 2 > STK) {
+                        atomicExch(a.err, 1);
+                        S.msp = 0;
+                    } else {
+                        S.mS[S.msp] = ls + split;  // right, after the whole left subtree
+                        S.mN[S.msp] = ln - split;
+                        S.mD[S.msp] = uint16_t(ld + 1);
+                        S.mS[S.msp + 1] = ls;
+                        S.mN[S.msp + 1] = split;
+                        S.mD[S.msp + 1] = uint16_t(ld + 1);
+                        S.msp += 2;
+                    }
+                }
+                __syncthreads();
+            }
+            for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = m_ids[p];
+            __syncthreads();
             continue;
         }
         // ── global mode ──
         if (tb0) tclk = clock64();
-        if (tr && tid == 0) {
-            atomicAdd(&tr[SEQ_T_GLOBAL_NODES], 1ull);
-            atomicAdd(&tr[SEQ_T_GLOBAL_POINTS], (unsigned long long)sz);
-        }
-        uint32_t pa, pb;
-        draw_pair(rng, sz, pa, pb);
-        {
-            const uint32_t A = ids[st + pa], B = ids[st + pb];
-            for (int j = tid; j < 2 * dp; j += NT)
-                xab[j] = j < dp ? a.X[size_t(A) * dp + j] : a.X[size_t(B) * dp + (j - dp)];
-        }
-        if (tid == 0) {
-            S.anytie = 0;
-            S.cntL = 0;
-            S.sc = 0;
-        }
-        __syncthreads();
-        for (int j = tid; j < dp; j += NT) nv[j] = j < d ? __fsub_rn(xab[j], xab[dp + j]) : 0.0f;
-        const float off = hyper_offset_t<D>(xab, xab + dp, d);
-        __syncthreads();
-        if (tb0) {
-            long long t1 = clock64();
-            tr[SEQ_T_CYC_DRAW] += t1 - tclk;
-            tclk = t1;
-        }
-        uint32_t cnt = 0;
-        bool tie = false;
-        constexpr int U = NT >= 512 ? 2 : 4;  // rows in flight per thread
-        for (uint32_t p0 = tid; p0 < sz; p0 += U * NT) {
-            uint32_t id[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t p = p0 + u * NT;
-                id[u] = ids[st + (p < sz ? p : p0)];
-            }
-            float m[U];
-#pragma unroll
-            for (int u = 0; u < U; ++u)
-                m[u] = __fadd_rn(dot_exact_t<D>(nv, a.X + size_t(id[u]) * dp, d), off);
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const uint32_t p = p0 + u * NT;
-                if (p < sz) {
-                    const uint8_t c = fabsf(m[u]) < 1e-8f ? 2 : (m[u] > 0.0f ? 1 : 0);
-                    side[st + p] = c;
-                    tie |= c == 2;
-                    cnt += c == 1;
-                }
-            }
-        }
-        if (tie) S.anytie = 1;
-        cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
-        if (lane == 0) atomicAdd(&S.cntL, cnt);
-        __syncthreads();
-        if (tb0) {
-            long long t1 = clock64();
-            tr[SEQ_T_CYC_MARGIN] += t1 - tclk;
-            tclk = t1;
-        }
-        if (S.anytie) {
-            if (tr && tid == 0) atomicAdd(&tr[SEQ_T_TIES], 1ull);
-            // every thread replays the tie draws; thread 0 writes the sides
-            uint32_t add = 0;
-            for (uint32_t p = 0; p < sz; ++p)
-                if (side[st + p] == 2) {
-                    uint8_t v = (rng.next_u64() & 1ull) == 0 ? 1 : 0;
-                    add += v;
-                    __syncthreads();
-                    if (tid == 0) side[st + p] = v;
-                    __syncthreads();
-                }
-            if (tid == 0) S.cntL += add;
-            __syncthreads();
-        }
-        const uint32_t nL = S.cntL;
-        uint32_t carry = 0;
-        for (uint32_t t0 = 0; t0 < sz; t0 += NT * PERT) {
-            uint8_t s[PERT];
-            uint32_t c2 = 0;
-#pragma unroll
-            for (int j = 0; j < PERT; ++j) {
-                uint32_t p = t0 + tid * PERT + j;
-                s[j] = p < sz ? side[st + p] : 0;
-                c2 += s[j];
-            }
-            uint32_t tt;
-            uint32_t lp = carry + bscan(c2, S.ws, &tt);
-#pragma unroll
-            for (int j = 0; j < PERT; ++j) {
-                uint32_t p = t0 + tid * PERT + j;
-                if (p < sz) {
-                    if (s[j]) {
-                        if (p >= nL) tabB[st + (nL - lp) - 1] = p;
-                    } else if (p < nL) {
-                        tabA[st + (p - lp)] = p;
-                    }
-                    if (p == nL) S.sc = nL - lp;
-                    lp += s[j];
-                }
-            }
-            carry += tt;
-        }
-        __syncthreads();
-        const uint32_t c = S.sc;
-        carry = 0;
-        for (uint32_t t0 = 0; t0 < sz; t0 += NT * PERT) {
-            uint8_t s[PERT];
-            uint32_t c2 = 0;
-#pragma unroll
-            for (int j = 0; j < PERT; ++j) {
-                uint32_t p = t0 + tid * PERT + j;
-                s[j] = p < sz ? side[st + p] : 0;
-                c2 += s[j];
-            }
-            uint32_t tt;
-            uint32_t lp = carry + bscan(c2, S.ws, &tt);
-#pragma unroll
-            for (int j = 0; j < PERT; ++j) {
-                uint32_t p = t0 + tid * PERT + j;
-                if (p < sz) {
-                    uint32_t dst;
-                    if (s[j]) {
-                        dst = p < nL ? p : tabA[st + (nL - lp) - 1];
-                    } else if (p < nL) {
-                        uint32_t rr = p - lp + 1;
-                        dst = (rr == 1 ? sz : tabB[st + rr - 2]) - 1;
-                    } else if (p > nL) {
-                        dst = p - 1;
-                    } else {
-                        dst = (c == 0 ? sz : tabB[st + c - 1]) - 1;
-                    }
-                    tmp[st + dst] = ids[st + p];
-                    lp += s[j];
-                }
-            }
-            carry += tt;
-        }
-        __syncthreads();
-        for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = tmp[st + p];
-        __syncthreads();
-        uint32_t split = nL;
-        if (nL == 0 || nL == sz) {
-            if (tr && tid == 0) atomicAdd(&tr[SEQ_T_DEGENERATE], 1ull);
-            for (uint32_t i = sz - 1; i >= 1; --i) {
-                uint32_t j = uint32_t(rng.below(uint64_t(i) + 1));
-                if (tid == 0) {
-                    uint32_t t = ids[st + i];
-                    ids[st + i] = ids[st + j];
-                    ids[st + j] = t;
-                }
-            }
-            split = sz / 2;
-        }
+        const uint32_t split =
+            split_node<NT, D>(a, S, ids, tmp, side, tabA, tabB, st, sz, rng, nv, xab, tb0, tclk);
         if (tid == 0) {
             if (S.sp + 2 > STK) {
                 atomicExch(a.err, 1);
@@ -677,7 +778,6 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
             }
         }
         __syncthreads();
-        if (tb0) tr[SEQ_T_CYC_PART] += clock64() - tclk;
     }
     if (tb0) tr[SEQ_T_CYC_TOTAL] = clock64() - t_start;
 }
@@ -861,12 +961,21 @@ void launch_degenerate(const ForestArgs& a, PNode* nodes, uint32_t nn, cudaStrea
 }
 template <int NT, int D>
 static void seqtree_launch(const ForestArgs& a, const SRoot* roots, uint32_t nr, int smax,
-                           size_t dyn, cudaStream_t st) {
+                           int mcap, cudaStream_t st) {
     if (nr == 0) return;
+    const size_t dyn = size_t(a.dp) * sizeof(float) * (3 + size_t(smax)) + size_t(mcap) * 17;
     if (dyn > 40 * 1024)
         cudaFuncSetAttribute(k_seqtree<NT, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(dyn));
-    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax); count_launch();
+    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax, mcap); count_launch();
+}
+
+// Mid-subtree capacity of a launch: as many points as fit in `budget` bytes
+// beside the staged rows (17 bytes per point), 0 below the staged capacity.
+static int mid_cap(size_t budget, size_t base, int smax) {
+    if (budget <= base) return 0;
+    int m = int(std::min<size_t>((budget - base) / 17, 1u << 15)) & ~255;
+    return m > smax ? m : 0;
 }
 
 void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, uint32_t nr,
@@ -876,14 +985,24 @@ void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, ui
     size_t row = size_t(a.dp) * sizeof(float);
     int smax = int(std::min<size_t>(SCAP, (28 * 1024) / row));
     if (smax < 2) smax = 0;
-    size_t dyn = row * (3 + size_t(smax));
+    const size_t base = row * (3 + size_t(smax));
+    // mid subtrees: the largest subtrees (one CTA per SM) take up to ~180 KB,
+    // the many small ones ~64 KB (several CTAs per SM)
+    int mcap_big = mid_cap(180 * 1024, base, smax), mcap_small = mid_cap(64 * 1024, base, smax);
+    if (const char* e = std::getenv("POLARISEQ_SEQ_MCAP")) {  // tuning: "big,small"
+        int b = 0, s2 = 0;
+        if (std::sscanf(e, "%d,%d", &b, &s2) == 2) {
+            mcap_big = std::max(0, b);
+            mcap_small = std::max(0, s2);
+        }
+    }
     // roots[0, n_big) are the largest subtrees: 512 threads each, own stream
     if (a.d == 50) {
-        seqtree_launch<512, 50>(a, roots, n_big, smax, dyn, st_big);
-        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, dyn, st);
+        seqtree_launch<512, 50>(a, roots, n_big, smax, mcap_big, st_big);
+        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, mcap_small, st);
     } else {
-        seqtree_launch<512, 0>(a, roots, n_big, smax, dyn, st_big);
-        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, dyn, st);
+        seqtree_launch<512, 0>(a, roots, n_big, smax, mcap_big, st_big);
+        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, mcap_small, st);
     }
 }
 void launch_leaf_compact(const uint8_t* leafflag_t, uint32_t n, uint32_t* leaf_start,
