@@ -28,8 +28,9 @@ import numpy as np
 from . import _lib
 
 __all__ = [
-    "PanicException", "DeviceError", "DeviceTimeout", "Context", "nndescent_dense", "nndescent", "effective_k", "default_context",
-    "neighbors_dense", "knn_batched", "fuzzy_connectivities",
+    "PanicException", "DeviceError", "DeviceTimeout", "Context", "nndescent_dense", "nndescent",
+    "effective_k", "default_context", "neighbors_dense", "knn_batched", "knn_batched_sharded",
+    "shard_samples", "fuzzy_connectivities",
 ]
 
 
@@ -385,6 +386,49 @@ def knn_batched(samples, ks, *, device: int = 0, autotune: bool = False, graph: 
         out.append((oi[o:o + m].reshape(a.shape[0], int(k)), od[o:o + m].reshape(a.shape[0], int(k))))
         o += m
     return out
+
+
+def shard_samples(sizes, world: int) -> list:
+    """The samples each of `world` ranks takes: every sample whole (its
+    search needs all of its points), largest cost (points squared) first, to
+    the rank with the least cost so far (ties to the lower rank).  A list of
+    ascending sample indices per rank; deterministic, so every rank computes
+    the same split without communication."""
+    order = sorted(range(len(sizes)), key=lambda s: (-int(sizes[s]) ** 2, s))
+    load = [0] * world
+    parts = [[] for _ in range(world)]
+    for s in order:
+        r = min(range(world), key=lambda q: (load[q], q))
+        parts[r].append(s)
+        load[r] += int(sizes[s]) ** 2
+    return [sorted(p) for p in parts]
+
+
+def knn_batched_sharded(samples, ks, *, rank: int, world: int, device: int = 0,
+                        gather: bool = True, autotune: bool = False, graph: bool = True,
+                        _compute=None):
+    """knn_batched over `world` GPUs (one process per GPU, torch.distributed
+    initialised): the samples are split whole between the ranks
+    (shard_samples) and each rank searches its share in one persistent
+    launch; no collective touches the search itself.  With `gather`, the
+    results are exchanged once at the end (all_gather_object) and every rank
+    returns the full list in sample order; else a dict {sample: (indices,
+    distances)} of its own share."""
+    parts = shard_samples([len(a) for a in samples], world)
+    mine = parts[rank]
+    run = _compute if _compute is not None else (
+        lambda xs, kk: knn_batched(xs, kk, device=device, autotune=autotune, graph=graph))
+    local = dict(zip(mine, run([samples[s] for s in mine], [ks[s] for s in mine]))) if mine else {}
+    if not gather or world == 1:
+        return local if not gather else [local[s] for s in range(len(samples))]
+    import torch.distributed as dist
+
+    allparts = [None] * world
+    dist.all_gather_object(allparts, local)
+    merged = {}
+    for part in allparts:
+        merged.update(part)
+    return [merged[s] for s in range(len(samples))]
 
 
 def neighbors_dense(embedding, n_neighbors, metric, *, device: int = 0) -> dict:
