@@ -204,3 +204,34 @@ def test_a_bounded_wait_that_gives_up_returns_timeout_and_the_context_recovers()
     for a, b in zip(got[1:], want[1:]):
         assert a.tobytes() == b.tobytes()
     ctx.close()
+
+
+def test_host_entry_point_with_short_rows_above_2_20_cells():
+    """Above 2^20 cells the host-buffer entry point copies rows to the host
+    while it re-ranks, only when no row can be short.  Forcing short rows (one
+    probe into 40,000 small buckets: some cells see fewer than k others), the
+    pre-check sends the build down the count-and-scan path: the result equals
+    the device entry point's, and the host arrays past nnz stay untouched."""
+    import torch
+
+    n, k = (1 << 20) + 1000, 15
+    x = synth.mixture_lognormal(n, 50, 30, seed=17)
+    opts = pq._opts(k, 0, 0, 0, 0, 0.001, mode=pq.MODES["bf16"], probes=1, buckets=40_000)
+    ctx = pq.default_context(0)
+    ip = np.zeros(n + 1, np.uint32)
+    ix = np.full(n * k, 0xDEADBEEF, np.uint32)
+    dx = np.full(n * k, -7.0, np.float32)
+    nnz = ctx.nndescent_into(x, opts, ip, ix, dx)
+    assert nnz < n * k, "expected some short rows"
+    assert (ix[nnz:] == 0xDEADBEEF).all() and (dx[nnz:] == -7.0).all()
+    dev = torch.device("cuda", 0)
+    xd = torch.from_numpy(x).to(dev)
+    dip = torch.empty(n + 1, dtype=torch.int32, device=dev)
+    dix = torch.empty(n * k, dtype=torch.int32, device=dev)
+    ddx = torch.empty(n * k, dtype=torch.float32, device=dev)
+    nnz2 = ctx.nndescent_device(xd, opts, dip, dix, ddx)
+    torch.cuda.synchronize(dev)
+    assert nnz2 == nnz
+    np.testing.assert_array_equal(dip.cpu().numpy().view(np.uint32), ip)
+    np.testing.assert_array_equal(dix[:nnz].cpu().numpy().view(np.uint32), ix[:nnz])
+    assert ddx[:nnz].cpu().numpy().tobytes() == dx[:nnz].tobytes()
