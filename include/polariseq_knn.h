@@ -267,6 +267,32 @@ int pq_knn_batched_into_device(pq_ctx* ctx, const float* d_data, uint64_t n_dim,
                                uint32_t* d_indices, float* d_dists, int32_t flags,
                                int32_t* shape_out, void* stream);
 
+/* Doublet scoring of many samples after their PCA (the steps of Scrublet's
+ * score_batch in crates/polariseq-core/src/doublets.rs:1040-1127), on the
+ * GPU.  Sample s has n_cells[s] cells and n_sim[s] simulated doublets, p <= 64
+ * components.  DEVICE inputs, samples back to back: d_u (f64, cells x p:
+ * each cell's counts over the gene deviations, projected), d_w and d_totals
+ * (f64 per cell: 1e6 / total and the total), d_mv (f64, n_samples x p: the
+ * projected gene means), d_pairs (u32, 2 per doublet: its two parents, cell
+ * indices local to the sample).  Each sample's points are its cells
+ * (w u - mv) and doublets (1e6 / (total_x + total_y) (u_x + u_y) - mv) in f32
+ * from f64 arithmetic in the reference's order; the exact kNN of every point
+ * within its sample runs in one persistent launch (pq_knn_batched_into_device)
+ * with k_adj = round_half_even(k (1 + n_sim / n)) neighbours; every point's
+ * score is the reference's Bayesian score from its simulated neighbours
+ * (q = (n_d + 1) / (k_adj + 2), rho the expected doublet rate), f64 into
+ * d_score_obs (cells) and d_score_sim (doublets), back to back.  Optional
+ * outputs (may be null): k_adj_out (HOST, per sample), d_pts_out (f32, all
+ * points x p) and d_knn_out (u32, each point's k_adj neighbours).  The
+ * threshold between the score modes (threshold_from_simulated) stays with the
+ * caller. */
+int pq_scrublet_scores_device(pq_ctx* ctx, uint32_t n_samples, uint64_t p,
+                              const uint64_t* n_cells, const uint64_t* n_sim, const uint32_t* k,
+                              const double* d_u, const double* d_w, const double* d_totals,
+                              const double* d_mv, const uint32_t* d_pairs, double rho,
+                              double* d_score_obs, double* d_score_sim, uint32_t* k_adj_out,
+                              float* d_pts_out, uint32_t* d_knn_out, void* stream);
+
 /* Allocation-free exact kNN.  No counterpart in the reference: it is an
  * addition of this library for callers that must not allocate device memory,
  * such as a host framework that owns the whole device budget through its own

@@ -30,7 +30,7 @@ from . import _lib
 __all__ = [
     "PanicException", "DeviceError", "DeviceTimeout", "Context", "nndescent_dense", "nndescent",
     "effective_k", "default_context", "neighbors_dense", "knn_batched", "knn_batched_sharded",
-    "shard_samples", "fuzzy_connectivities",
+    "shard_samples", "fuzzy_connectivities", "scrublet_scores",
 ]
 
 
@@ -385,6 +385,72 @@ def knn_batched(samples, ks, *, device: int = 0, autotune: bool = False, graph: 
         m = a.shape[0] * int(k)
         out.append((oi[o:o + m].reshape(a.shape[0], int(k)), od[o:o + m].reshape(a.shape[0], int(k))))
         o += m
+    return out
+
+
+def scrublet_scores(u, w, totals, mv, pairs, ks, rho: float = 0.1, *, device: int = 0,
+                    debug: bool = False):
+    """Doublet scores of many samples after their PCA, on the GPU (the steps
+    of Scrublet's score_batch, crates/polariseq-core/src/doublets.rs:
+    1040-1127): each sample's cells and simulated doublets as points, their
+    exact kNN within the sample (k_adj = round_half_even(k (1 + n_sim / n))),
+    and the Bayesian score from the simulated neighbours.
+
+    Per sample s: ``u[s]`` f64 [n, p] (projected scaled counts), ``w[s]`` and
+    ``totals[s]`` f64 [n], ``mv[s]`` f64 [p], ``pairs[s]`` int [n_sim, 2]
+    (parents of each simulated doublet), ``ks[s]`` the neighbour count.
+    Returns a list of dicts {"obs": f64 [n], "sim": f64 [n_sim], "k_adj"}
+    (with ``debug``, also the f32 points and the neighbour indices)."""
+    import torch
+
+    S = len(u)
+    p = int(np.asarray(u[0]).shape[1])
+    dev = torch.device("cuda", device)
+    nc = np.array([len(a) for a in u], np.uint64)
+    ns = np.array([len(a) for a in pairs], np.uint64)
+    kk = np.ascontiguousarray(ks, np.uint32)
+
+    def cat(xs, dt):
+        return torch.from_numpy(np.ascontiguousarray(np.concatenate(
+            [np.asarray(a, dt).reshape(len(a), -1) if np.asarray(a).ndim > 1
+             else np.asarray(a, dt) for a in xs]))).to(dev)
+
+    du, dw, dt_ = cat(u, np.float64), cat(w, np.float64), cat(totals, np.float64)
+    dmv = torch.from_numpy(np.ascontiguousarray(np.stack(mv).astype(np.float64))).to(dev)
+    dpr = cat(pairs, np.uint32) if int(ns.sum()) else None
+    so = torch.empty(int(nc.sum()), dtype=torch.float64, device=dev)
+    ss = torch.empty(int(ns.sum()), dtype=torch.float64, device=dev)
+    kadj = np.zeros(S, np.uint32)
+    npt = int(nc.sum() + ns.sum())
+    pts = torch.empty((npt, p), dtype=torch.float32, device=dev) if debug else None
+    # every sample's k_adj is at most 512 and below its point count
+    nk = int(sum((int(a) + int(b)) * min(512, int(a) + int(b) - 1) for a, b in zip(nc, ns)))
+    knn = torch.empty(max(nk, 1), dtype=torch.int32, device=dev) if debug else None
+    ctx = default_context(device)
+    with ctx._lock:
+        rc = _lib.load().pq_scrublet_scores_device(
+            ctx._h, S, p, nc.ctypes.data, ns.ctypes.data, kk.ctypes.data, du.data_ptr(),
+            dw.data_ptr(), dt_.data_ptr(), dmv.data_ptr(),
+            None if dpr is None else dpr.data_ptr(), float(rho), so.data_ptr(), ss.data_ptr(),
+            kadj.ctypes.data, None if pts is None else pts.data_ptr(),
+            None if knn is None else knn.data_ptr(), None)
+        if rc == _lib.PQ_EINVAL:
+            msg = _lib.load().pq_ctx_last_error(ctx._h).decode(errors="replace")
+            raise ValueError(f"scrublet_scores: {msg}")
+        ctx._check(rc, "scrublet_scores")
+    torch.cuda.synchronize(dev)
+    so, ss = so.cpu().numpy(), ss.cpu().numpy()
+    out, a, b, pa, ka = [], 0, 0, 0, 0
+    knn_h = knn.cpu().numpy().view(np.uint32) if debug else None
+    pts_h = pts.cpu().numpy() if debug else None
+    for s in range(S):
+        n, m, k = int(nc[s]), int(ns[s]), int(kadj[s])
+        r = {"obs": so[a:a + n], "sim": ss[b:b + m], "k_adj": k}
+        if debug:
+            r["points"] = pts_h[pa:pa + n + m]
+            r["knn"] = knn_h[ka:ka + (n + m) * k].reshape(n + m, k)
+        out.append(r)
+        a, b, pa, ka = a + n, b + m, pa + n + m, ka + (n + m) * k
     return out
 
 

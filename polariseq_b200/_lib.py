@@ -25,7 +25,7 @@ EXPORTS = (
     "pq_nndescent_probe", "pq_debug_tree", "pq_ctx_set_profiling", "pq_neighbors_into",
     "pq_neighbors_into_device", "pq_neighbors_into_device_noalloc", "pq_knn_batched_into_device",
     "pq_mlp_params", "pq_mlp_grad", "pq_fuzzy_connectivities", "pq_fuzzy_connectivities_device",
-    "pq_ctx_set_test_wait",
+    "pq_ctx_set_test_wait", "pq_scrublet_scores_device",
 )
 
 
@@ -158,5 +158,8 @@ def load(build_if_missing: bool = False):
         L.pq_fuzzy_connectivities_device.argtypes = [P, U64, P, P, P, U64, P, P, P, U64,
                                                      C.POINTER(U64), P]
         L.pq_fuzzy_connectivities_device.restype = C.c_int
+        L.pq_scrublet_scores_device.argtypes = [P, C.c_uint32, U64, P, P, P, P, P, P, P, P,
+                                                C.c_double, P, P, P, P, P, P]
+        L.pq_scrublet_scores_device.restype = C.c_int
         _lib = L
         return L
