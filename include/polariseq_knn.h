@@ -49,7 +49,7 @@ enum { PQ_MODE_PLAIN = 0, PQ_MODE_BF16 = 1, PQ_MODE_FP8 = 2 };
  *   - with PQ_MODE_BF16 / PQ_MODE_FP8 the router chooses the buckets each
  *     cell's shortlist searches;
  *   - with PQ_MODE_PLAIN it is the learned-init NN-Descent: each cell's
- *     initial list is its k nearest within its `probes` (default 4) most
+ *     initial list is its k nearest within its `probes` (default 12) most
  *     likely buckets (BF16 tensor-core tiles, exact FP32 re-rank), in place
  *     of the RP forest + random fill (nndescent.rs:768-845); the reference's
  *     rounds (max_iterations, delta, max_candidates) then run to

@@ -902,7 +902,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const uint32_t C = learned ? 1024u
                        : o.buckets > 0 ? std::min<uint32_t>(uint32_t(o.buckets), n)
                                        : std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
-    const uint32_t P_auto = nnd ? 4u : learned ? 6u : 14u;
+    const uint32_t P_auto = nnd ? 12u : learned ? 6u : 14u;
     const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : P_auto, std::min(C, 16u)));
     const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
     if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};

@@ -18,8 +18,6 @@
 // position of the j-th left point in [nL, size) counted from the top, and c
 // the number of right points in [0, nL).
 #include <algorithm>
-#include <cstdio>
-#include <cstdlib>
 
 #include "common.cuh"
 #include "kernels.cuh"
@@ -265,17 +263,10 @@ __global__ void k_degenerate(ForestArgs a, PNode* nodes, uint32_t nn) {
 // with ballots, without block barriers.  The largest subtrees (their
 // depth-first chains are the critical path) run with NT = 512.
 constexpr int SCAP = 128;   // staged capacity (points): 4 per lane of warp 0
-// A subtree of at most `mcap` points (a launch parameter) is finished in mid
-// mode: its ids, sides and partition tables live in shared memory for the
-// whole subtree (the rows stay in HBM / L2), so a node costs two memory round
-// trips (the hyperplane rows, the margin rows) instead of the global mode's
-// seven; the split steps are the same code on shared-memory arrays.
 
 struct SeqShared {
     uint32_t stS[STK], stN[STK];
     uint16_t stD[STK];
-    uint32_t mS[STK], mN[STK];  // the depth-first stack inside a mid subtree
-    uint16_t mD[STK];
     uint32_t lS[STK], lN[STK];
     uint16_t lD[STK];
     uint32_t sid[SCAP], sslot[SCAP], sid2[SCAP], sslot2[SCAP];
@@ -284,7 +275,7 @@ struct SeqShared {
     uint32_t ws[32];
     uint64_t rng;
     uint32_t cntL, sc;
-    int sp, msp, anytie;
+    int sp, anytie;
 };
 
 // Draws of random_hyperplane (nndescent.rs:369-375) as positions: ids within
@@ -452,12 +443,12 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
     }
 }
 
-// One node split (random_hyperplane, margins with tie draws in position
-// order, the two-pointer partition in its closed form, random_split when the
-// hyperplane separates nothing) of positions [st, st + sz) of `ids`, with the
-// scratch arrays tmp / side / tabA / tabB at the same positions: the per-tree
-// arrays in HBM (global mode) or a mid subtree's shared-memory arrays.
-// Every thread holds the same Rng.  Returns the split point.
+// One node split in global mode (random_hyperplane, margins with tie draws
+// in position order, the two-pointer partition in its closed form,
+// random_split when the hyperplane separates nothing) of positions
+// [st, st + sz) of `ids`, with the per-tree scratch arrays tmp / side / tabA /
+// tabB at the same positions.  Every thread holds the same Rng.  Returns the
+// split point.
 template <int NT, int D>
 __device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t* tmp,
                                uint8_t* side, uint32_t* tabA, uint32_t* tabB, uint32_t st,
@@ -629,10 +620,9 @@ __device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids,
     return split;
 }
 
-// A staged subtree of at most smax points: ids[0, sz) (from HBM or from a mid
-// subtree's shared memory) with their rows in shared memory, finished by warp
-// 0; the ids come back in tree order.  `gpos` is its first position in the
-// tree (for the leaf flags).
+// A staged subtree of at most smax points: ids[0, sz) with their rows in
+// shared memory, finished by warp 0; the ids come back in tree order.  `gpos`
+// is its first position in the tree (for the leaf flags).
 template <int NT, int D>
 __device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t gpos,
                                uint32_t sz, uint32_t dep, Rng& rng, float* rows, float* nv,
@@ -663,19 +653,12 @@ __device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids,
 }
 
 template <int NT, int D>
-__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax,
-                                                int mcap) {
+__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax) {
     extern __shared__ __align__(16) float dyn[];
     __shared__ SeqShared S;
     float* nv = dyn;                 // dp
     float* xab = dyn + a.dp;         // 2 * dp: the two hyperplane rows
     float* rows = dyn + 3 * a.dp;    // smax * dp
-    // mid-subtree arrays (mcap entries each)
-    uint32_t* m_ids = reinterpret_cast<uint32_t*>(rows + size_t(smax) * a.dp);
-    uint32_t* m_tmp = m_ids + mcap;
-    uint32_t* m_tabA = m_tmp + mcap;
-    uint32_t* m_tabB = m_tabA + mcap;
-    uint8_t* m_side = reinterpret_cast<uint8_t*>(m_tabB + mcap);
     const int tid = threadIdx.x;
     const SRoot rt = roots[blockIdx.x];
     const size_t tb = size_t(rt.tree) * a.n;
@@ -709,54 +692,6 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
             if (tb0) tclk = clock64();
             staged_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf);
             if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
-            continue;
-        }
-        if (sz <= uint32_t(mcap)) {
-            // ── mid mode: the subtree's ids in shared memory until it is done ──
-            for (uint32_t p = tid; p < sz; p += NT) m_ids[p] = ids[st + p];
-            if (tid == 0) {
-                S.msp = 1;
-                S.mS[0] = 0;
-                S.mN[0] = sz;
-                S.mD[0] = uint16_t(dep);
-            }
-            __syncthreads();
-            while (S.msp > 0) {
-                const uint32_t ls = S.mS[S.msp - 1], ln = S.mN[S.msp - 1], ld = S.mD[S.msp - 1];
-                __syncthreads();
-                if (tid == 0) S.msp -= 1;
-                if (ln <= a.leaf_size || ld > 100) {
-                    if (tid == 0) leaf[st + ls] = 1;
-                    __syncthreads();
-                    continue;
-                }
-                if (ln <= uint32_t(smax)) {
-                    if (tb0) tclk = clock64();
-                    staged_subtree<NT, D>(a, S, m_ids + ls, st + ls, ln, ld, rng, rows, nv, leaf);
-                    if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
-                    continue;
-                }
-                if (tb0) tclk = clock64();
-                const uint32_t split = split_node<NT, D>(a, S, m_ids, m_tmp, m_side, m_tabA,
-                                                         m_tabB, ls, ln, rng, nv, xab, tb0, tclk);
-                if (tid == 0) {
-                    if (S.msp + 2 > STK) {
-                        atomicExch(a.err, 1);
-                        S.msp = 0;
-                    } else {
-                        S.mS[S.msp] = ls + split;  // right, after the whole left subtree
-                        S.mN[S.msp] = ln - split;
-                        S.mD[S.msp] = uint16_t(ld + 1);
-                        S.mS[S.msp + 1] = ls;
-                        S.mN[S.msp + 1] = split;
-                        S.mD[S.msp + 1] = uint16_t(ld + 1);
-                        S.msp += 2;
-                    }
-                }
-                __syncthreads();
-            }
-            for (uint32_t p = tid; p < sz; p += NT) ids[st + p] = m_ids[p];
-            __syncthreads();
             continue;
         }
         // ── global mode ──
@@ -961,21 +896,12 @@ void launch_degenerate(const ForestArgs& a, PNode* nodes, uint32_t nn, cudaStrea
 }
 template <int NT, int D>
 static void seqtree_launch(const ForestArgs& a, const SRoot* roots, uint32_t nr, int smax,
-                           int mcap, cudaStream_t st) {
+                           size_t dyn, cudaStream_t st) {
     if (nr == 0) return;
-    const size_t dyn = size_t(a.dp) * sizeof(float) * (3 + size_t(smax)) + size_t(mcap) * 17;
     if (dyn > 40 * 1024)
         cudaFuncSetAttribute(k_seqtree<NT, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(dyn));
-    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax, mcap); count_launch();
-}
-
-// Mid-subtree capacity of a launch: as many points as fit in `budget` bytes
-// beside the staged rows (17 bytes per point), 0 below the staged capacity.
-static int mid_cap(size_t budget, size_t base, int smax) {
-    if (budget <= base) return 0;
-    int m = int(std::min<size_t>((budget - base) / 17, 1u << 15)) & ~255;
-    return m > smax ? m : 0;
+    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax); count_launch();
 }
 
 void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, uint32_t nr,
@@ -985,24 +911,14 @@ void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, ui
     size_t row = size_t(a.dp) * sizeof(float);
     int smax = int(std::min<size_t>(SCAP, (28 * 1024) / row));
     if (smax < 2) smax = 0;
-    const size_t base = row * (3 + size_t(smax));
-    // mid subtrees: the largest subtrees (one CTA per SM) take up to ~180 KB,
-    // the many small ones ~64 KB (several CTAs per SM)
-    int mcap_big = mid_cap(180 * 1024, base, smax), mcap_small = mid_cap(64 * 1024, base, smax);
-    if (const char* e = std::getenv("POLARISEQ_SEQ_MCAP")) {  // tuning: "big,small"
-        int b = 0, s2 = 0;
-        if (std::sscanf(e, "%d,%d", &b, &s2) == 2) {
-            mcap_big = std::max(0, b);
-            mcap_small = std::max(0, s2);
-        }
-    }
+    size_t dyn = row * (3 + size_t(smax));
     // roots[0, n_big) are the largest subtrees: 512 threads each, own stream
     if (a.d == 50) {
-        seqtree_launch<512, 50>(a, roots, n_big, smax, mcap_big, st_big);
-        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, mcap_small, st);
+        seqtree_launch<512, 50>(a, roots, n_big, smax, dyn, st_big);
+        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, dyn, st);
     } else {
-        seqtree_launch<512, 0>(a, roots, n_big, smax, mcap_big, st_big);
-        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, mcap_small, st);
+        seqtree_launch<512, 0>(a, roots, n_big, smax, dyn, st_big);
+        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, dyn, st);
     }
 }
 void launch_leaf_compact(const uint8_t* leafflag_t, uint32_t n, uint32_t* leaf_start,

@@ -1,6 +1,6 @@
 // Learned probes for the tensor-core form (PQ_INIT_LEARNED).
 //
-// 1. an evenly strided subsample of the cells (at most 1M) gets its plain
+// 1. an evenly strided subsample of the cells (at most 262,144) gets its plain
 //    NN-Descent graph (k = 15, the bit-exact form, on a separate context);
 // 2. each subsample cell's target is the distribution of the k-means buckets
 //    of itself and its neighbours (at most 16 distinct buckets);
@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <chrono>
 #include <numeric>
 #include <random>
@@ -179,7 +181,7 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     prior.ld = d;
     prior.cb = pcb;
     // ── 1. the subsample and its plain graph ──
-    const uint32_t ns = std::min<uint32_t>(n, 1u << 20);
+    const uint32_t ns = std::min<uint32_t>(n, 1u << 18);
     float* xs = c->get<float>("ml_xs", size_t(ns) * d);
     k_take_rows<<<blocks(size_t(ns) * d, 256), 256, 0, st>>>(X, d, dp, n, ns, xs); count_launch();
     ck(cudaStreamSynchronize(st), "subsample");
@@ -200,6 +202,16 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
         pq_ctx_destroy(g);
         cudaSetDevice(c->device);
         if (rc != PQ_OK) throw DeviceError{"subsample graph: " + msg};
+    }
+    const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
+    auto since = [](std::chrono::steady_clock::time_point a) {
+        return std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - a)
+            .count();
+    };
+    if (trace) {
+        ck(cudaStreamSynchronize(st), "trace");
+        std::fprintf(stderr, "[learned] subsample of %u cells and its plain graph: %.1f ms\n", ns,
+                     since(t0));
     }
     // ── 2. targets ──
     uint32_t* tb = c->get<uint32_t>("ml_tb", size_t(ns) * T_MAX);
@@ -263,6 +275,9 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     *loss_last = hl[epochs - 1] / double(std::max<uint64_t>(erows[epochs - 1], 1));
     const auto t1 = std::chrono::steady_clock::now();
     *ms_train = std::chrono::duration<double, std::milli>(t1 - t0).count();
+    if (trace)
+        std::fprintf(stderr, "[learned] %d epochs of %u cells (batches of %d): done at %.1f ms\n",
+                     epochs, ns, B, *ms_train);
     // ── 4. probes of every cell ──
     const uint32_t R = 65536;
     float* xr = c->get<float>("ml_xr", size_t(R) * d);
