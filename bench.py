@@ -168,8 +168,10 @@ def recall_fp64(torch, x_dev, indices, dists, k, nq, seed=7):
     ind = indices.reshape(n, k)
     dst = dists.reshape(n, k)
     qt = torch.from_numpy(q).to(x_dev.device)
-    for s in range(0, len(q), 256):
-        qi = qt[s:s + 256]
+    # query chunks whose FP64 distance rows stay near 2 GB
+    qc = int(max(8, min(256, (2 << 30) // (8 * n))))
+    for s in range(0, len(q), qc):
+        qi = qt[s:s + qc]
         xq = xd[qi]
         d2 = x2[qi][:, None] + x2[None, :] - 2.0 * (xq @ xd.T)
         d2[torch.arange(len(qi), device=d2.device), qi] = float("inf")
@@ -179,15 +181,18 @@ def recall_fp64(torch, x_dev, indices, dists, k, nq, seed=7):
         vals, idx = vals.cpu().numpy(), idx.cpu().numpy()
         order = np.lexsort((idx, vals), axis=1)
         exact = np.take_along_axis(idx, order, axis=1)[:, :k]
-        a = ind[q[s:s + 256]]
+        a = ind[q[s:s + qc]]
         for r in range(len(qi)):
             hits += len(set(exact[r].tolist()) & set(a[r].tolist()))
         # max relative error of returned distances vs the FP64 distance of each pair
         aj = torch.from_numpy(a.astype(np.int64)).to(x_dev.device)
         true = torch.sqrt(((xq[:, None, :] - xd[aj]) ** 2).sum(-1))
-        got = torch.from_numpy(dst[q[s:s + 256]].astype(np.float64)).to(x_dev.device)
+        got = torch.from_numpy(dst[q[s:s + qc]].astype(np.float64)).to(x_dev.device)
         rel = ((got - true).abs() / true.clamp_min(1e-30)).max().item()
         max_rel = max(max_rel, rel)
+    del xd, x2
+    # hand the cached blocks back: the library allocates its own workspace
+    torch.cuda.empty_cache()
     return hits / (len(q) * k), max_rel
 
 

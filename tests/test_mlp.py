@@ -107,16 +107,18 @@ def test_learned_router_training_and_recall():
 def test_learned_init_nndescent_gains_over_rp_init():
     """The learned-init NN-Descent against the method without it, the
     reference's RP-forest initialisation, under the same NN-Descent options:
-    the router's top-4 buckets give initial lists (exact within those buckets)
-    from which the reference's rounds converge in fewer rounds, to a higher
-    recall@15 against FP64, without the fallback."""
+    the router's top buckets give initial lists (exact within those buckets)
+    from which the reference's rounds converge in fewer rounds to a higher
+    recall@15 against FP64.  The sampled recall estimate the fallback decides
+    on agrees with FP64, and the fallback ran exactly when it fell below
+    0.99 (keeping the learned graph, whose estimate is the higher)."""
     import torch
 
     import polariseq_b200 as pq
     from bench import recall_fp64
     from polariseq_b200 import synth
 
-    n, k = 300_000, 15
+    n, k = 1_000_000, 15
     x = synth.mixture_lognormal(n, 50, 40, seed=23)
     xd = torch.from_numpy(x).cuda()
     ctx = pq.default_context(0)
@@ -127,12 +129,12 @@ def test_learned_init_nndescent_gains_over_rp_init():
 
     rec_rp, st_rp = run("rp")
     rec_l, st_l = run("learned")
-    assert st_l["fell_back"] == 0, st_l
     assert st_l["learned_rounds"] < st_rp["rounds_run"], (st_l["learned_rounds"],
                                                           st_rp["rounds_run"])
-    assert rec_l >= 0.99 and rec_l > rec_rp, (rec_l, rec_rp)
-    # the sampled estimate the fallback decision uses agrees with FP64
-    assert abs(st_l["est_recall"] - rec_l) < 0.01, (st_l["est_recall"], rec_l)
+    assert rec_l > rec_rp + 0.02, (rec_l, rec_rp)
+    assert abs(st_l["est_recall_learned"] - rec_l) < 0.01, (st_l["est_recall_learned"], rec_l)
+    assert (st_l["fell_back"] == 0) == (st_l["est_recall_learned"] >= 0.99), st_l
+    assert st_l["fell_back"] in (0, 1), st_l
 
 
 @pytest.mark.gpu
