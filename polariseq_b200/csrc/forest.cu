@@ -732,7 +732,8 @@ __global__ void k_leaf_scatter(const uint8_t* f, const uint32_t* pre, uint32_t n
 // position receives every other member of its leaf in leaf order, which is
 // the order the reference's (i<j, p-then-q) generation addresses it.
 //
-// A CTA takes LPB consecutive leaves: it stages their ids, rows and their
+// A CTA takes lpb consecutive leaves (as many as fit LCAP positions at the
+// tree's leaf size, at most LPB): it stages their ids, rows and their
 // members' heap rows in shared memory once (the heap rows column-major, one
 // column per position, so that the pushes of a warp hit distinct banks),
 // computes each pair's distance once into a per-position table, and then each
@@ -740,9 +741,9 @@ __global__ void k_leaf_scatter(const uint8_t* f, const uint32_t* pre, uint32_t n
 // back if it changed.  A push whose distance is not below the row's root (its
 // current worst) is rejected unchanged (nndescent.rs:176).  Tiles whose span
 // exceeds LCAP or whose leaves exceed LMAX members take the direct path.
-constexpr int LPB = 8;      // leaves per CTA
+constexpr int LPB = 8;      // leaves per CTA, at most
 constexpr int LCAP = 128;   // staged positions per CTA (= threads)
-constexpr int LMAXC = 32;   // largest leaf of the staged path
+constexpr int LMAXC = 64;   // largest leaf of the staged path
 
 size_t leaf_pairs_smem(int dp, int lmax, int k) {
     return size_t(LCAP) * dp * 4 + size_t(LCAP) * lmax * 4 + size_t(LCAP) * k * 9;
@@ -752,7 +753,7 @@ template <int D>
 __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
     const float* __restrict__ X, int d, int dp, const uint32_t* __restrict__ ids,
     const uint32_t* __restrict__ leaf_start, uint32_t nleaves, uint32_t n, int k, uint32_t* hidx,
-    float* hdist, uint8_t* hflag, int LMAX) {
+    float* hdist, uint8_t* hflag, int LMAX, int lpb) {
     extern __shared__ __align__(16) float lsm[];
     __shared__ uint32_t sls[LPB + 1];
     __shared__ int staged;
@@ -763,8 +764,8 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
     uint8_t* hF = reinterpret_cast<uint8_t*>(hD + size_t(k) * LCAP);       // k x LCAP
     __shared__ uint32_t sid[LCAP];
     __shared__ uint16_t sl0[LCAP], sl1[LCAP];     // leaf bounds of each staged position
-    const uint32_t L0 = blockIdx.x * LPB;
-    const uint32_t L1 = min(nleaves, L0 + LPB);
+    const uint32_t L0 = blockIdx.x * uint32_t(lpb);
+    const uint32_t L1 = min(nleaves, L0 + uint32_t(lpb));
     const int tid = threadIdx.x;
     if (tid <= int(L1 - L0)) {
         const uint32_t li = L0 + tid;
@@ -933,27 +934,30 @@ void launch_leaf_pairs(const float* X, int d, int dp, const uint32_t* ids_t,
                        uint32_t leaf_cap, uint32_t* hidx, float* hdist, uint8_t* hflag,
                        cudaStream_t st) {
     if (nleaves == 0) return;
-    // leaves never exceed leaf_size (or come from depth > 100); a 16-wide mate
-    // table covers the default leaf size 15 and keeps more CTAs resident
-    int lmax = leaf_cap <= 16 ? 16 : LMAXC;
+    // leaves never exceed leaf_size (or come from depth > 100); the mate table
+    // is as wide as the leaf size allows (16, 32 or 64), and a CTA takes as
+    // many leaves as fit its LCAP positions at that size
+    int lmax = leaf_cap <= 16 ? 16 : leaf_cap <= 32 ? 32 : LMAXC;
+    const int lpb = int(std::max<uint32_t>(1, std::min<uint32_t>(LPB, LCAP / std::max(leaf_cap, 1u))));
     size_t sm = leaf_pairs_smem(dp, lmax, k);
-    if (sm > 200 * 1024) {  // wide rows or large k: every tile takes the direct path
+    if (sm > 200 * 1024 || leaf_cap > uint32_t(LMAXC)) {
+        // wide rows, large k or large leaves: every tile takes the direct path
         lmax = 0;
         sm = 0;
     }
-    const unsigned grid = (nleaves + LPB - 1) / LPB;
+    const unsigned grid = (nleaves + lpb - 1) / lpb;
     if (d == 50) {
         if (sm > 40 * 1024)
             cudaFuncSetAttribute(k_leaf_pairs<50>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sm));
         k_leaf_pairs<50><<<grid, LCAP, sm, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
-                                                 hidx, hdist, hflag, lmax); count_launch();
+                                                 hidx, hdist, hflag, lmax, lpb); count_launch();
     } else {
         if (sm > 40 * 1024)
             cudaFuncSetAttribute(k_leaf_pairs<0>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  int(sm));
         k_leaf_pairs<0><<<grid, LCAP, sm, st>>>(X, d, dp, ids_t, leaf_start, nleaves, n, k,
-                                                hidx, hdist, hflag, lmax); count_launch();
+                                                hidx, hdist, hflag, lmax, lpb); count_launch();
     }
 }
 void launch_random_fill(const float* X, int d, int dp, uint32_t n, int k, uint64_t seed,
