@@ -229,6 +229,7 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     ck(cudaMemsetAsync(av, 0, np * 4, st), "adam");
     k_init_params<<<blocks(np, 256), 256, 0, st>>>(net.w, np, mlp_layout(d), d, seed); count_launch();
     mlp_sync_bf16(net, st);
+    mlp_set_prior(net, prior, st);
     const int B = 4096, epochs = 8;
     float* xb = c->get<float>("ml_xb", size_t(B) * d);
     uint32_t* bb = c->get<uint32_t>("ml_bb", size_t(B) * T_MAX);

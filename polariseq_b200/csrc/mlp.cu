@@ -12,8 +12,10 @@
 // next one's operand without another pass.  Weights are BF16 copies of FP32
 // master weights (both orientations); activations and output gradients are
 // rounded to BF16 where they feed a product.  The nearest-centroid prior of
-// the routing logits (K = d, FP32) stays a CUDA-core GEMM; so do the softmax
-// cross-entropy, the bias-gradient column sums, Adam and the per-row top-P.
+// the routing logits rides in the output product as 192 extra K columns:
+// x.cs = x_hi.cs_hi + x_lo.cs_hi + x_hi.cs_lo with BF16 hi / lo splits of
+// both sides (about 16 bits of each).  The softmax cross-entropy, the
+// bias-gradient column sums, Adam and the per-row top-P run on CUDA cores.
 #include <cuda_bf16.h>
 
 #include "common.cuh"
@@ -23,81 +25,6 @@
 
 namespace pq {
 namespace {
-
-constexpr int GT = 64;   // output tile (rows and columns)
-constexpr int GK = 16;   // K step
-
-__device__ __forceinline__ float ld(const float* p, size_t i) { return p[i]; }
-
-// C[M x N] (= or +=) op(A)[M x K] . op(B)[K x N] (+ bias[n]) (ReLU).  A is
-// M x K row-major (lda) or, transposed, K x M; B is K x N row-major (ldb) or,
-// transposed, N x K.
-template <typename TA, typename TB, bool TRA, bool TRB>
-__global__ void __launch_bounds__(256) k_gemm(int M, int N, int K, const TA* __restrict__ A,
-                                              int lda, const TB* __restrict__ B, int ldb,
-                                              float* __restrict__ C, int ldc,
-                                              const float* __restrict__ bias, int relu,
-                                              int accumulate) {
-    __shared__ float As[GK][GT + 4];
-    __shared__ float Bs[GK][GT + 4];
-    const int tx = threadIdx.x & 15, ty = threadIdx.x >> 4;
-    const int m0 = blockIdx.y * GT, n0 = blockIdx.x * GT;
-    float acc[4][4] = {};
-    for (int k0 = 0; k0 < K; k0 += GK) {
-        for (int t = threadIdx.x; t < GT * GK; t += 256) {
-            // A tile: As[kk][mm] = op(A)[m0 + mm][k0 + kk]
-            const int mm = TRA ? t % GT : t / GK, kk = TRA ? t / GT : t % GK;
-            const int m = m0 + mm, k = k0 + kk;
-            float va = 0.f;
-            if (m < M && k < K) va = TRA ? ld(A, size_t(k) * lda + m) : ld(A, size_t(m) * lda + k);
-            As[kk][mm] = va;
-            // B tile: Bs[kk][nn] = op(B)[k0 + kk][n0 + nn]
-            const int nn = TRB ? t / GK : t % GT, kb = TRB ? t % GK : t / GT;
-            const int n = n0 + nn, kq = k0 + kb;
-            float vb = 0.f;
-            if (n < N && kq < K) vb = TRB ? ld(B, size_t(n) * ldb + kq) : ld(B, size_t(kq) * ldb + n);
-            Bs[kb][nn] = vb;
-        }
-        __syncthreads();
-#pragma unroll
-        for (int kk = 0; kk < GK; ++kk) {
-            float a[4], b[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = As[kk][ty * 4 + i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) b[j] = Bs[kk][tx * 4 + j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i) {
-        const int m = m0 + ty * 4 + i;
-        if (m >= M) continue;
-#pragma unroll
-        for (int j = 0; j < 4; ++j) {
-            const int n = n0 + tx * 4 + j;
-            if (n >= N) continue;
-            float v = acc[i][j];
-            if (bias) v += bias[n];
-            if (relu) v = fmaxf(v, 0.f);
-            float* c = C + size_t(m) * ldc + n;
-            *c = accumulate ? *c + v : v;
-        }
-    }
-}
-
-template <typename TA, typename TB, bool TRA, bool TRB>
-void gemm(int M, int N, int K, const TA* A, int lda, const TB* B, int ldb, float* C, int ldc,
-          const float* bias, bool relu, bool accumulate, cudaStream_t st) {
-    dim3 grid((N + GT - 1) / GT, (M + GT - 1) / GT);
-    k_gemm<TA, TB, TRA, TRB><<<grid, 256, 0, st>>>(M, N, K, A, lda, B, ldb, C, ldc, bias,
-                                                   relu ? 1 : 0, accumulate ? 1 : 0);
-    count_launch();
-}
 
 // ── tensor-core GEMM: C[M x N] = A[M x K] . B[N x K]^T ─────────────────────
 constexpr int TM = 128;   // output rows per CTA (TMEM lanes)
@@ -109,6 +36,7 @@ constexpr int A_BYTES = TM * 128, B_BYTES = TN * 128;  // one 64-deep K block
 
 struct TcOut {
     const float* bias;    // [N] or null
+    const float* bias2;   // a second [N] added, or null
     int relu;             // max(0, .)
     const float* mask;    // optional ReLU-backward mask: out *= (mask[m][n] > 0)
     int ldm;
@@ -225,6 +153,7 @@ __global__ void __launch_bounds__(G_THREADS, 1) k_tc_gemm(const __grid_constant_
                 for (int j = 0; j < 32; ++j) {
                     float x = __uint_as_float(r[j]);
                     if (o.bias) x += o.bias[nb + j];
+                    if (o.bias2) x += o.bias2[nb + j];
                     if (o.relu) x = fmaxf(x, 0.f);
                     v[j] = x;
                 }
@@ -305,14 +234,42 @@ TcOut tc_out(int M, int N, int K, int* err) {
 
 // X [rows x d] FP32 -> BF16 rows padded to 64 columns (zeros) and the
 // transposed copy [64 x ldt] (rows d..63 zero).
+// (ext, if not null: the prior's columns [x_hi | x_lo | x_hi] of the output
+// product's A operand, 192 columns from ext + r * ldext.)
 __global__ void k_x_bf16(const float* __restrict__ X, int rows, int d, __nv_bfloat16* __restrict__ xb,
-                         __nv_bfloat16* __restrict__ xt, int ldt) {
+                         __nv_bfloat16* __restrict__ xt, int ldt, __nv_bfloat16* __restrict__ ext,
+                         int ldext) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
     if (t >= size_t(rows) * 64) return;
     const int r = int(t / 64), c = int(t % 64);
-    const __nv_bfloat16 v = __float2bfloat16_rn(c < d ? X[size_t(r) * d + c] : 0.f);
+    const float x = c < d ? X[size_t(r) * d + c] : 0.f;
+    const __nv_bfloat16 v = __float2bfloat16_rn(x);
     xb[t] = v;
     if (xt) xt[size_t(c) * ldt + r] = v;
+    if (ext) {
+        const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(v));
+        __nv_bfloat16* e = ext + size_t(r) * ldext;
+        e[c] = v;
+        e[64 + c] = lo;
+        e[128 + c] = v;
+    }
+}
+
+// The prior's columns of the output product's B operand: row n (bucket) of
+// W3t gets [cs_hi | cs_hi | cs_lo] of cs[n] (d values, zeros to 64 each) in
+// columns MLP_H .. MLP_H + 191.
+__global__ void k_prior_cols(const float* __restrict__ cs, int ld, int d,
+                             __nv_bfloat16* __restrict__ w3t, int ldw) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(MLP_OUT) * 64) return;
+    const int n = int(t / 64), c = int(t % 64);
+    const float x = c < d ? cs[size_t(n) * ld + c] : 0.f;
+    const __nv_bfloat16 hi = __float2bfloat16_rn(x);
+    const __nv_bfloat16 lo = __float2bfloat16_rn(x - __bfloat162float(hi));
+    __nv_bfloat16* e = w3t + size_t(n) * ldw + MLP_H;
+    e[c] = hi;
+    e[64 + c] = hi;
+    e[128 + c] = lo;
 }
 
 // Y [rows x N] FP32 -> BF16 row-major (may be null) and transposed [N x ldt],
@@ -340,8 +297,8 @@ __global__ void k_bf16_both(const float* __restrict__ Y, int rows, int N,
 }
 
 // BF16 transposed weights: W1t [256 x 64] (columns >= d zero), W2t [256 x 256],
-// W3t [1024 x 256], from the FP32 masters W1 [d x 256], W2 [256 x 256],
-// W3 [256 x 1024].
+// W3t [1024 x 256] (leading dimension MLP_K3: its prior columns are left as
+// they are), from the FP32 masters W1 [d x 256], W2 [256 x 256], W3 [256 x 1024].
 __global__ void k_w_transpose(const float* __restrict__ w, MlpLayout L, int d,
                               __nv_bfloat16* __restrict__ wt) {
     const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -356,7 +313,7 @@ __global__ void k_w_transpose(const float* __restrict__ w, MlpLayout L, int d,
     } else if (t < n1 + n2 + n3) {
         const size_t u = t - n1 - n2;
         const int n = int(u / MLP_H), k = int(u % MLP_H);
-        wt[t] = __float2bfloat16_rn(w[L.w3 + size_t(k) * MLP_OUT + n]);
+        wt[n1 + n2 + size_t(n) * MLP_K3 + k] = __float2bfloat16_rn(w[L.w3 + size_t(k) * MLP_OUT + n]);
     }
 }
 
@@ -433,27 +390,33 @@ __global__ void k_adam(float* __restrict__ w, float* __restrict__ m, float* __re
 
 
 // The P largest logits of each row (ties by index), descending, skipping the
-// bucket `skip[r]` (the row's own primary, probed anyway).  One warp per row.
-__global__ void k_topp(const float* __restrict__ Z, int rows, int N, int P,
+// bucket `skip[r]` (the row's own primary, probed anyway).  One warp per row:
+// each lane holds its 32 columns (j = 32 t + lane) in registers, and each of
+// the P picks is a register scan and a warp argmax.
+__global__ void k_topp(const float* __restrict__ Z, int rows, int P,
                        const uint32_t* __restrict__ skip, uint32_t* __restrict__ out) {
     const int r = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
     const int lane = threadIdx.x & 31;
     if (r >= rows) return;
-    const float* z = Z + size_t(r) * N;
+    constexpr int PER = MLP_OUT / 32;
+    const float* z = Z + size_t(r) * MLP_OUT;
     const uint32_t sk = skip ? skip[r] : 0xFFFFFFFFu;
-    uint32_t taken = 0;  // bits of this lane's columns already chosen (N <= 1024)
+    float v[PER];
+#pragma unroll
+    for (int t = 0; t < PER; ++t) {
+        const int j = t * 32 + lane;
+        v[t] = uint32_t(j) == sk ? -__int_as_float(0x7f800000) : z[j];
+    }
     for (int p = 0; p < P; ++p) {
         float bv = -__int_as_float(0x7f800000);
-        int bj = 0x7FFFFFFF;
-        for (int t = 0; t * 32 + lane < N; ++t) {
-            const int j = t * 32 + lane;
-            if ((taken >> t) & 1u || uint32_t(j) == sk) continue;
-            const float v = z[j];
-            if (v > bv || (v == bv && j < bj)) {
-                bv = v;
-                bj = j;
+        int bt = 0;
+#pragma unroll
+        for (int t = 0; t < PER; ++t)
+            if (v[t] > bv) {  // strict: the lowest column wins a tie within the lane
+                bv = v[t];
+                bt = t;
             }
-        }
+        int bj = bv == -__int_as_float(0x7f800000) ? 0x7FFFFFFF : bt * 32 + lane;
         for (int o = 16; o > 0; o >>= 1) {
             const float ov = __shfl_xor_sync(0xFFFFFFFFu, bv, o);
             const int oj = __shfl_xor_sync(0xFFFFFFFFu, bj, o);
@@ -462,8 +425,12 @@ __global__ void k_topp(const float* __restrict__ Z, int rows, int N, int P,
                 bj = oj;
             }
         }
-        if (lane == (bj & 31)) taken |= 1u << (bj >> 5);
-        if (lane == 0) out[size_t(r) * P + p] = uint32_t(bj);
+        if (bj != 0x7FFFFFFF && lane == (bj & 31)) {
+#pragma unroll
+            for (int t = 0; t < PER; ++t)
+                if (t == (bj >> 5)) v[t] = -__int_as_float(0x7f800000);
+        }
+        if (lane == 0) out[size_t(r) * P + p] = bj == 0x7FFFFFFF ? 0u : uint32_t(bj);
     }
 }
 
@@ -493,7 +460,8 @@ MlpLayout mlp_layout(int d) {
 }
 
 size_t mlp_wt_elems() {
-    return size_t(MLP_H) * 64 + 2 * size_t(MLP_H) * MLP_H + 2 * size_t(MLP_OUT) * MLP_H;
+    return size_t(MLP_H) * 64 + 2 * size_t(MLP_H) * MLP_H + size_t(MLP_OUT) * MLP_K3 +
+           size_t(MLP_OUT) * MLP_H;
 }
 
 namespace {
@@ -506,7 +474,7 @@ WtLayout wt_layout() {
     L.w1t = 0;
     L.w2t = L.w1t + size_t(MLP_H) * 64;
     L.w3t = L.w2t + size_t(MLP_H) * MLP_H;
-    L.w2 = L.w3t + size_t(MLP_OUT) * MLP_H;
+    L.w2 = L.w3t + size_t(MLP_OUT) * MLP_K3;
     L.w3 = L.w2 + size_t(MLP_H) * MLP_H;
     return L;
 }
@@ -538,7 +506,7 @@ size_t up64(size_t x) { return (x + 63) / 64 * 64; }
 
 size_t mlp_bufs_bytes(int rows, bool train) {
     const size_t R = up64(size_t(rows));
-    size_t e = R * (64 + 2 * MLP_H);                              // xb, h1b, h2b
+    size_t e = R * (64 + MLP_H + MLP_K3);                         // xb, h1b, h2b
     if (train) e += R * (MLP_OUT + MLP_H) + R * (64 + 4 * MLP_H + MLP_OUT);  // dzb, dh2b; transposes
     return e * sizeof(__nv_bfloat16) + 16 * 256;
 }
@@ -555,7 +523,7 @@ MlpBufs mlp_bufs(void* base, int rows, bool train) {
     };
     b.xb = take(R * 64);
     b.h1b = take(R * MLP_H);
-    b.h2b = take(R * MLP_H);
+    b.h2b = take(R * MLP_K3);
     if (train) {
         b.dzb = take(R * MLP_OUT);
         b.dh2b = take(R * MLP_H);
@@ -574,8 +542,10 @@ cudaError_t mlp_forward(const MlpView& net, const float* X, int rows, float* H1,
                         const MlpPrior* prior) {
     const MlpLayout L = mlp_layout(net.d);
     const WtLayout W = wt_layout();
+    const bool pr = prior && prior->cs;
     k_x_bf16<<<unsigned((size_t(rows) * 64 + 255) / 256), 256, 0, st>>>(
-        X, rows, net.d, b.xb, train ? b.xt : nullptr, b.ldt);
+        X, rows, net.d, b.xb, train ? b.xt : nullptr, b.ldt, pr ? b.h2b + MLP_H : nullptr,
+        MLP_K3);
     count_launch();
     TcOut o = tc_out(rows, MLP_H, 64, net.err);
     o.bias = net.w + L.b1;
@@ -595,20 +565,19 @@ cudaError_t mlp_forward(const MlpView& net, const float* X, int rows, float* H1,
     o.C = H2;
     o.ldc = MLP_H;
     o.Cb = b.h2b;
-    o.ldcb = MLP_H;
+    o.ldcb = MLP_K3;
     if (train) {
         o.Ct = b.h2t;
         o.ldct = b.ldt;
     }
     if (!tc_gemm(b.h1b, MLP_H, net.wt + W.w2t, MLP_H, o, st)) return cudaErrorInvalidValue;
-    o = tc_out(rows, MLP_OUT, MLP_H, net.err);
+    // the output product, with the prior's 192 columns when there is one
+    o = tc_out(rows, MLP_OUT, pr ? MLP_K3 : MLP_H, net.err);
     o.bias = net.w + L.b3;
+    o.bias2 = pr ? prior->cb : nullptr;
     o.C = Z;
     o.ldc = MLP_OUT;
-    if (!tc_gemm(b.h2b, MLP_H, net.wt + W.w3t, MLP_H, o, st)) return cudaErrorInvalidValue;
-    if (prior && prior->cs)
-        gemm<float, float, false, true>(rows, MLP_OUT, net.d, X, net.d, prior->cs, prior->ld, Z,
-                                        MLP_OUT, prior->cb, false, true, st);
+    if (!tc_gemm(b.h2b, MLP_K3, net.wt + W.w3t, MLP_K3, o, st)) return cudaErrorInvalidValue;
     return cudaGetLastError();
 }
 
@@ -676,9 +645,16 @@ void mlp_adam(MlpView& net, float* m, float* v, const float* grad, int step, flo
 
 void mlp_sync_bf16(MlpView& net, cudaStream_t st) { refresh_wt(net, st); }
 
+void mlp_set_prior(MlpView& net, const MlpPrior& prior, cudaStream_t st) {
+    const WtLayout W = wt_layout();
+    k_prior_cols<<<unsigned((size_t(MLP_OUT) * 64 + 255) / 256), 256, 0, st>>>(
+        prior.cs, prior.ld, net.d, net.wt + W.w3t, MLP_K3);
+    count_launch();
+}
+
 void mlp_topp(const float* Z, int rows, int P, const uint32_t* skip, uint32_t* out,
               cudaStream_t st) {
-    k_topp<<<(rows + 7) / 8, 256, 0, st>>>(Z, rows, MLP_OUT, P, skip, out);
+    k_topp<<<(rows + 7) / 8, 256, 0, st>>>(Z, rows, P, skip, out);
     count_launch();
 }
 

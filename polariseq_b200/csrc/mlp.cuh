@@ -10,6 +10,7 @@ namespace pq {
 
 constexpr int MLP_H = 256;     // hidden width
 constexpr int MLP_OUT = 1024;  // bucket logits
+constexpr int MLP_K3 = MLP_H + 192;  // the output product's K with the prior's columns
 
 // Offsets (in parameters) of W1 [d x H], b1 [H], W2 [H x H], b2, W3 [H x OUT], b3.
 struct MlpLayout {
@@ -21,8 +22,9 @@ size_t mlp_scratch_floats();
 
 // FP32 master parameters `w`; `wt` (mlp_wt_elems) holds the BF16 copies the
 // tensor-core products read (mlp_sync_bf16 / mlp_adam refresh them): W1^T
-// [256 x 64], W2^T, W3^T [1024 x 256], W2 and W3 row-major; `err` (device
-// int) receives 2 if a bounded wait of a product gave up.
+// [256 x 64], W2^T, W3^T [1024 x MLP_K3: 256 weights + the prior's 192
+// columns], W2 and W3 row-major; `err` (device int) receives 2 if a bounded
+// wait of a product gave up.
 struct MlpView {
     int d;
     float* w;
@@ -69,6 +71,9 @@ cudaError_t mlp_backward(const MlpView& net, int rows, float* H1, float* H2, flo
 void mlp_adam(MlpView& net, float* m, float* v, const float* grad, int step, float lr,
               cudaStream_t st);
 void mlp_sync_bf16(MlpView& net, cudaStream_t st);
+// Writes the prior's columns of the output product's BF16 weights once (they
+// survive the Adam steps' refreshes); a forward pass given the prior uses them.
+void mlp_set_prior(MlpView& net, const MlpPrior& prior, cudaStream_t st);
 // The P largest logits of each row, skipping skip[r] (may be null).
 void mlp_topp(const float* Z, int rows, int P, const uint32_t* skip, uint32_t* out,
               cudaStream_t st);
