@@ -126,8 +126,9 @@ struct Probe {
 }  // namespace
 
 namespace pqh {
-float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp) {
-    cudaStream_t st = c->stream;
+float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp,
+                      cudaStream_t st) {
+    if (!st) st = c->stream;
     float* X = c->get<float>("X", size_t(n) * dp);
     const size_t bytes = size_t(n) * d * sizeof(float);
     if (dp == d) {

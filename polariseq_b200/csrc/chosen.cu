@@ -34,6 +34,25 @@ namespace {
 
 constexpr float FP32_BOUND = 1e-5f;  // relative band of the FP64 boundary step
 
+// Rows j * s (j < ns) of the padded rows: the k-means sample.
+__global__ void k_stride_rows(const float* __restrict__ X, int dp, uint64_t s, uint32_t ns,
+                              float* __restrict__ out) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(ns) * dp) return;
+    const uint32_t j = uint32_t(t / dp), c = uint32_t(t - size_t(j) * dp);
+    out[t] = X[uint64_t(j) * s * dp + c];
+}
+
+// n rows of d columns -> padded rows of dp (zeros past d).
+__global__ void k_pad_cols(const float* __restrict__ src, uint32_t n, int d, int dp,
+                           float* __restrict__ dst) {
+    const size_t t = size_t(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (t >= size_t(n) * dp) return;
+    const size_t i = t / dp;
+    const int j = int(t - i * dp);
+    dst[t] = j < d ? src[i * d + j] : 0.0f;
+}
+
 // Evenly strided sample of the padded rows.
 __global__ void k_sample_rows(const float* __restrict__ X, int dp, uint32_t n, uint32_t ns,
                               float* __restrict__ out) {
@@ -887,7 +906,19 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     tot.start();
     const unsigned long long launches0 = g_launches;
 
-    float* X = load_embedding(c, data, data_on_host, n, d, dp);
+    // host data: the k-means sample (a strided set of rows) is copied first
+    // and the whole embedding follows on the second stream while k-means
+    // runs; the first use of all rows waits for it
+    EventSet xev(2);
+    float* X = nullptr;
+    if (data_on_host) {
+        ck(cudaEventRecord(xev.ev[0], st), "event");
+        ck(cudaStreamWaitEvent(c->stream2, xev.ev[0], 0), "event");
+        X = load_embedding(c, data, true, n, d, dp, c->stream2);
+        ck(cudaEventRecord(xev.ev[1], c->stream2), "event");
+    } else {
+        X = load_embedding(c, data, false, n, d, dp);
+    }
 
     // ── 1. buckets ──
     tm.start();
@@ -902,9 +933,14 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const uint32_t C = learned ? 1024u
                        : o.buckets > 0 ? std::min<uint32_t>(uint32_t(o.buckets), n)
                                        : std::max<uint32_t>(1, uint32_t(std::llround(double(n) / 4096.0)));
-    const uint32_t P_auto = nnd ? 12u : learned ? 6u : 14u;
+    // probes: 14 (16 from 6M cells, where the buckets are closer together)
+    const uint32_t P_auto = nnd ? 12u : learned ? 6u : (n >= 6000000u ? 16u : 14u);
     const int P = int(std::min<uint32_t>(o.probes > 0 ? uint32_t(o.probes) : P_auto, std::min(C, 16u)));
-    const uint32_t ns = std::min<uint32_t>(n, std::max<uint32_t>(65536, 128 * C));
+    // the k-means sample: every s-th row, ns of them (all rows up to twice the
+    // target size, so that the sample always spans the embedding)
+    const uint32_t ns_target = std::max<uint32_t>(65536, 128 * C);
+    const uint64_t s_stride = n <= 2ull * ns_target ? 1 : n / ns_target;
+    const uint32_t ns = s_stride == 1 ? n : ns_target;
     if (d > 62) throw DeviceError{"the tensor-core form supports n_dim <= 62"};
     if (uint64_t(C) * C * 2 >= 0xFFFFFFFFull)
         throw DeviceError{"the tensor-core form supports n_obs below 190M"};
@@ -918,7 +954,16 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     ck(cudaMemsetAsync(zeros, 0, size_t(std::max<uint32_t>(C, n)) * 4, st), "zeros");
     uint32_t* noself = c->get<uint32_t>("noself", n);
     ck(cudaMemsetAsync(noself, 0xFF, size_t(n) * 4, st), "noself");
-    k_sample_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, n, ns, xs); count_launch();
+    if (data_on_host) {
+        float* xraw = c->get<float>("km_sample_raw", size_t(ns) * d);
+        ck(cudaMemcpy2DAsync(xraw, size_t(d) * 4, data, size_t(s_stride) * d * 4, size_t(d) * 4, ns,
+                             cudaMemcpyHostToDevice, st),
+           "copy sample");
+        k_pad_cols<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(xraw, ns, d, dp, xs); count_launch();
+    } else {
+        k_stride_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, s_stride, ns, xs);
+        count_launch();
+    }
     // the sample's mean: the BF16 centre of the centroid search
     float* mean = c->get<float>("mean", dp);
     k_col_mean<<<dp, 256, 0, st>>>(xs, ns, dp, mean); count_launch();
@@ -1004,6 +1049,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     }
     k_to_bf16<<<cvt_blocks(C), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
     // every cell's P nearest centroids, ascending; the first is its primary bucket
+    if (data_on_host) ck(cudaStreamWaitEvent(st, xev.ev[1], 0), "event");
     __nv_bfloat16* qa = c->get<__nv_bfloat16>("assign_q", size_t(n) * 64);
     float* qan = c->get<float>("assign_qn", n);
     k_to_bf16<<<cvt_blocks(n), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan); count_launch();
@@ -1334,9 +1380,10 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     const int R = std::min(P * Sout, std::min(64, std::max(fp8 ? 4 * k : 2 * k, k + 1)));
     if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
     ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
-    // auto: no polish round for BF16; one for E4M3, whose shortlist misses more
+    // auto: no polish round (the E4M3 shortlist with per-row scales reaches the
+    // BF16 form's recall without one)
     const uint64_t polish = nnd ? resolve(n64, o).n_iters
-                            : o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : (fp8 ? 1 : 0);
+                            : o.refine_rounds >= 0 ? uint64_t(o.refine_rounds) : 0;
     auto rerank = [&](const uint32_t* by_cell, uint32_t a, uint32_t b) {
         if (d == 50)
             k_rerank<50><<<blocks(b - a, 4), 128, 0, st>>>(X, xp, d, dp, b, k, P, Sout, Ssh, R,

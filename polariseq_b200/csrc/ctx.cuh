@@ -178,8 +178,10 @@ inline void kg_collect(pq_ctx* c) {
 }
 
 // The caller's row-major n x d f32 embedding (host or device) as padded rows
-// X[n][dp] in the context's workspace, 16-byte aligned and zero padded (api.cu).
-float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp);
+// X[n][dp] in the context's workspace, 16-byte aligned and zero padded, on
+// stream st (null: the context's stream) (api.cu).
+float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp,
+                      cudaStream_t st = nullptr);
 
 // NN-Descent rounds on heaps in place (api.cu).
 int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m, uint64_t seed,
