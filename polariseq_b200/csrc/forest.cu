@@ -320,15 +320,20 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
         const float* xb = rows + size_t(S.sslot[ls + pb]) * dp;
         for (int j = lane; j < dp; j += 32) nv[j] = j < d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
         __syncwarp();
-        // margins of the positions this lane owns (lane + 32*i); the dot
-        // products and the offset chain are independent and overlap
-        float dots[SCAP / 32];
-#pragma unroll 1
-        for (int i = 0; i < SCAP / 32; ++i) {
-            const uint32_t p = lane + 32 * i;
-            dots[i] = p < ln ? dot_exact_t<D>(nv, rows + size_t(S.sslot[ls + p]) * dp, d) : 0.f;
-        }
+        // margins of the positions this lane owns (lane + 32*i): the offset's
+        // sequential sum and the dot products are independent chains, issued
+        // together (the dots stay in registers; groups past the node's size
+        // are skipped by the whole warp)
         const float off = hyper_offset_t<D>(xa, xb, d);
+        float dots[SCAP / 32];
+#pragma unroll
+        for (int i = 0; i < SCAP / 32; ++i) {
+            dots[i] = 0.f;
+            if (32u * i < ln) {
+                const uint32_t p = lane + 32 * i;
+                if (p < ln) dots[i] = dot_exact_t<D>(nv, rows + size_t(S.sslot[ls + p]) * dp, d);
+            }
+        }
         unsigned any_tie = 0;
 #pragma unroll
         for (int i = 0; i < SCAP / 32; ++i) {

@@ -119,7 +119,7 @@ def test_bf16_form_small_inputs_are_exact():
 
 def test_fp8_form_recall_and_exact_distances():
     """E4M3 tiles (every query and candidate row with its own scale) with the
-    exact FP32 re-rank, no polish round: recall against FP64 and
+    exact FP32 re-rank and its default polish round (below 2^20 cells): recall against FP64 and
     exact returned distances."""
     n, k = 120_000, 15
     x = synth.mixture_lognormal(n, 50, 30, seed=11)
