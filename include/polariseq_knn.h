@@ -74,8 +74,8 @@ typedef struct pq_nnd_opts {
     int32_t mode;            /* PQ_MODE_* */
     int32_t init;            /* PQ_INIT_* */
     /* Tensor-core forms only (ignored by PQ_MODE_PLAIN): */
-    int32_t probes;          /* buckets each cell searches (<= 16); 0 -> min(14, buckets)
-                              * (16 from 6M cells), 6 with PQ_INIT_LEARNED (1024 buckets,
+    int32_t probes;          /* buckets each cell searches (<= 16); 0 -> min(13, buckets)
+                              * (14 for k > 15, 16 from 6M cells), 6 with PQ_INIT_LEARNED (1024 buckets,
                               * own bucket + MLP), 12 for the learned-init NN-Descent */
     int32_t refine_rounds;   /* NN-Descent rounds after the shortlist; -1 -> auto (none; one
                               * for FP8 below 2^20 cells) */

@@ -469,6 +469,19 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
                      "[nndescent]   largest subtree cycles: draw %llu margin %llu partition %llu "
                      "staged %llu total %llu\n",
                      h[6], h[7], h[8], h[9], h[10]);
+        std::fprintf(stderr,
+                     "[nndescent]   largest subtree: global nodes %llu, CTA-staged nodes %llu, "
+                     "staged subtrees %llu (nodes %llu, warp cycles %llu); CTA-staged subtrees "
+                     "%llu (nodes %llu) in all\n",
+                     h[SEQ_T_R0_GNODES], h[SEQ_T_R0_MNODES], h[SEQ_T_R0_STAGED],
+                     h[SEQ_T_R0_SNODES], h[SEQ_T_R0_CYC_WARP], h[SEQ_T_MID_TREES],
+                     h[SEQ_T_MID_NODES]);
+        std::fprintf(stderr,
+                     "[nndescent]   largest subtree, warp splits: leaf pops %llu draws %llu "
+                     "margins %llu partition %llu; CTA splits: staging %llu draws %llu margins "
+                     "%llu partition %llu cycles\n",
+                     h[SEQ_T_W_LEAF], h[SEQ_T_W_DRAW], h[SEQ_T_W_MARGIN], h[SEQ_T_W_PART],
+                     h[SEQ_T_M_STAGE], h[SEQ_T_M_DRAW], h[SEQ_T_M_MARGIN], h[SEQ_T_M_PART]);
     }
     if (herr) throw DeviceError{"forest: a subtree exceeded the depth-first stack"};
 
@@ -601,7 +614,13 @@ uint64_t build_learned_nnd(pq_ctx* c, const float* data, bool data_on_host, uint
     const uint32_t Q = 1024;
     uint64_t nnz = build_chosen(c, data, data_on_host, n64, d64, o, d_indptr, d_indices, d_dists);
     const float* X = c->get<float>("X", size_t(n) * dp);  // the padded rows of this build
+    Timer tm(st);
+    tm.start();
     const double rl = pq::sampled_recall(c, X, d, dp, n, k, d_indptr, d_indices, Q, o.seed);
+    const double ms_check = tm.stop();
+    if (std::getenv("POLARISEQ_TRACE"))
+        std::fprintf(stderr, "[learned] sampled recall %.4f (%u queries): %.2f ms; build %.2f ms\n",
+                     rl, Q, ms_check, c->stats.ms_total);
     pq_nnd_stats learned = c->stats;
     learned.est_recall = learned.est_recall_learned = rl;
     learned.learned_rounds = learned.rounds_run;
@@ -771,6 +790,7 @@ int pq_ctx_create(int device, pq_ctx** out) {
 
 void pq_ctx_destroy(pq_ctx* c) {
     if (!c) return;
+    if (c->sub) pq_ctx_destroy(c->sub);
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     for (auto& kv : c->bufs)

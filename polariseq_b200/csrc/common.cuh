@@ -58,6 +58,24 @@ __device__ __forceinline__ uint32_t mod_u64_u32(uint64_t x, uint32_t n) {
     return r;
 }
 
+// x mod n with a reciprocal rn = RN(1 / n) shared by several draws of one
+// n: three steps of 32, 16 and 16 bits, each partial dividend t < 2^48 so
+// that trunc(t * rn) is within one of floor(t / n) (relative error below
+// 2^-51); one correction either way makes each remainder exact.
+__device__ __forceinline__ uint32_t mod_u64_u32_r(uint64_t x, uint32_t n, double rn) {
+    uint64_t r = 0;
+#pragma unroll
+    for (int step = 2; step >= 0; --step) {
+        const uint64_t t = step == 2 ? (x >> 32) : ((r << 16) | ((x >> (16 * step)) & 0xFFFFull));
+        const int64_t q = int64_t(double(t) * rn);
+        int64_t rem = int64_t(t) - q * int64_t(n);
+        if (rem < 0) rem += n;
+        if (rem >= int64_t(n)) rem -= n;
+        r = uint64_t(rem);
+    }
+    return uint32_t(r);
+}
+
 // Rng (nndescent.rs:101-112): the state is replaced by splitmix(state).
 struct Rng {
     uint64_t s;

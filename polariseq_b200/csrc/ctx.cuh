@@ -115,6 +115,9 @@ struct pq_ctx {
     };
     std::vector<KGRec> kg_pending;
     std::map<uint64_t, int> batch_shape;  // autotuned tile shape per (dims, heap size)
+    // the learned-init subsample's plain graph is built on this context, kept
+    // from build to build (its workspace is not reallocated each time)
+    pq_ctx* sub = nullptr;
 
     template <class T>
     T* get(const std::string& name, size_t count) {

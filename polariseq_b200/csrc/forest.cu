@@ -263,29 +263,68 @@ __global__ void k_degenerate(ForestArgs a, PNode* nodes, uint32_t nn) {
 // with ballots, without block barriers.  The largest subtrees (their
 // depth-first chains are the critical path) run with NT = 512.
 constexpr int SCAP = 128;   // staged capacity (points): 4 per lane of warp 0
+// A node of at most MCAP points in a 512-thread CTA is staged with its whole
+// subtree (ids and rows in shared memory): its splits of more than SCAP
+// points take one point per thread, the smaller ones go to warp 0.
+constexpr int MCAP = 512;
 
 struct SeqShared {
     uint32_t stS[STK], stN[STK];
     uint16_t stD[STK];
     uint32_t lS[STK], lN[STK];
     uint16_t lD[STK];
-    uint32_t sid[SCAP], sslot[SCAP], sid2[SCAP], sslot2[SCAP];
-    uint8_t code[SCAP];
-    uint32_t tabA[SCAP], tabB[SCAP];
+    uint32_t mS[STK], mN[STK];
+    uint16_t mD[STK];
+    uint32_t sid[MCAP], sslot[MCAP], sid2[MCAP], sslot2[MCAP];
+    uint8_t code[MCAP];
+    uint32_t tabA[MCAP], tabB[MCAP];
     uint32_t ws[32];
     uint64_t rng;
+    float off;
     uint32_t cntL, sc;
     int sp, anytie;
 };
 
+// 16-byte asynchronous global -> shared copies (both addresses 16-byte
+// aligned), bypassing L1.
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const uint32_t a = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(a), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;" ::: "memory");
+}
+
 // Draws of random_hyperplane (nndescent.rs:369-375) as positions: ids within
 // a node are distinct, so the reference's `b == a` is a position test.
+// x mod n for n < 2^16 in 32-bit arithmetic: (hi * 2^32 + lo) mod n =
+// ((hi mod n) * t32 + lo mod n) mod n with t32 = 2^32 mod n (every product and
+// sum stays below n^2 + n < 2^32).
+__device__ __forceinline__ uint32_t mod_u64_small(uint64_t x, uint32_t n, uint32_t t32) {
+    const uint32_t hi = uint32_t(x >> 32) % n, lo = uint32_t(x) % n;
+    return (hi * t32 + lo) % n;
+}
+
+// The draws of one node share their divisor's constants (below(n) is
+// next_u64() % n): 32-bit steps for n < 2^16 (staged nodes), a shared
+// reciprocal above.
 __device__ __forceinline__ void draw_pair(Rng& r, uint32_t n, uint32_t& pa, uint32_t& pb) {
-    pa = uint32_t(r.below(n));
-    pb = uint32_t(r.below(n));
     int tries = 0;
+    if (n < 65536u) {
+        const uint32_t t32 = (0xFFFFFFFFu % n + 1u) % n;
+        pa = mod_u64_small(r.next_u64(), n, t32);
+        pb = mod_u64_small(r.next_u64(), n, t32);
+        while (pb == pa && tries < 8) {
+            pb = mod_u64_small(r.next_u64(), n, t32);
+            ++tries;
+        }
+        return;
+    }
+    const double rn = __drcp_rn(double(n));
+    pa = mod_u64_u32_r(r.next_u64(), n, rn);
+    pb = mod_u64_u32_r(r.next_u64(), n, rn);
     while (pb == pa && tries < 8) {
-        pb = uint32_t(r.below(n));
+        pb = mod_u64_u32_r(r.next_u64(), n, rn);
         ++tries;
     }
 }
@@ -293,9 +332,20 @@ __device__ __forceinline__ void draw_pair(Rng& r, uint32_t n, uint32_t& pa, uint
 // Warp 0 finishes a staged subtree: local positions [0, n0) of the staged
 // ids/slots, rows in `rows` (slot-indexed), normal in `nv`.
 template <int D>
-__device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, float* nv,
-                             uint32_t st, uint32_t n0, uint32_t dep0, Rng& rng, uint8_t* leaf) {
+__device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* sid, uint32_t* sslot,
+                                 float* rows, float* nv, uint32_t st, uint32_t n0, uint32_t dep0,
+                                 Rng& rng, uint8_t* leaf, bool tb0 = false) {
     const int lane = threadIdx.x & 31;
+    uint32_t nodes = 0;
+    unsigned long long* tr = a.trace;
+    long long tc = tb0 ? clock64() : 0;
+    auto phase = [&](int slot) {
+        if (tb0) {
+            const long long t1 = clock64();
+            tr[slot] += t1 - tc;
+            tc = t1;
+        }
+    };
     const int d = a.d, dp = a.dp;
     const unsigned lt = (1u << lane) - 1u;
     int lsp = 1;
@@ -311,13 +361,16 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
         lsp -= 1;
         if (ln <= a.leaf_size || ld > 100) {
             if (lane == 0) leaf[st + ls] = 1;
+            phase(SEQ_T_W_LEAF);
             continue;
         }
         if (a.trace && lane == 0) atomicAdd(&a.trace[SEQ_T_STAGED_NODES], 1ull);
+        ++nodes;
         uint32_t pa, pb;
         draw_pair(rng, ln, pa, pb);
-        const float* xa = rows + size_t(S.sslot[ls + pa]) * dp;
-        const float* xb = rows + size_t(S.sslot[ls + pb]) * dp;
+        phase(SEQ_T_W_DRAW);
+        const float* xa = rows + size_t(sslot[ls + pa]) * dp;
+        const float* xb = rows + size_t(sslot[ls + pb]) * dp;
         for (int j = lane; j < dp; j += 32) nv[j] = j < d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
         __syncwarp();
         // margins of the positions this lane owns (lane + 32*i): the offset's
@@ -331,25 +384,32 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
             dots[i] = 0.f;
             if (32u * i < ln) {
                 const uint32_t p = lane + 32 * i;
-                if (p < ln) dots[i] = dot_exact_t<D>(nv, rows + size_t(S.sslot[ls + p]) * dp, d);
+                if (p < ln) dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
             }
         }
+        // sides in registers; through shared memory only when a tie draws
         unsigned any_tie = 0;
+        uint8_t code[SCAP / 32];
 #pragma unroll
         for (int i = 0; i < SCAP / 32; ++i) {
             const uint32_t p = lane + 32 * i;
+            code[i] = 0;
             if (p < ln) {
                 const float m = __fadd_rn(dots[i], off);
-                const uint8_t c = fabsf(m) < 1e-8f ? 2 : (m > 0.0f ? 1 : 0);
-                S.code[p] = c;
-                any_tie |= c == 2;
+                code[i] = fabsf(m) < 1e-8f ? 2 : (m > 0.0f ? 1 : 0);
+                any_tie |= code[i] == 2;
             }
         }
-        __syncwarp();
         if (__any_sync(0xFFFFFFFFu, any_tie)) {
             // ties draw from the Rng in position order (every lane replays the
             // same draws so that all copies of the Rng stay equal)
             if (a.trace && lane == 0) atomicAdd(&a.trace[SEQ_T_TIES], 1ull);
+#pragma unroll
+            for (int i = 0; i < SCAP / 32; ++i) {
+                const uint32_t p = lane + 32 * i;
+                if (p < ln) S.code[p] = code[i];
+            }
+            __syncwarp();
             for (uint32_t p = 0; p < ln; ++p)
                 if (S.code[p] == 2) {
                     uint8_t v = (rng.next_u64() & 1ull) == 0 ? 1 : 0;
@@ -357,13 +417,19 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
                     if (lane == 0) S.code[p] = v;
                     __syncwarp();
                 }
+#pragma unroll
+            for (int i = 0; i < SCAP / 32; ++i) {
+                const uint32_t p = lane + 32 * i;
+                if (p < ln) code[i] = S.code[p];
+            }
         }
+        phase(SEQ_T_W_MARGIN);
         unsigned mask[SCAP / 32];
         uint32_t nL = 0;
 #pragma unroll
         for (int i = 0; i < SCAP / 32; ++i) {
             const uint32_t p = lane + 32 * i;
-            mask[i] = __ballot_sync(0xFFFFFFFFu, p < ln && S.code[p] == 1);
+            mask[i] = __ballot_sync(0xFFFFFFFFu, p < ln && code[i] == 1);
             nL += __popc(mask[i]);
         }
         uint32_t c = 0;
@@ -404,15 +470,15 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
                 } else {
                     dst = (c == 0 ? ln : S.tabB[c - 1]) - 1;
                 }
-                S.sid2[dst] = S.sid[ls + p];
-                S.sslot2[dst] = S.sslot[ls + p];
+                S.sid2[dst] = sid[ls + p];
+                S.sslot2[dst] = sslot[ls + p];
             }
             pre += __popc(mask[i]);
         }
         __syncwarp();
         for (uint32_t p = lane; p < ln; p += 32) {
-            S.sid[ls + p] = S.sid2[p];
-            S.sslot[ls + p] = S.sslot2[p];
+            sid[ls + p] = S.sid2[p];
+            sslot[ls + p] = S.sslot2[p];
         }
         __syncwarp();
         uint32_t split = nL;
@@ -421,11 +487,11 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
             for (uint32_t i = ln - 1; i >= 1; --i) {
                 uint32_t j = uint32_t(rng.below(uint64_t(i) + 1));
                 if (lane == 0) {
-                    uint32_t t1 = S.sid[ls + i], t2 = S.sslot[ls + i];
-                    S.sid[ls + i] = S.sid[ls + j];
-                    S.sslot[ls + i] = S.sslot[ls + j];
-                    S.sid[ls + j] = t1;
-                    S.sslot[ls + j] = t2;
+                    uint32_t t1 = sid[ls + i], t2 = sslot[ls + i];
+                    sid[ls + i] = sid[ls + j];
+                    sslot[ls + i] = sslot[ls + j];
+                    sid[ls + j] = t1;
+                    sslot[ls + j] = t2;
                 }
                 __syncwarp();
             }
@@ -433,7 +499,7 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
         }
         if (lsp + 2 > STK) {
             if (lane == 0) atomicExch(a.err, 1);
-            return;
+            return nodes;
         }
         if (lane == 0) {
             S.lS[lsp] = ls + split;
@@ -445,7 +511,9 @@ __device__ void warp_subtree(const ForestArgs& a, SeqShared& S, float* rows, flo
         }
         lsp += 2;
         __syncwarp();
+        phase(SEQ_T_W_PART);
     }
+    return nodes;
 }
 
 // One node split in global mode (random_hyperplane, margins with tie draws
@@ -490,26 +558,29 @@ __device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids,
     }
     uint32_t cnt = 0;
     bool tie = false;
-    constexpr int U = NT >= 512 ? 2 : 4;  // rows in flight per thread
-    for (uint32_t p0 = tid; p0 < sz; p0 += U * NT) {
-        uint32_t id[U];
+    // margins: each thread reads its rows directly, U in flight
+    {
+        constexpr int U = NT >= 512 ? 2 : 4;  // rows in flight per thread
+        for (uint32_t p0 = tid; p0 < sz; p0 += U * NT) {
+            uint32_t id[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t p = p0 + u * NT;
-            id[u] = ids[st + (p < sz ? p : p0)];
-        }
-        float m[U];
+            for (int u = 0; u < U; ++u) {
+                const uint32_t p = p0 + u * NT;
+                id[u] = ids[st + (p < sz ? p : p0)];
+            }
+            float m[U];
 #pragma unroll
-        for (int u = 0; u < U; ++u)
-            m[u] = __fadd_rn(dot_exact_t<D>(nv, a.X + size_t(id[u]) * dp, d), off);
+            for (int u = 0; u < U; ++u)
+                m[u] = __fadd_rn(dot_exact_t<D>(nv, a.X + size_t(id[u]) * dp, d), off);
 #pragma unroll
-        for (int u = 0; u < U; ++u) {
-            const uint32_t p = p0 + u * NT;
-            if (p < sz) {
-                const uint8_t c = fabsf(m[u]) < 1e-8f ? 2 : (m[u] > 0.0f ? 1 : 0);
-                side[st + p] = c;
-                tie |= c == 2;
-                cnt += c == 1;
+            for (int u = 0; u < U; ++u) {
+                const uint32_t p = p0 + u * NT;
+                if (p < sz) {
+                    const uint8_t c = fabsf(m[u]) < 1e-8f ? 2 : (m[u] > 0.0f ? 1 : 0);
+                    side[st + p] = c;
+                    tie |= c == 2;
+                    cnt += c == 1;
+                }
             }
         }
     }
@@ -625,13 +696,215 @@ __device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids,
     return split;
 }
 
+// One split of a staged node of m <= NT points (positions [0, m) of
+// sid/sslot, rows in shared memory), one point per thread: the same draws,
+// margins, tie draws, closed-form partition and random split as the
+// global-mode split.  Returns the split point.
+template <int NT, int D>
+__device__ uint32_t cta_split(const ForestArgs& a, SeqShared& S, uint32_t* sid, uint32_t* sslot,
+                              uint32_t m, Rng& rng, float* rows, float* nv, bool tb0) {
+    const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
+    const int d = a.d, dp = a.dp;
+    const uint32_t p = uint32_t(tid);
+    unsigned long long* tr = a.trace;
+    long long tc = tb0 ? clock64() : 0;
+    auto phase = [&](int slot) {
+        if (tb0) {
+            const long long t1 = clock64();
+            tr[slot] += t1 - tc;
+            tc = t1;
+        }
+    };
+    uint32_t pa, pb;
+    draw_pair(rng, m, pa, pb);
+    phase(SEQ_T_M_DRAW);
+    const float* xa = rows + size_t(sslot[pa]) * dp;
+    const float* xb = rows + size_t(sslot[pb]) * dp;
+    for (int j = tid; j < dp; j += NT) nv[j] = j < d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
+    __syncthreads();
+    // the offset's sequential sum in warp 0 alone (beside its dot products)
+    float dt = 0.0f;
+    if (p < m) dt = dot_exact_t<D>(nv, rows + size_t(sslot[p]) * dp, d);
+    if (w == 0) {
+        const float o = hyper_offset_t<D>(xa, xb, d);
+        if (lane == 0) S.off = o;
+    }
+    __syncthreads();
+    uint8_t c = 0;
+    if (p < m) {
+        const float mg = __fadd_rn(dt, S.off);
+        c = fabsf(mg) < 1e-8f ? 2 : (mg > 0.0f ? 1 : 0);
+        S.code[p] = c;
+    }
+    if (__syncthreads_or(c == 2)) {
+        // ties draw from the Rng in position order (every thread replays the
+        // same draws; thread 0 writes the sides)
+        if (a.trace && tid == 0) atomicAdd(&a.trace[SEQ_T_TIES], 1ull);
+        for (uint32_t q = 0; q < m; ++q)
+            if (S.code[q] == 2) {
+                const uint8_t v = (rng.next_u64() & 1ull) == 0 ? 1 : 0;
+                __syncthreads();
+                if (tid == 0) S.code[q] = v;
+                __syncthreads();
+            }
+        c = p < m ? S.code[p] : 0;
+    }
+    phase(SEQ_T_M_MARGIN);
+    // left points before each position: warp ballots, then a scan of the
+    // warp counts
+    const bool isL = p < m && c == 1;
+    const unsigned bal = __ballot_sync(0xFFFFFFFFu, isL);
+    if (lane == 0) S.ws[w] = __popc(bal);
+    __syncthreads();
+    if (w == 0) {
+        uint32_t v = lane < NT / 32 ? S.ws[lane] : 0u;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, v, o);
+            if (lane >= o) v += y;
+        }
+        if (lane < NT / 32) S.ws[lane] = v;  // inclusive
+    }
+    __syncthreads();
+    const uint32_t nL = S.ws[NT / 32 - 1];
+    const uint32_t lp = (w > 0 ? S.ws[w - 1] : 0u) + __popc(bal & ((1u << lane) - 1u));
+    if (p < m) {
+        if (isL) {
+            if (p >= nL) S.tabB[(nL - lp) - 1] = p;
+        } else if (p < nL) {
+            S.tabA[p - lp] = p;
+        }
+        if (p == nL) S.sc = nL - lp;  // right points in [0, nL)
+    }
+    __syncthreads();
+    if (p < m) {
+        uint32_t dst;
+        if (isL) {
+            dst = p < nL ? p : S.tabA[(nL - lp) - 1];
+        } else if (p < nL) {
+            const uint32_t rr = p - lp + 1;
+            dst = (rr == 1 ? m : S.tabB[rr - 2]) - 1;
+        } else if (p > nL) {
+            dst = p - 1;
+        } else {
+            const uint32_t cr = S.sc;
+            dst = (cr == 0 ? m : S.tabB[cr - 1]) - 1;
+        }
+        S.sid2[dst] = sid[p];
+        S.sslot2[dst] = sslot[p];
+    }
+    __syncthreads();
+    if (p < m) {
+        sid[p] = S.sid2[p];
+        sslot[p] = S.sslot2[p];
+    }
+    __syncthreads();
+    uint32_t split = nL;
+    if (nL == 0 || nL == m) {
+        if (a.trace && tid == 0) atomicAdd(&a.trace[SEQ_T_DEGENERATE], 1ull);
+        for (uint32_t i = m - 1; i >= 1; --i) {
+            const uint32_t j = uint32_t(rng.below(uint64_t(i) + 1));
+            if (tid == 0) {
+                const uint32_t t1 = sid[i], t2 = sslot[i];
+                sid[i] = sid[j];
+                sslot[i] = sslot[j];
+                sid[j] = t1;
+                sslot[j] = t2;
+            }
+            __syncthreads();
+        }
+        split = m / 2;
+    }
+    phase(SEQ_T_M_PART);
+    return split;
+}
+
+// A staged subtree of at most MCAP points (NT = 512): ids[0, sz) and their
+// rows are staged once; its nodes of more than SCAP points are split by the
+// whole CTA (cta_split), the smaller ones finished by warp 0; the ids come
+// back in tree order.  `gpos` is its first position in the tree.
+template <int NT, int D>
+__device__ void mid_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t gpos,
+                            uint32_t sz, uint32_t dep, Rng& rng, float* rows, float* nv,
+                            uint8_t* leaf, bool tb0) {
+    const int tid = threadIdx.x;
+    const int dp = a.dp, q4 = dp / 4;
+    for (uint32_t p = tid; p < sz; p += NT) {
+        S.sid[p] = ids[p];
+        S.sslot[p] = p;
+    }
+    __syncthreads();
+    for (uint32_t t = tid; t < sz * q4; t += NT) {
+        const uint32_t r = t / q4, c4 = t - r * q4;
+        cp_async16(rows + size_t(r) * dp + 4 * c4, a.X + size_t(S.sid[r]) * dp + 4 * c4);
+    }
+    cp_async_wait_all();
+    const long long cst = tb0 ? clock64() : 0;
+    if (tid == 0) {
+        S.mS[0] = 0;
+        S.mN[0] = sz;
+        S.mD[0] = uint16_t(dep);
+    }
+    int msp = 1;  // every thread tracks the same stack depth
+    __syncthreads();
+    if (tb0) a.trace[SEQ_T_M_STAGE] += clock64() - cst;
+    while (msp > 0) {
+        const uint32_t ls = S.mS[msp - 1], ln = S.mN[msp - 1], ld = S.mD[msp - 1];
+        __syncthreads();  // the top is read before it is overwritten
+        msp -= 1;
+        if (ln <= a.leaf_size || ld > 100) {
+            if (tid == 0) leaf[gpos + ls] = 1;
+            continue;
+        }
+        if (ln <= uint32_t(SCAP)) {
+            if (tid < 32) {
+                const long long c0 = tb0 ? clock64() : 0;
+                const uint32_t nodes = warp_subtree<D>(a, S, S.sid + ls, S.sslot + ls, rows, nv,
+                                                       gpos + ls, ln, ld, rng, leaf, tb0);
+                if (tid == 0) S.rng = rng.s;
+                if (tb0) {
+                    a.trace[SEQ_T_R0_CYC_WARP] += clock64() - c0;
+                    a.trace[SEQ_T_R0_SNODES] += nodes;
+                    a.trace[SEQ_T_R0_STAGED] += 1;
+                }
+            }
+            __syncthreads();
+            rng.s = S.rng;  // the other warps adopt warp 0's Rng state
+            continue;
+        }
+        if (a.trace && tid == 0) {
+            atomicAdd(&a.trace[SEQ_T_MID_NODES], 1ull);
+            if (tb0) a.trace[SEQ_T_R0_MNODES] += 1;
+        }
+        const uint32_t split =
+            cta_split<NT, D>(a, S, S.sid + ls, S.sslot + ls, ln, rng, rows, nv, tb0);
+        if (msp + 2 > STK) {
+            if (tid == 0) atomicExch(a.err, 1);
+            break;
+        }
+        if (tid == 0) {
+            S.mS[msp] = ls + split;  // right, popped after the whole left subtree
+            S.mN[msp] = ln - split;
+            S.mD[msp] = uint16_t(ld + 1);
+            S.mS[msp + 1] = ls;
+            S.mN[msp + 1] = split;
+            S.mD[msp + 1] = uint16_t(ld + 1);
+        }
+        msp += 2;
+        __syncthreads();
+    }
+    for (uint32_t p = tid; p < sz; p += NT) ids[p] = S.sid[p];
+    __syncthreads();
+    if (a.trace && tid == 0) atomicAdd(&a.trace[SEQ_T_MID_TREES], 1ull);
+}
+
 // A staged subtree of at most smax points: ids[0, sz) with their rows in
 // shared memory, finished by warp 0; the ids come back in tree order.  `gpos`
 // is its first position in the tree (for the leaf flags).
 template <int NT, int D>
 __device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t gpos,
                                uint32_t sz, uint32_t dep, Rng& rng, float* rows, float* nv,
-                               uint8_t* leaf) {
+                               uint8_t* leaf, bool tb0) {
     const int tid = threadIdx.x;
     const int dp = a.dp;
     for (uint32_t p = tid; p < sz; p += NT) {
@@ -647,8 +920,15 @@ __device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids,
     }
     __syncthreads();
     if (tid < 32) {
-        warp_subtree<D>(a, S, rows, nv, gpos, sz, dep, rng, leaf);
+        const long long c0 = tb0 ? clock64() : 0;
+        const uint32_t nodes =
+            warp_subtree<D>(a, S, S.sid, S.sslot, rows, nv, gpos, sz, dep, rng, leaf, tb0);
         if (tid == 0) S.rng = rng.s;
+        if (tb0) {
+            a.trace[SEQ_T_R0_CYC_WARP] += clock64() - c0;
+            a.trace[SEQ_T_R0_SNODES] += nodes;
+            a.trace[SEQ_T_R0_STAGED] += 1;
+        }
     }
     __syncthreads();
     rng.s = S.rng;  // the other warps adopt warp 0's Rng state
@@ -658,12 +938,13 @@ __device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids,
 }
 
 template <int NT, int D>
-__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax) {
+__global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax,
+                                                int trows) {
     extern __shared__ __align__(16) float dyn[];
     __shared__ SeqShared S;
     float* nv = dyn;                 // dp
     float* xab = dyn + a.dp;         // 2 * dp: the two hyperplane rows
-    float* rows = dyn + 3 * a.dp;    // smax * dp
+    float* rows = dyn + 3 * a.dp;    // max(smax, trows) * dp: staged subtrees
     const int tid = threadIdx.x;
     const SRoot rt = roots[blockIdx.x];
     const size_t tb = size_t(rt.tree) * a.n;
@@ -693,14 +974,23 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
             __syncthreads();
             continue;
         }
+        if (NT == MCAP && trows >= MCAP && sz > uint32_t(smax) && sz <= uint32_t(MCAP)) {
+            if (tb0) tclk = clock64();
+            mid_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf, tb0);
+            if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
+            continue;
+        }
         if (sz <= uint32_t(smax)) {
             if (tb0) tclk = clock64();
-            staged_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf);
+            staged_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf, tb0);
             if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
             continue;
         }
         // ── global mode ──
-        if (tb0) tclk = clock64();
+        if (tb0) {
+            tclk = clock64();
+            tr[SEQ_T_R0_GNODES] += 1;
+        }
         const uint32_t split =
             split_node<NT, D>(a, S, ids, tmp, side, tabA, tabB, st, sz, rng, nv, xab, tb0, tclk);
         if (tid == 0) {
@@ -902,12 +1192,19 @@ void launch_degenerate(const ForestArgs& a, PNode* nodes, uint32_t nn, cudaStrea
 }
 template <int NT, int D>
 static void seqtree_launch(const ForestArgs& a, const SRoot* roots, uint32_t nr, int smax,
-                           size_t dyn, cudaStream_t st) {
+                           cudaStream_t st) {
     if (nr == 0) return;
-    if (dyn > 40 * 1024)
-        cudaFuncSetAttribute(k_seqtree<NT, D>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             int(dyn));
-    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax); count_launch();
+    // shared rows: the two hyperplane rows, the normal, and max(smax, tr) rows
+    // for staged subtrees (tr = NT rows, the CTA-staged subtrees of 512-thread
+    // CTAs, when they fit in 200 KB)
+    const size_t row = size_t(a.dp) * sizeof(float);
+    const size_t fit = (200 * 1024) / row;
+    int tr = int(std::min<size_t>(NT, fit > 3 ? fit - 3 : 0));
+    if (tr < 32) tr = 0;
+    const size_t dyn = row * (3 + size_t(std::max(smax, tr)));
+    // (with the static staged arrays the total passes 48 KB well before dyn does)
+    cudaFuncSetAttribute(k_seqtree<NT, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, int(dyn));
+    k_seqtree<NT, D><<<nr, NT, dyn, st>>>(a, roots, smax, tr); count_launch();
 }
 
 void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, uint32_t nr,
@@ -917,14 +1214,13 @@ void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, ui
     size_t row = size_t(a.dp) * sizeof(float);
     int smax = int(std::min<size_t>(SCAP, (28 * 1024) / row));
     if (smax < 2) smax = 0;
-    size_t dyn = row * (3 + size_t(smax));
     // roots[0, n_big) are the largest subtrees: 512 threads each, own stream
     if (a.d == 50) {
-        seqtree_launch<512, 50>(a, roots, n_big, smax, dyn, st_big);
-        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, dyn, st);
+        seqtree_launch<512, 50>(a, roots, n_big, smax, st_big);
+        seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, st);
     } else {
-        seqtree_launch<512, 0>(a, roots, n_big, smax, dyn, st_big);
-        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, dyn, st);
+        seqtree_launch<512, 0>(a, roots, n_big, smax, st_big);
+        seqtree_launch<128, 0>(a, roots + n_big, nr - n_big, smax, st);
     }
 }
 void launch_leaf_compact(const uint8_t* leafflag_t, uint32_t n, uint32_t* leaf_start,

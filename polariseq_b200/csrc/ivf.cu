@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     float* hsall = reinterpret_cast<float*>(biall + NG * BUF * TQ);        // 2 x NG x CPG
     float* hkall = hsall + 2 * NG * CPG;                                   // 2 x NG x CPG
     __shared__ IvfBars B;
+    __shared__ unsigned long long ld_cyc;  // tracing: block 0 warp 0's TMEM load waits
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
     volatile int* abort_flag = &B.abort;
 
@@ -168,6 +169,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
         tc::mbar_init(&B.never, 1);
         tc::fence_barrier_init();
         B.abort = 0;
+        ld_cyc = 0;
         // the timeout test hook: a bounded wait that runs out before any work
         if (a.test_wait_polls && !tc::mbar_wait(&B.never, 0, a.test_wait_polls)) B.abort = 1;
     }
@@ -387,8 +389,10 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
 #pragma unroll 1
                 for (int q = 0; q < CPG / 32; ++q) {
                     uint32_t r[32];
+                    const long long cl = t0 ? clock64() : 0;
                     tc::tmem_ld32(tcol + uint32_t(q * 32), r);
                     tc::tmem_ld_wait();
+                    if (t0) ld_cyc += clock64() - cl;
                     float v[32];
                     if constexpr (F8) {
 #pragma unroll
@@ -514,6 +518,7 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
             a.trace[IVF_T_ADMITS] = admits;
             a.trace[IVF_T_WMBITS] = wmbits;
             a.trace[IVF_T_SLOW_CYC] = (unsigned long long)c_slow;
+            a.trace[IVF_T_LD_CYC] = ld_cyc;
         }
     }
     __syncthreads();

@@ -55,7 +55,7 @@ struct IvfTileArgs {
 enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT_C = 3,
        IVF_T_MMA_WAIT_T = 4, IVF_T_TMA_WAIT = 5, IVF_T_TILES = 6, IVF_T_TOTAL = 7,
        IVF_T_JOBS = 8, IVF_T_SLOW = 9, IVF_T_ADMITS = 10, IVF_T_WMBITS = 11,
-       IVF_T_SLOW_CYC = 12, IVF_TRACE_N = 16 };
+       IVF_T_SLOW_CYC = 12, IVF_T_LD_CYC = 13, IVF_TRACE_N = 16 };
 
 bool make_bf16_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t box_rows);
 // A [rows x cols] BF16 matrix with leading dimension ld (elements, a multiple

@@ -56,7 +56,22 @@ enum {
     SEQ_T_CYC_STAGED = 9,     // block 0 cycles: staged subtrees
     SEQ_T_CYC_TOTAL = 10,     // block 0 cycles: whole kernel
     SEQ_T_ROOT0 = 11,         // block 0 root size
-    SEQ_TRACE_N = 16
+    SEQ_T_R0_STAGED = 12,     // block 0: staged subtrees
+    SEQ_T_R0_SNODES = 13,     // block 0: nodes split in staged subtrees
+    SEQ_T_R0_GNODES = 14,     // block 0: nodes split in global mode
+    SEQ_T_R0_CYC_WARP = 15,   // block 0 cycles: warp 0's splits of staged subtrees
+    SEQ_T_MID_TREES = 16,     // staged subtrees of up to 512 points (512-thread CTAs)
+    SEQ_T_MID_NODES = 17,     // their nodes split by the whole CTA
+    SEQ_T_R0_MNODES = 18,     // block 0: the same
+    SEQ_T_W_LEAF = 20,        // block 0 cycles, warp 0's staged splits: leaf pops
+    SEQ_T_W_DRAW = 21,        //   draws
+    SEQ_T_W_MARGIN = 22,      //   normal, offset, margins, sides
+    SEQ_T_W_PART = 23,        //   partition and pushes
+    SEQ_T_M_DRAW = 24,        // block 0 cycles, CTA-staged splits: draws
+    SEQ_T_M_MARGIN = 25,      //   normal, offset, margins, sides
+    SEQ_T_M_PART = 26,        //   partition
+    SEQ_T_M_STAGE = 27,       //   staging ids and rows
+    SEQ_TRACE_N = 32
 };
 
 constexpr int FOREST_CHUNK = 2048;

@@ -4,8 +4,9 @@
 //    NN-Descent graph (k = 15, the bit-exact form, on a separate context);
 // 2. each subsample cell's target is the distribution of the k-means buckets
 //    of itself and its neighbours (at most 16 distinct buckets);
-// 3. the MLP (mlp.cu) is trained on those targets with Adam, batches of 4096,
-//    a fixed number of epochs, a seeded initialisation and seeded shuffles;
+// 3. the MLP (mlp.cu) is trained on those targets with Adam, batches of 8192,
+//    a fixed number of epochs, a seeded initialisation and seeded shuffles
+//    (every epoch's order from one device sort of hashed keys);
 // 4. every cell's probes are its own bucket followed by the P - 1 most likely
 //    other buckets.
 // The logits are the MLP's output plus a nearest-centroid prior,
@@ -18,17 +19,27 @@
 #include <cstdio>
 #include <cstdlib>
 #include <chrono>
-#include <numeric>
-#include <random>
 #include <vector>
 
 #include "ctx.cuh"
 #include "mlp.cuh"
+#include "primitives.cuh"
 
 namespace pq {
 namespace {
 
 constexpr int T_MAX = 16;  // target buckets per training cell
+
+// Shuffle keys of one epoch: 32 hashed bits per subsample cell, the cell's
+// index as the value; a stable sort gives the epoch's order.
+__global__ void k_shuffle_keys(uint32_t ns, uint32_t ep, uint64_t seed, uint32_t* __restrict__ keys,
+                               uint64_t* __restrict__ vals) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    const uint64_t h = splitmix(seed ^ splitmix(0x5348554646ull + ep) ^ splitmix(uint64_t(i) << 3));
+    keys[i] = uint32_t(h >> 32);
+    vals[i] = i;
+}
 
 // Rows i * n / ns of the padded embedding, d columns each, contiguous.
 __global__ void k_take_rows(const float* __restrict__ X, int d, int dp, uint64_t n, uint32_t ns,
@@ -74,7 +85,7 @@ __global__ void k_targets(const uint32_t* __restrict__ indptr, const uint32_t* _
     }
 }
 
-__global__ void k_gather_batch(const float* __restrict__ Xs, int d, const uint32_t* __restrict__ perm,
+__global__ void k_gather_batch(const float* __restrict__ Xs, int d, const uint64_t* __restrict__ perm,
                                uint32_t rows, const uint32_t* __restrict__ tb,
                                const float* __restrict__ tw, float* __restrict__ xb,
                                uint32_t* __restrict__ bb, float* __restrict__ wbt) {
@@ -190,18 +201,19 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     uint32_t* gix = c->get<uint32_t>("ml_ix", size_t(ns) * gk);
     float* gdx = c->get<float>("ml_dx", size_t(ns) * gk);
     {
-        pq_ctx* g = nullptr;
-        if (pq_ctx_create(c->device, &g) != PQ_OK) throw DeviceError{"graph context"};
+        if (!c->sub && pq_ctx_create(c->device, &c->sub) != PQ_OK) {
+            c->sub = nullptr;
+            throw DeviceError{"graph context"};
+        }
+        pq_ctx* g = c->sub;
         pq_nnd_opts go;
         pq_nnd_opts_default(&go);
         go.k = uint64_t(gk);
         go.seed = seed;
         uint64_t nnz = 0;
         const int rc = pq_nndescent_into_device(g, xs, ns, uint64_t(d), &go, gip, gix, gdx, &nnz, st);
-        const std::string msg = pq_ctx_last_error(g);
-        pq_ctx_destroy(g);
         cudaSetDevice(c->device);
-        if (rc != PQ_OK) throw DeviceError{"subsample graph: " + msg};
+        if (rc != PQ_OK) throw DeviceError{"subsample graph: " + std::string(pq_ctx_last_error(g))};
     }
     const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
     auto since = [](std::chrono::steady_clock::time_point a) {
@@ -230,7 +242,11 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     k_init_params<<<blocks(np, 256), 256, 0, st>>>(net.w, np, mlp_layout(d), d, seed); count_launch();
     mlp_sync_bf16(net, st);
     mlp_set_prior(net, prior, st);
-    const int B = 4096, epochs = 8;
+    // batches of 8192 at learning rate 2e-3: at 4M x 50 the same recall as
+    // 4096 at 1e-3 (0.994) in half the steps; 16384 at 2e-3 or 3e-3 needs a
+    // third round
+    const int B = 8192, epochs = 8;
+    const float lr = 2e-3f;
     float* xb = c->get<float>("ml_xb", size_t(B) * d);
     uint32_t* bb = c->get<uint32_t>("ml_bb", size_t(B) * T_MAX);
     float* bw = c->get<float>("ml_bw", size_t(B) * T_MAX);
@@ -242,43 +258,56 @@ double learned_probes(pq_ctx* c, const float* X, int d, int dp, uint32_t n, uint
     float* loss = c->get<float>("ml_loss", B);
     float* scratch = c->get<float>("ml_scratch", mlp_scratch_floats());
     const MlpBufs tb16 = mlp_bufs(c->get<uint8_t>("ml_b16", mlp_bufs_bytes(B, true)), B, true);
-    uint32_t* dperm = c->get<uint32_t>("ml_perm", ns);
-    std::vector<uint32_t> perm(ns);
-    std::iota(perm.begin(), perm.end(), 0u);
-    std::mt19937_64 rng(seed ^ 0x9e3779b97f4a7c15ull);
+    // every epoch's seeded order, on the device (no host round trip between
+    // epochs)
+    const size_t ne = size_t(ns) * epochs;
+    uint32_t* skeys = c->get<uint32_t>("ml_skeys", ns);
+    uint32_t* skeys2 = c->get<uint32_t>("ml_skeys2", ns);
+    uint64_t* dperm = c->get<uint64_t>("ml_perm", ne);  // the sorted values: the orders
+    uint64_t* svals2 = c->get<uint64_t>("ml_svals2", ns);
+    void* stemp = c->get<uint8_t>("ml_sort_temp", radix_temp_bytes(ns));
+    for (int ep = 0; ep < epochs; ++ep) {
+        uint64_t* order = dperm + size_t(ep) * ns;
+        k_shuffle_keys<<<blocks(ns, 256), 256, 0, st>>>(ns, uint32_t(ep), seed, skeys, order);
+        count_launch();
+        ck(radix_sort_pairs(skeys, order, skeys2, svals2, ns, 32, stemp, st), "shuffle");
+    }
     int step = 0;
     double* eloss = c->get<double>("ml_eloss", epochs);
     ck(cudaMemsetAsync(eloss, 0, epochs * 8, st), "loss");
     std::vector<uint64_t> erows(epochs, 0);
     for (int ep = 0; ep < epochs; ++ep) {
-        std::shuffle(perm.begin(), perm.end(), rng);
-        ck(cudaMemcpyAsync(dperm, perm.data(), size_t(ns) * 4, cudaMemcpyHostToDevice, st), "perm");
         for (uint32_t b0 = 0; b0 + B <= ns || (b0 == 0 && ns > 0); b0 += B) {
             const uint32_t rows = std::min<uint32_t>(B, ns - b0);
             k_gather_batch<<<blocks(size_t(rows) * std::max(d, T_MAX), 256), 256, 0, st>>>(
-                xs, d, dperm + b0, rows, tb, tw, xb, bb, bw);
+                xs, d, dperm + size_t(ep) * ns + b0, rows, tb, tw, xb, bb, bw);
             count_launch();
             ck(mlp_forward(net, xb, int(rows), h1, h2, z, tb16, true, st, &prior), "mlp forward");
             ck(mlp_backward(net, int(rows), h1, h2, z, tb16, bb, bw, T_MAX, loss, dh1, dh2, grad,
                             scratch, st),
                "mlp backward");
-            mlp_adam(net, am, av, grad, ++step, 1e-3f, st);
+            mlp_adam(net, am, av, grad, ++step, lr, st);
             k_sum_f32<<<8, 256, 0, st>>>(loss, rows, eloss + ep); count_launch();
             erows[ep] += rows;
             if (rows < uint32_t(B)) break;
         }
-        ck(cudaStreamSynchronize(st), "epoch");  // the host permutation is reused
     }
     ck(cudaGetLastError(), "training");
     std::vector<double> hl(epochs);
-    ck(cudaMemcpy(hl.data(), eloss, epochs * 8, cudaMemcpyDeviceToHost), "loss");
+    // on the training stream: the losses are complete only when it is
+    ck(cudaMemcpyAsync(hl.data(), eloss, epochs * 8, cudaMemcpyDeviceToHost, st), "loss");
+    ck(cudaStreamSynchronize(st), "loss");
     *loss_first = hl[0] / double(std::max<uint64_t>(erows[0], 1));
     *loss_last = hl[epochs - 1] / double(std::max<uint64_t>(erows[epochs - 1], 1));
     const auto t1 = std::chrono::steady_clock::now();
     *ms_train = std::chrono::duration<double, std::milli>(t1 - t0).count();
-    if (trace)
-        std::fprintf(stderr, "[learned] %d epochs of %u cells (batches of %d): done at %.1f ms\n",
-                     epochs, ns, B, *ms_train);
+    if (trace) {
+        std::fprintf(stderr, "[learned] %d epochs of %u cells (batches of %d): done at %.1f ms; "
+                     "loss per epoch", epochs, ns, B, *ms_train);
+        for (int e = 0; e < epochs; ++e)
+            std::fprintf(stderr, " %.4f", hl[e] / double(std::max<uint64_t>(erows[e], 1)));
+        std::fprintf(stderr, "\n");
+    }
     // ── 4. probes of every cell ──
     const uint32_t R = 65536;
     float* xr = c->get<float>("ml_xr", size_t(R) * d);

@@ -5,11 +5,14 @@
 // NN-Descent uses it to decide whether to fall back to the RP-forest
 // initialisation.
 //
-//   k_sample_scan: CTA (query group of 32, split s of the cells); 8 threads
-//     per query, each keeping its own ascending register list of the 32 best
-//     (distance bits, index) keys over its share of the split's cells, which
-//     are staged in shared memory 128 rows at a time (coalesced float4 loads);
-//     the lists go to global scratch, 8 per (query, split);
+//   k_sample_scan_reg (d = 50): CTA (128 queries, split s of the cells); one
+//     thread per query holds the query row in registers and its ascending
+//     list of the 32 best (distance bits, index) keys; the split's cells are
+//     staged in shared memory 128 rows at a time (contiguous rows, coalesced
+//     float4 loads) and every thread reads the same row at the same time (a
+//     broadcast); one list per (query, split);
+//   k_sample_scan (other d): CTA (query group of 32, split s); 8 threads per
+//     query with their own lists, the query rows also in shared memory;
 //   k_sample_merge: one CTA per query sorts its S x 8 x 32 keys (bitonic, in
 //     shared memory) and counts how many of the k best its graph row holds.
 #include <cuda_runtime.h>
@@ -28,6 +31,7 @@ constexpr int TPQ = 8;   // threads per query
 constexpr int LK = 32;   // keys kept per thread (k <= 32)
 constexpr int CH = 128;  // cells staged per chunk
 constexpr int SCAN_T = QG * TPQ;
+constexpr int QB = 128;  // queries per register-row scan CTA
 constexpr int MERGE_T = 512;
 constexpr int MERGE_MAX = 4096;  // keys per query in the merge (S <= 16)
 
@@ -85,6 +89,84 @@ __global__ void __launch_bounds__(SCAN_T) k_sample_scan(const float* __restrict_
     }
     if (qi < Q) {
         uint64_t* o = out + ((size_t(qi) * S + s) * TPQ + j) * LK;
+#pragma unroll
+        for (int r = 0; r < LK; ++r) o[r] = L[r];
+    }
+}
+
+// Squared distance of a register-held query row to a row in shared memory,
+// in sq_dist_exact_t's order ((a - b)^2 is symmetric bit for bit).
+template <int D>
+__device__ __forceinline__ float sq_dist_reg(const float (&q)[D], const float* __restrict__ c) {
+    constexpr int FULL = D / 8;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float4* c4 = reinterpret_cast<const float4*>(c);
+#pragma unroll
+    for (int b = 0; b < FULL; ++b) {
+        const float4 y0 = c4[2 * b], y1 = c4[2 * b + 1];
+        const float y[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+        for (int l = 0; l < 8; ++l) {
+            const float t = __fsub_rn(q[8 * b + l], y[l]);
+            acc[l] = __fadd_rn(acc[l], __fmul_rn(t, t));
+        }
+    }
+    float tail = 0.0f;
+#pragma unroll
+    for (int j = FULL * 8; j < D; ++j) {
+        const float t = __fsub_rn(q[j], c[j]);
+        tail = __fadd_rn(tail, __fmul_rn(t, t));
+    }
+    const float r = __fadd_rn(__fadd_rn(__fadd_rn(acc[0], acc[4]), __fadd_rn(acc[1], acc[5])),
+                              __fadd_rn(__fadd_rn(acc[2], acc[6]), __fadd_rn(acc[3], acc[7])));
+    return __fadd_rn(r, tail);
+}
+
+template <int D>
+__global__ void __launch_bounds__(QB) k_sample_scan_reg(const float* __restrict__ X, int dp,
+                                                        uint32_t n,
+                                                        const uint32_t* __restrict__ q,
+                                                        uint32_t Q, uint32_t S,
+                                                        uint64_t* __restrict__ out) {
+    extern __shared__ __align__(16) float sm[];  // CH x dp
+    const int tid = threadIdx.x;
+    const uint32_t qi = blockIdx.x * QB + tid;
+    const uint32_t s = blockIdx.y;
+    const uint32_t c0 = uint32_t(uint64_t(n) * s / S), c1 = uint32_t(uint64_t(n) * (s + 1) / S);
+    const uint32_t self = qi < Q ? q[qi] : 0xFFFFFFFFu;
+    const float* qrow = X + size_t(qi < Q ? self : 0u) * dp;
+    float qr[D];
+#pragma unroll
+    for (int j = 0; j < D; ++j) qr[j] = qi < Q ? qrow[j] : 0.0f;
+    uint64_t L[LK];
+#pragma unroll
+    for (int r = 0; r < LK; ++r) L[r] = ~0ull;
+    const int q4 = dp / 4;
+    for (uint32_t b0 = c0; b0 < c1; b0 += CH) {
+        const uint32_t len = min(uint32_t(CH), c1 - b0);
+        __syncthreads();
+        const float4* src = reinterpret_cast<const float4*>(X + size_t(b0) * dp);
+        for (int t = tid; t < int(len) * q4; t += QB) reinterpret_cast<float4*>(sm)[t] = src[t];
+        __syncthreads();
+        if (qi < Q) {
+            for (uint32_t r = 0; r < len; ++r) {
+                const float dd = sq_dist_reg<D>(qr, sm + r * dp);
+                const uint32_t id = b0 + r;
+                const uint64_t key = (uint64_t(__float_as_uint(dd)) << 32) | id;
+                if (key < L[LK - 1] && id != self) {
+#pragma unroll
+                    for (int t = LK - 1; t > 0; --t) {
+                        const bool up = key < L[t - 1];
+                        const bool here = !up && key < L[t];
+                        L[t] = up ? L[t - 1] : (here ? key : L[t]);
+                    }
+                    if (key < L[0]) L[0] = key;
+                }
+            }
+        }
+    }
+    if (qi < Q) {
+        uint64_t* o = out + (size_t(qi) * S + s) * LK;
 #pragma unroll
         for (int r = 0; r < LK; ++r) o[r] = L[r];
     }
@@ -148,18 +230,27 @@ double sampled_recall(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int 
     std::vector<uint32_t> hq(Q);
     const uint64_t off = splitmix(seed ^ 0x5a4d504cull) % n;
     for (uint32_t t = 0; t < Q; ++t) hq[t] = uint32_t((off + uint64_t(t) * n / Q) % n);
-    const uint32_t groups = (Q + QG - 1) / QG;
-    uint32_t S = std::max<uint32_t>(1, (296 + groups - 1) / groups);
-    S = std::min<uint32_t>(S, MERGE_MAX / (TPQ * LK));
+    const bool reg = d == 50;
+    const uint32_t groups = (Q + (reg ? QB : QG) - 1) / (reg ? QB : QG);
+    // lists per (query, split): 1 (register rows) or TPQ
+    const uint32_t per = reg ? 1u : uint32_t(TPQ);
+    // about three CTAs per SM (148 SMs)
+    uint32_t S = std::max<uint32_t>(1, (reg ? 444u : 296u + groups - 1) / groups);
+    S = std::min<uint32_t>(S, MERGE_MAX / (per * LK));
     S = std::min<uint32_t>(S, std::max<uint32_t>(1, n / CH));
     uint32_t* dq = c->get<uint32_t>("sr_q", Q);
-    uint64_t* keys = c->get<uint64_t>("sr_keys", size_t(Q) * S * TPQ * LK);
+    uint64_t* keys = c->get<uint64_t>("sr_keys", size_t(Q) * S * per * LK);
     unsigned long long* hits = c->d_acc + 2;
     ck(cudaMemcpyAsync(dq, hq.data(), size_t(Q) * 4, cudaMemcpyHostToDevice, st), "sample");
     ck(cudaMemsetAsync(hits, 0, 8, st), "hits");
     const size_t smem = size_t(QG + CH) * dp * sizeof(float);
     dim3 grid(groups, S);
-    if (d == 50) {
+    if (reg) {
+        const size_t sm2 = size_t(CH) * dp * sizeof(float);
+        cudaFuncSetAttribute(k_sample_scan_reg<50>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             int(sm2));
+        k_sample_scan_reg<50><<<grid, QB, sm2, st>>>(X, dp, n, dq, Q, S, keys);
+    } else if (d == 50) {
         cudaFuncSetAttribute(k_sample_scan<50>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              int(smem));
         k_sample_scan<50><<<grid, SCAN_T, smem, st>>>(X, d, dp, n, dq, Q, S, keys);
@@ -169,7 +260,7 @@ double sampled_recall(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int 
         k_sample_scan<0><<<grid, SCAN_T, smem, st>>>(X, d, dp, n, dq, Q, S, keys);
     }
     count_launch();
-    k_sample_merge<<<Q, MERGE_T, 0, st>>>(keys, S * TPQ * LK, k, dq, d_indptr, d_indices, hits);
+    k_sample_merge<<<Q, MERGE_T, 0, st>>>(keys, S * per * LK, k, dq, d_indptr, d_indices, hits);
     count_launch();
     unsigned long long h = 0;
     ck(cudaMemcpyAsync(&h, hits, 8, cudaMemcpyDeviceToHost, st), "hits");

@@ -161,3 +161,32 @@ def test_learned_init_falls_back_to_rp_init(monkeypatch):
     np.testing.assert_array_equal(got["indptr"], want["indptr"])
     np.testing.assert_array_equal(got["indices"], want["indices"])
     assert got["data"].tobytes() == want["data"].tobytes()
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("d", [50, 48])
+def test_sampled_recall_matches_an_exact_count(d):
+    """The sampled recall the fallback decides on (1,024 evenly strided cells
+    from a seeded offset, their exact k nearest against all cells) equals the
+    count of the graph's hits among the FP64 k nearest of the same cells, up
+    to FP32-vs-FP64 order at the boundary.  d = 50 runs the register-row scan,
+    d = 48 the shared-memory one."""
+    import oracle
+    import polariseq_b200 as pq
+    from polariseq_b200 import synth
+
+    n, k, seed = 70_000, 15, 7
+    x = synth.mixture_lognormal(n, d, 20, seed=31)
+    g = pq.nndescent_dense(x, k, init="learned", seed=seed)
+    st = pq.default_context(0).stats()
+    Q = 1024
+    off = oracle.splitmix(seed ^ 0x5A4D504C) % n
+    q = np.array([(off + t * n // Q) % n for t in range(Q)], np.uint32)
+    want, _ = oracle.exact_knn_f64(x, q, k)
+    ip, ix = g["indptr"], g["indices"]
+    hits = sum(len(set(ix[ip[i]:ip[i + 1]].tolist()) & set(want[t].tolist()))
+               for t, i in enumerate(q.tolist()))
+    est = hits / (Q * k)
+    # est_recall is the estimate of the graph returned (learned, or the RP
+    # build's when the fallback kept that)
+    assert abs(st["est_recall"] - est) <= 5e-4, (st["est_recall"], est)
