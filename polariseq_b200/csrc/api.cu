@@ -741,6 +741,9 @@ int guarded(pq_ctx* c, F&& f) {
     } catch (const std::string& s) {
         drain();
         return fail(c, PQ_ENOMEM, s);
+    } catch (const std::exception& e) {  // host-side failures (allocation, sizes)
+        drain();
+        return fail(c, PQ_EDEVICE, std::string("host error: ") + e.what());
     }
 }
 

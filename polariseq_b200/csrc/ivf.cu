@@ -59,6 +59,8 @@ constexpr int NEPI = TQ * NG;   // epilogue threads
 constexpr int NT = NEPI + 64;   // + TMA warp + MMA warp
 constexpr int CPG = TCN / NG;   // columns per warpgroup
 constexpr int BUF = 32;         // staged admissions per (row, column half), buffered mode
+                                // (at least the 32 one chunk can admit)
+constexpr int STASH = 32;       // BF16: floats per epilogue thread, a flagged chunk's values
 constexpr int QST = 2;          // Q tile stages
 constexpr int MAXCS = 3;        // candidate tile stages (at most)
 constexpr uint32_t WAIT_LIMIT = 1u << 24;
@@ -143,6 +145,10 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     // same values)
     float* hsall = reinterpret_cast<float*>(biall + NG * BUF * TQ);        // 2 x NG x CPG
     float* hkall = hsall + 2 * NG * CPG;                                   // 2 x NG x CPG
+    // BF16: each epilogue thread's stash row for a flagged chunk (its 16-byte
+    // groups XOR-swizzled by lane so that a warp's stores hit every bank);
+    // E4M3 (whose scale slots take the room) selects from registers instead
+    float* stash = hsall;                                                  // NEPI x STASH
     __shared__ IvfBars B;
     __shared__ unsigned long long ld_cyc;  // tracing: block 0 warp 0's TMEM load waits
     const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
@@ -419,6 +425,16 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
                         if (v[j] > ath) lm |= 1u << j;
+                    // BF16: the chunk's values go to this thread's stash row, read
+                    // back by column below (no register select per admission)
+                    float* srow = stash + size_t(tid) * STASH;
+                    const int swz = (lane & 7) << 2;
+                    if constexpr (!F8) {
+#pragma unroll
+                        for (int j = 0; j < 32; j += 4)
+                            *reinterpret_cast<float4*>(srow + (j ^ swz)) =
+                                make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                    }
                     if (tracing) {
                         const uint32_t na = __reduce_add_sync(FULL, uint32_t(__popc(lm)));
                         const uint32_t wm = __reduce_or_sync(FULL, lm);
@@ -440,8 +456,12 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
                         if (lm) {
                             const int j = __ffs(lm) - 1;
                             lm &= lm - 1;
-                            float vj = __uint_as_float(select32(r, j));
-                            if constexpr (F8) vj = fmaf(vj * hk[q * 32 + j], rq, -hs[q * 32 + j]);
+                            float vj;
+                            if constexpr (F8)
+                                vj = fmaf(__uint_as_float(select32(r, j)) * hk[q * 32 + j], rq,
+                                          -hs[q * 32 + j]);
+                            else
+                                vj = srow[j ^ swz];
                             const float dj = fmaf(-2.0f, vj, qn);
                             if (dj < thr && cb0 + j != qself) {
                                 if (buffered) {
@@ -550,7 +570,7 @@ EncodeTiledFn encode_fn() {
 template <int S, bool F8>
 size_t tiles_smem() {
     return 1024 + size_t(QST) * TQ * ROWB + size_t(cand_stages(S, F8)) * TCN * ROWB +
-           size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * 2 * NG * CPG * 4 : 0);
+           size_t(NG) * BUF * TQ * 8 + (F8 ? 2 * 2 * NG * CPG * 4 : size_t(NEPI) * STASH * 4);
 }
 
 template <int S, bool F8>
