@@ -152,13 +152,13 @@ __global__ void k_job_tstart(const uint32_t* __restrict__ job_bucket,
                              const uint32_t* __restrict__ job_qstart, uint32_t njobs,
                              const uint32_t* __restrict__ ekeys, uint32_t C,
                              const uint32_t* __restrict__ c_off,
-                             const uint32_t* __restrict__ pair_off,
+                             const uint32_t* __restrict__ pair_off, uint32_t tile_cols,
                              uint32_t* __restrict__ tstart) {
     const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= njobs) return;
     const uint32_t b = job_bucket[j];
     const uint32_t a = ekeys[job_qstart[j]] % C;
-    tstart[j] = (pair_off[size_t(b) * C + a] - c_off[b]) / 256u;
+    tstart[j] = (pair_off[size_t(b) * C + a] - c_off[b]) / tile_cols;
 }
 
 // Seed thresholds of the non-primary entries: the R-th best approximate
@@ -987,13 +987,22 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     uint32_t* lab = c->get<uint32_t>("km_lab", ns);
     // one-bucket nearest-centroid search on the tensor cores: queries [0, nq)
     // against all C centroids, S_out nearest per query
+    // BF16 tiles with 16-entry shortlists run the wide kernel (jobs of 256
+    // query entries, candidate tiles of 128)
+    const bool wide_tiles = [] {
+        const char* e = std::getenv("POLARISEQ_TILES_WIDE");
+        return !(e && e[0] == '0');
+    }();
     auto centroid_search = [&](const __nv_bfloat16* qrows, const float* qnorm, uint32_t nq,
                                int s_out, float* od, uint32_t* oi) {
-        const uint32_t nj = (nq + 127) / 128;
+        const int sr = s_out == 1 ? 1 : 16;  // per column half: the nearest, or up to 16
+        const int wide = sr == 16 && wide_tiles ? 1 : 0;
+        const uint32_t JR = uint32_t(ivf_job_rows(wide)), TC = uint32_t(ivf_tile_cols(wide));
+        const uint32_t nj = (nq + JR - 1) / JR;
         std::vector<uint32_t> hb(nj, 0), hq(nj), he(nj);
         for (uint32_t j = 0; j < nj; ++j) {
-            hq[j] = j * 128;
-            he[j] = std::min(nq, j * 128 + 128);
+            hq[j] = j * JR;
+            he[j] = std::min(nq, j * JR + JR);
         }
         uint32_t* jb = c->get<uint32_t>("ajob_b", nj);
         uint32_t* jq = c->get<uint32_t>("ajob_q", nj);
@@ -1005,7 +1014,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         ck(cudaMemcpyAsync(je, he.data(), size_t(nj) * 4, cudaMemcpyHostToDevice, st), "jobs");
         ck(cudaMemcpyAsync(offs, ho, 16, cudaMemcpyHostToDevice, st), "jobs");
         CUtensorMap tq, tcm;
-        if (!make_bf16_map(&tq, qrows, nq, 128) || !make_bf16_map(&tcm, cb, C, 256))
+        if (!make_bf16_map(&tq, qrows, nq, JR) || !make_bf16_map(&tcm, cb, C, TC))
             throw DeviceError{"cuTensorMapEncodeTiled failed"};
         IvfTileArgs a{};
         a.job_bucket = jb;
@@ -1015,8 +1024,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         a.c_off = offs;
         a.qnorm = qnorm;
         a.qself = noself;
-        const int sr = s_out == 1 ? 1 : 16;  // per column half: the nearest, or up to 16
         a.S = sr;
+        a.wide = wide;
         a.out_d = c->get<float>("arun_d", size_t(nq) * 2 * 16);
         a.out_i = c->get<uint32_t>("arun_i", size_t(nq) * 2 * 16);
         a.err = c->d_err;
@@ -1193,22 +1202,25 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     std::vector<uint32_t> hc(C + 1);
     ck(cudaMemcpy(hc.data(), c_off, size_t(C + 1) * 4, cudaMemcpyDeviceToHost), "c_off");
     // jobs of one pass from its entries' bucket bounds (hq[key] for key in
-    // [key0, key0 + C)): 128 entries of one probe bucket each
+    // [key0, key0 + C)): JR entries of one probe bucket each, against
+    // candidate tiles of TC
+    const int wide_pass = (!fp8 && ivf_shortlist(k + 1) == 16 && wide_tiles) ? 1 : 0;
+    const uint32_t JR = uint32_t(ivf_job_rows(wide_pass)), TC = uint32_t(ivf_tile_cols(wide_pass));
     std::vector<uint32_t> jb[2], jq[2], je[2], jt0;
     uint64_t tile_pairs = 0, maxb = 0, cells = 0, pass_pairs[2] = {0, 0};
     auto make_jobs = [&](int pass, const std::vector<uint32_t>& bounds, uint32_t key0,
                          uint32_t base) {
         for (uint32_t b = 0; b < C; ++b) {
             const uint32_t key = b + key0;
-            const uint64_t nct = (hc[b + 1] - hc[b] + 255) / 256;
+            const uint64_t nct = (hc[b + 1] - hc[b] + TC - 1) / TC;
             maxb = std::max<uint64_t>(maxb, hc[b + 1] - hc[b]);
-            for (uint32_t q0 = base + bounds[key]; q0 < base + bounds[key + 1]; q0 += 128) {
-                const uint32_t q1 = std::min(q0 + 128, base + bounds[key + 1]);
+            for (uint32_t q0 = base + bounds[key]; q0 < base + bounds[key + 1]; q0 += JR) {
+                const uint32_t q1 = std::min(q0 + JR, base + bounds[key + 1]);
                 jb[pass].push_back(b);
                 jq[pass].push_back(q0);
                 je[pass].push_back(q1);
                 // a primary job's own cells are its candidates at the same offset
-                if (pass == 0) jt0.push_back((q0 - base - bounds[key]) / 256);
+                if (pass == 0) jt0.push_back((q0 - base - bounds[key]) / TC);
                 tile_pairs += nct;
                 pass_pairs[pass] += nct;
                 cells += uint64_t(q1 - q0) * (hc[b + 1] - hc[b]);
@@ -1295,8 +1307,8 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             if (nj == 0) continue;
             CUtensorMap tq, tcm;
             const bool maps =
-                fp8 ? make_fp8_map(&tq, qb8, ne, 128) && make_fp8_map(&tcm, xc8, n, 256)
-                    : make_bf16_map(&tq, qb, ne, 128) && make_bf16_map(&tcm, xc, n, 256);
+                fp8 ? make_fp8_map(&tq, qb8, ne, JR) && make_fp8_map(&tcm, xc8, n, TC)
+                    : make_bf16_map(&tq, qb, ne, JR) && make_bf16_map(&tcm, xc, n, TC);
             if (!maps) throw DeviceError{"cuTensorMapEncodeTiled failed"};
             uint32_t* djb = c->get<uint32_t>(pass ? "job_b1" : "job_b0", nj);
             uint32_t* djq = c->get<uint32_t>(pass ? "job_q1" : "job_q0", nj);
@@ -1310,7 +1322,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
                    "jobs");
             } else {
                 k_job_tstart<<<blocks(nj, 256), 256, 0, st>>>(djb, djq, nj, ekeys2, C, c_off,
-                                                              pair_off, djt);
+                                                              pair_off, TC, djt);
                 count_launch();
             }
             IvfTileArgs a{};
@@ -1336,6 +1348,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
             a.err = c->d_err;
             a.trace = tbuf;
             a.test_wait_polls = test_wait;
+            a.wide = wide_pass;
             {
                 KGScope kg(c, PQ_KG_TILES);
                 ck(launch_ivf_tiles(tq, tcm, a, std::min<int>(num_sms, int(nj)), st), "ivf tiles");

@@ -548,6 +548,382 @@ __global__ void __launch_bounds__(NT, 1) k_ivf_tiles(const __grid_constant__ CUt
     if (w == 0) tc::tmem_dealloc(taddr, 512);
 }
 
+// ── wide variant (BF16, S = 16) ─────────────────────────────────────────
+// Jobs of 256 query entries against candidate tiles of 128: each tile is two
+// M = 128, N = 128 products (query rows 0-127 and 128-255) into the two
+// halves of one TMEM buffer (256 columns, two buffers), and 16 epilogue warps
+// (four per scheduler) take them: warp w reads TMEM lanes 32(w%4).. of row
+// half w/8 for column half (w/4)%2 (64 columns), 16 columns per load.  Each
+// (entry, column half) keeps one shortlist as in the standard kernel, so the
+// output runs are the same; twice the warps hide the epilogue's dependency
+// chains.
+enum { ET_WAIT, ET_WORK, ET_END, ET_SLOW_CYC, ET_JOBS, ET_SLOW, ET_ADMITS, ET_WMBITS };
+constexpr int WQ = 256;            // query entries per job
+constexpr int WCN = 128;           // candidates per tile
+constexpr int WEPI = 512;          // epilogue threads
+constexpr int WNT = WEPI + 64;     // + TMA warp + MMA warp
+constexpr int WCPG = WCN / NG;     // columns per warp and tile (64)
+constexpr int WBUF = 16;           // staged admissions per (entry, half): one 16-column chunk's
+constexpr int WSTASH = 16;         // floats per epilogue thread: a flagged chunk's values
+constexpr int WCS = 3;             // candidate tile stages
+
+__device__ __forceinline__ float max16(const float (&v)[16]) {
+    const float a = max3f(v[0], v[1], v[2]), b = max3f(v[3], v[4], v[5]),
+                c = max3f(v[6], v[7], v[8]), e = max3f(v[9], v[10], v[11]),
+                f = max3f(v[12], v[13], v[14]);
+    return fmaxf(max3f(a, b, c), max3f(e, f, v[15]));
+}
+
+size_t wide_smem() {
+    return 1024 + size_t(QST) * WQ * ROWB + size_t(WCS) * WCN * ROWB +
+           size_t(NG) * WBUF * WQ * 8 + size_t(WEPI) * WSTASH * 4;
+}
+
+__global__ void __launch_bounds__(WNT, 1) k_ivf_wide(const __grid_constant__ CUtensorMap tmQ,
+                                                     const __grid_constant__ CUtensorMap tmC,
+                                                     IvfTileArgs a) {
+    constexpr int S = 16;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = smem_raw + ((1024u - (tc::smem_u32(smem_raw) & 1023u)) & 1023u);
+    uint8_t* sQ = smem;                                                    // QST x 32 KB
+    uint8_t* sC = sQ + QST * WQ * ROWB;                                    // WCS x 16 KB
+    float* bdall = reinterpret_cast<float*>(sC + WCS * WCN * ROWB);        // NG x WBUF x WQ
+    uint32_t* biall = reinterpret_cast<uint32_t*>(bdall + NG * WBUF * WQ); // NG x WBUF x WQ
+    float* stash = reinterpret_cast<float*>(biall + NG * WBUF * WQ);       // WEPI x WSTASH
+    __shared__ IvfBars B;
+    __shared__ unsigned long long et[8];  // tracing: block 0 thread 0's counters
+    const int tid = threadIdx.x, w = tid >> 5, lane = tid & 31;
+    volatile int* abort_flag = &B.abort;
+
+    if (w == 0) {
+        tc::tmem_alloc(&B.tmem, 512);
+        tc::tmem_relinquish();
+    }
+    if (tid == 0) {
+        for (int s = 0; s < QST; ++s) {
+            tc::mbar_init(&B.q_full[s], 1);
+            tc::mbar_init(&B.q_empty[s], 1);
+        }
+        for (int s = 0; s < MAXCS; ++s) {
+            tc::mbar_init(&B.c_full[s], 1);
+            tc::mbar_init(&B.c_empty[s], 1);
+        }
+        for (int s = 0; s < 2; ++s) {
+            tc::mbar_init(&B.t_full[s], 1);
+            tc::mbar_init(&B.t_empty[s], WEPI / 32);
+        }
+        tc::mbar_init(&B.done, 1);
+        tc::mbar_init(&B.never, 1);
+        tc::fence_barrier_init();
+        B.abort = 0;
+        for (int i = 0; i < 8; ++i) et[i] = 0;
+        if (a.test_wait_polls && !tc::mbar_wait(&B.never, 0, a.test_wait_polls)) B.abort = 1;
+    }
+    if (tid == WEPI) {
+        tc::prefetch_tmap(&tmQ);
+        tc::prefetch_tmap(&tmC);
+    }
+    __syncthreads();
+    tc::tc_fence_after();
+    const uint32_t taddr = B.tmem;
+    const bool tracing = a.trace && blockIdx.x == 0;
+    const long long c_start = clock64();
+
+    if (w == WEPI / 32) {
+        // ── TMA producer ──
+        if (lane == 0) {
+            uint32_t qi = 0, ci = 0;
+            long long c_wait = 0;
+            for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
+                const uint32_t b = a.job_bucket[job], qs = a.job_qstart[job];
+                const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
+                const uint32_t nct = (ce - cs + WCN - 1) / WCN;
+                const uint32_t tfirst =
+                    (a.job_tstart && a.job_tstart[job] < nct) ? a.job_tstart[job] : 0u;
+                if (nct == 0) continue;
+                const int qsd = int(qi % QST);
+                long long c0 = clock64();
+                if (!tc::mbar_wait(&B.q_empty[qsd], ((qi / QST) & 1) ^ 1, WAIT_LIMIT)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                c_wait += clock64() - c0;
+                tc::mbar_expect_tx(&B.q_full[qsd], WQ * ROWB);
+                tc::tma_load_2d(sQ + qsd * WQ * ROWB, &tmQ, &B.q_full[qsd], 0, int(qs));
+                ++qi;
+                for (uint32_t t = 0; t < nct; ++t) {
+                    const int s = int(ci % WCS);
+                    c0 = clock64();
+                    if (!tc::mbar_wait(&B.c_empty[s], ((ci / WCS) & 1) ^ 1, WAIT_LIMIT)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    c_wait += clock64() - c0;
+                    tc::mbar_expect_tx(&B.c_full[s], WCN * ROWB);
+                    const uint32_t tt = tfirst + t >= nct ? tfirst + t - nct : tfirst + t;
+                    tc::tma_load_2d(sC + s * WCN * ROWB, &tmC, &B.c_full[s], 0, int(cs + tt * WCN));
+                    ++ci;
+                }
+            }
+            for (int s = 0; s < WCS; ++s) {
+                const uint32_t uses = ci / WCS + (uint32_t(s) < ci % WCS ? 1u : 0u);
+                if (uses > 0 && !tc::mbar_wait(&B.c_full[s], (uses - 1) & 1, WAIT_LIMIT))
+                    *abort_flag = 1;
+            }
+            for (int s = 0; s < QST; ++s) {
+                const uint32_t uses = qi / QST + (uint32_t(s) < qi % QST ? 1u : 0u);
+                if (uses > 0 && !tc::mbar_wait(&B.q_full[s], (uses - 1) & 1, WAIT_LIMIT))
+                    *abort_flag = 1;
+            }
+            if (tracing) a.trace[IVF_T_TMA_WAIT] = (unsigned long long)c_wait;
+        }
+        __syncwarp();
+    } else if (w == WEPI / 32 + 1) {
+        // ── MMA issuer: two M = 128 products per tile ──
+        if (lane == 0) {
+            const uint32_t idesc = tc::idesc_bf16_f32(128, WCN);
+            uint32_t qi = 0, ci = 0, ti = 0;
+            long long c_wait_c = 0, c_wait_t = 0;
+            for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
+                const uint32_t b = a.job_bucket[job];
+                const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
+                const uint32_t nct = (ce - cs + WCN - 1) / WCN;
+                if (nct == 0) continue;
+                const int qsd = int(qi % QST);
+                if (!tc::mbar_wait(&B.q_full[qsd], (qi / QST) & 1, WAIT_LIMIT)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                // the query tile's row halves: 128 rows of 128 B each, 16 KB apart
+                const uint64_t dQ0 = tc::desc_k_sw128(tc::smem_u32(sQ + qsd * WQ * ROWB));
+                const uint64_t dQ1 =
+                    tc::desc_k_sw128(tc::smem_u32(sQ + qsd * WQ * ROWB + 128 * ROWB));
+                bool ok = true;
+                for (uint32_t t = 0; t < nct && ok; ++t) {
+                    const int s = int(ci % WCS), tb = int(ti & 1);
+                    long long c0 = clock64();
+                    ok = tc::mbar_wait(&B.c_full[s], (ci / WCS) & 1, WAIT_LIMIT);
+                    long long c1 = clock64();
+                    ok = ok && tc::mbar_wait(&B.t_empty[tb], ((ti >> 1) & 1) ^ 1, WAIT_LIMIT);
+                    c_wait_c += c1 - c0;
+                    c_wait_t += clock64() - c1;
+                    if (!ok) break;
+                    tc::tc_fence_after();
+                    const uint64_t dC = tc::desc_k_sw128(tc::smem_u32(sC + s * WCN * ROWB));
+                    const uint32_t d0 = taddr + uint32_t(tb * 2 * WCN);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+                        tc::umma_f16(d0, dQ0 + uint64_t(2 * kk), dC + uint64_t(2 * kk), idesc,
+                                     kk > 0 ? 1u : 0u);
+#pragma unroll
+                    for (int kk = 0; kk < 4; ++kk)
+                        tc::umma_f16(d0 + uint32_t(WCN), dQ1 + uint64_t(2 * kk),
+                                     dC + uint64_t(2 * kk), idesc, kk > 0 ? 1u : 0u);
+                    tc::umma_commit(&B.c_empty[s]);
+                    tc::umma_commit(&B.t_full[tb]);
+                    ++ci;
+                    ++ti;
+                }
+                tc::umma_commit(&B.q_empty[qsd]);
+                ++qi;
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+            }
+            tc::umma_commit(&B.done);
+            if (!tc::mbar_wait(&B.done, 0, WAIT_LIMIT)) *abort_flag = 1;
+            if (tracing) {
+                a.trace[IVF_T_MMA_WAIT_C] = (unsigned long long)c_wait_c;
+                a.trace[IVF_T_MMA_WAIT_T] = (unsigned long long)c_wait_t;
+                a.trace[IVF_T_TILES] = ti;
+            }
+        }
+        __syncwarp();
+    } else {
+        // ── epilogue: row half h, column half g, TMEM lane quarter w % 4 ──
+        const int h = w >> 3, g = (w >> 2) & 1;
+        const int row = h * 128 + (w & 3) * 32 + lane;
+        const uint32_t lane_base = uint32_t((w & 3) * 32) << 16;
+        const bool t0 = tracing && tid == 0;
+        const bool buffered = a.buffered != 0;
+        float* bd = bdall + size_t(g) * WBUF * WQ + row;
+        uint32_t* bi = biall + size_t(g) * WBUF * WQ + row;
+        float* srow = stash + size_t(tid) * WSTASH;
+        // 16-byte groups of the stash row swizzled so that 8 lanes' stores
+        // (64-byte rows) cover all 32 banks
+        const int swz = ((lane >> 1) & 3) << 2;
+        uint32_t ti = 0;
+        uint32_t nb = 0, nqs = 0, nqe = 0, nts = 0;
+        auto load_job = [&](uint32_t j) {
+            if (j < a.njobs) {
+                nb = a.job_bucket[j];
+                nqs = a.job_qstart[j];
+                nqe = a.job_qend[j];
+                nts = a.job_tstart ? a.job_tstart[j] : 0u;
+            }
+        };
+        load_job(blockIdx.x);
+        for (uint32_t job = blockIdx.x; job < a.njobs && !*abort_flag; job += gridDim.x) {
+            const uint32_t b = nb, qs = nqs, qe = nqe, ts = nts;
+            load_job(job + gridDim.x);
+            const uint32_t cs = a.c_off[b], ce = a.c_off[b + 1];
+            const uint32_t nct = (ce - cs + WCN - 1) / WCN;
+            const uint32_t tfirst = ts < nct ? ts : 0u;
+            const uint32_t entry = qs + row;
+            const bool valid = entry < qe;
+            const float qn = valid ? a.qnorm[entry] : __int_as_float(0x7f800000);
+            const uint32_t qself = valid ? a.qself[entry] : 0xFFFFFFFFu;
+            const float thr0 = (valid && a.qthr) ? a.qthr[entry] : __int_as_float(0x7f800000);
+            const uint32_t slot = (valid && a.out_slot) ? a.out_slot[entry] : entry;
+            float thr = thr0;
+            float ath = (qn - thr) * 0.5f;
+            float sv[S];
+            uint32_t sx[S];
+#pragma unroll
+            for (int j = 0; j < S; ++j) {
+                sv[j] = __int_as_float(0x7f800000);
+                sx[j] = 0xFFFFFFFFu;
+            }
+            int cnt = 0;
+            auto flush = [&]() {
+                for (int u = 0; u < cnt; ++u) {
+                    const float d = bd[u * WQ];
+                    if (d < thr) {
+                        shortlist_push<S>(sv, sx, d, bi[u * WQ]);
+                        thr = fminf(thr0, sv[S - 1]);
+                    }
+                }
+                cnt = 0;
+                ath = (qn - thr) * 0.5f;
+            };
+            bool ok = true;
+            for (uint32_t t = 0; t < nct; ++t) {
+                const int tb = int(ti & 1);
+                long long c0 = t0 ? clock64() : 0;
+                ok = tc::mbar_wait(&B.t_full[tb], (ti >> 1) & 1, WAIT_LIMIT);
+                ok = __all_sync(FULL, ok);
+                if (!ok) break;
+                tc::tc_fence_after();
+                const uint32_t tcol =
+                    taddr + lane_base + uint32_t(tb * 2 * WCN + h * WCN + g * WCPG);
+                const uint32_t tt = tfirst + t >= nct ? tfirst + t - nct : tfirst + t;
+                const int lim = int(ce) - int(cs + tt * WCN + g * WCPG);
+                const uint32_t cbase = cs + tt * WCN + g * WCPG;
+                long long c1 = t0 ? clock64() : 0;
+#pragma unroll 1
+                for (int q = 0; q < WCPG / 16; ++q) {
+                    uint32_t r[16];
+                    tc::tmem_ld16(tcol + uint32_t(q * 16), r);
+                    tc::tmem_ld_wait();
+                    float v[16];
+#pragma unroll
+                    for (int j = 0; j < 16; ++j) v[j] = __uint_as_float(r[j]);
+                    if (lim < (q + 1) * 16) {
+#pragma unroll
+                        for (int j = 0; j < 16; ++j)
+                            if (q * 16 + j >= lim) v[j] = __int_as_float(0xff800000);
+                    }
+                    if (!__any_sync(FULL, max16(v) > ath)) continue;
+                    const long long cs0 = t0 ? clock64() : 0;
+                    uint32_t lm = 0;
+#pragma unroll
+                    for (int j = 0; j < 16; ++j)
+                        if (v[j] > ath) lm |= 1u << j;
+#pragma unroll
+                    for (int j = 0; j < 16; j += 4)
+                        *reinterpret_cast<float4*>(srow + (j ^ swz)) =
+                            make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+                    if (tracing) {
+                        const uint32_t na = __reduce_add_sync(FULL, uint32_t(__popc(lm)));
+                        const uint32_t wm = __reduce_or_sync(FULL, lm);
+                        if (t0) {
+                            et[ET_SLOW] += 1;
+                            et[ET_ADMITS] += na;
+                            et[ET_WMBITS] += __popc(wm);
+                        }
+                    }
+                    if (buffered &&
+                        __reduce_max_sync(FULL, uint32_t(cnt + __popc(lm))) > uint32_t(WBUF))
+                        flush();
+                    const uint32_t cb0 = cbase + q * 16;
+                    while (__any_sync(FULL, lm != 0)) {
+                        if (lm) {
+                            const int j = __ffs(lm) - 1;
+                            lm &= lm - 1;
+                            const float dj = fmaf(-2.0f, srow[j ^ swz], qn);
+                            if (dj < thr && cb0 + j != qself) {
+                                if (buffered) {
+                                    bd[cnt * WQ] = dj;
+                                    bi[cnt * WQ] = cb0 + j;
+                                    ++cnt;
+                                } else {
+                                    shortlist_push<S>(sv, sx, dj, cb0 + j);
+                                    thr = fminf(thr0, sv[S - 1]);
+                                    ath = (qn - thr) * 0.5f;
+                                }
+                            }
+                        }
+                    }
+                    if (t0) et[ET_SLOW_CYC] += clock64() - cs0;
+                }
+                tc::tc_fence_before();
+                __syncwarp();
+                if (lane == 0) tc::mbar_arrive(&B.t_empty[tb]);
+                ++ti;
+                if (t0) {
+                    const long long c2 = clock64();
+                    et[ET_WAIT] += c1 - c0;
+                    et[ET_WORK] += c2 - c1;
+                }
+            }
+            if (!ok) {
+                *abort_flag = 1;
+                break;
+            }
+            long long c3 = t0 ? clock64() : 0;
+            if (cnt > 0) flush();
+            if (valid) {
+                int live = S;
+                if (a.out_n) {
+                    live = 0;
+#pragma unroll
+                    for (int j = 0; j < S; ++j)
+                        live += sv[j] < __int_as_float(0x7f800000) ? 1 : 0;
+                    a.out_n[size_t(slot) * NG + g] = uint8_t(live);
+                }
+                float4* od = reinterpret_cast<float4*>(a.out_d + (size_t(entry) * NG + g) * S);
+                uint4* oi = reinterpret_cast<uint4*>(a.out_i + (size_t(entry) * NG + g) * S);
+#pragma unroll
+                for (int j = 0; j < S / 4; ++j)
+                    if (4 * j < live) {
+                        od[j] = make_float4(sv[4 * j], sv[4 * j + 1], sv[4 * j + 2], sv[4 * j + 3]);
+                        oi[j] = make_uint4(sx[4 * j], sx[4 * j + 1], sx[4 * j + 2], sx[4 * j + 3]);
+                    }
+            }
+            if (t0) {
+                et[ET_JOBS] += 1;
+                et[ET_END] += clock64() - c3;
+            }
+        }
+        if (t0) {
+            a.trace[IVF_T_EPI_WAIT] = et[ET_WAIT];
+            a.trace[IVF_T_EPI_WORK] = et[ET_WORK];
+            a.trace[IVF_T_EPI_END] = et[ET_END];
+            a.trace[IVF_T_JOBS] = et[ET_JOBS];
+            a.trace[IVF_T_SLOW] = et[ET_SLOW];
+            a.trace[IVF_T_ADMITS] = et[ET_ADMITS];
+            a.trace[IVF_T_WMBITS] = et[ET_WMBITS];
+            a.trace[IVF_T_SLOW_CYC] = et[ET_SLOW_CYC];
+        }
+    }
+    __syncthreads();
+    if (tracing && tid == 0) a.trace[IVF_T_TOTAL] = (unsigned long long)(clock64() - c_start);
+    if (*abort_flag && tid == 0) atomicExch(a.err, 2);
+    tc::tc_fence_after();
+    if (w == 0) tc::tmem_dealloc(taddr, 512);
+}
+
 // ── host: tensor maps ────────────────────────────────────────────────────
 typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
@@ -635,6 +1011,15 @@ int ivf_shortlist(int want) { return want <= 16 ? 16 : (want <= 32 ? 32 : 0); }
 cudaError_t launch_ivf_tiles(const CUtensorMap& tmQ, const CUtensorMap& tmC,
                              const IvfTileArgs& a, int grid, cudaStream_t st) {
     if (a.njobs == 0) return cudaSuccess;
+    if (a.wide) {
+        if (a.fp8 || a.S != 16) return cudaErrorInvalidValue;
+        const size_t sm = wide_smem();
+        cudaError_t e = cudaFuncSetAttribute(k_ivf_wide, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             int(sm));
+        if (e != cudaSuccess) return e;
+        k_ivf_wide<<<grid, WNT, sm, st>>>(tmQ, tmC, a); count_launch();
+        return cudaGetLastError();
+    }
     if (a.fp8) {
         if (a.S == 16) return launch_s<16, true>(tmQ, tmC, a, grid, st);
         if (a.S == 32) return launch_s<32, true>(tmQ, tmC, a, grid, st);

@@ -50,6 +50,10 @@ struct IvfTileArgs {
     // issued; the wait gives up, every role skips its jobs and the kernel
     // reports error 2 (a bounded wait gave up) with nothing in flight
     uint32_t test_wait_polls;
+    // BF16 with S = 16: jobs of ivf_job_rows(1) = 256 query entries against
+    // candidate tiles of ivf_tile_cols(1) = 128 (16 epilogue warps); else 128
+    // entries against tiles of 256
+    int wide;
 };
 
 enum { IVF_T_EPI_WAIT = 0, IVF_T_EPI_WORK = 1, IVF_T_EPI_END = 2, IVF_T_MMA_WAIT_C = 3,
@@ -69,6 +73,10 @@ bool make_fp8_map(CUtensorMap* map, const void* base, uint64_t rows, uint32_t bo
 int ivf_groups();
 // The shortlist length the kernel supports for `want` entries (0 = too many).
 int ivf_shortlist(int want);
+// Job and tile geometry: query entries per job and candidates per tile (the
+// maps' box rows), for the wide (BF16, S = 16) or the standard kernel.
+inline int ivf_job_rows(int wide) { return wide ? 256 : 128; }
+inline int ivf_tile_cols(int wide) { return wide ? 128 : 256; }
 cudaError_t launch_ivf_tiles(const CUtensorMap& tmQ, const CUtensorMap& tmC,
                              const IvfTileArgs& a, int grid, cudaStream_t st);
 
