@@ -239,12 +239,14 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-# DRAM bytes (read + write) per 128 x 256 tile pair of the shortlist tile kernel:
-# an ncu capture (--set full) of its two passes at 1M x 50 read
-# and wrote 0.537 GB over 184,331 tile pairs (primary pass) and 1.443 GB over
-# 806,044 (other probes), 1,999 bytes per pair over both; a launch's traffic
+# DRAM bytes (read + write) per tile pair (128 x 256 or 256 x 128 contractions)
+# of the shortlist tile kernels, from ncu captures (--set full) of their two
+# passes at 1M x 50: the wide kernel (BF16, 16-entry shortlists) read and wrote
+# 0.528 GB over 170,761 pairs (primary pass) and 1.379 GB over 721,611 (other
+# probes), 2,137 bytes per pair over both; the standard kernel 0.537 GB over
+# 184,331 and 1.443 GB over 806,044, 1,999 bytes per pair.  A launch's traffic
 # is taken to scale with the tile pairs it processes.
-TILE_DRAM_BYTES_PER_PAIR = 1999.0
+TILE_DRAM_BYTES_PER_PAIR = {"k_ivf_wide": 2137.0, "k_ivf_tiles": 1999.0}
 
 
 def tiles_roofline(per, st, args, peaks):
@@ -262,9 +264,11 @@ def tiles_roofline(per, st, args, peaks):
     achieved = flops / sec / 1e12
     peak = peaks.get("bf16_tflops_sustained") or 1400.0
     padded = 2.0 * tile_pairs * 128 * 256 * 64 / L / sec / 1e12
-    traffic = (TILE_DRAM_BYTES_PER_PAIR * tile_pairs / L
-               if TILE_DRAM_BYTES_PER_PAIR is not None else None)
-    return {"bound": "tensor", "kernel": "k_ivf_tiles", "achieved": achieved, "peak": peak,
+    # BF16 tiles with 16-entry shortlists (k <= 15) run the wide kernel
+    kernel = ("k_ivf_wide" if args.form in ("bf16", "learned") and args.k <= 15
+              else "k_ivf_tiles")
+    traffic = TILE_DRAM_BYTES_PER_PAIR[kernel] * tile_pairs / L
+    return {"bound": "tensor", "kernel": kernel, "achieved": achieved, "peak": peak,
             "unit": "TFLOP/s", "frac": achieved / peak, "traffic": traffic,
             "padded_tflops": padded, "launches_per_build": L,
             "peak_source": ("measured sustained bf16" if "bf16_tflops_sustained" in peaks

@@ -1400,8 +1400,7 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     float* rdist = c->get<float>("list_dist", size_t(n) * k);
     // the exact re-rank list: 2k candidates ("2k-4k shortlist"), at most 64
     // (E4M3: 4k, the wider end of the 2k-4k range, for its cruder ranking)
-    int R = std::min(P * Sout, std::min(64, std::max(fp8 ? 4 * k : 2 * k, k + 1)));
-    if (const char* e = std::getenv("POLARISEQ_RERANK_R")) R = std::max(k + 1, std::min(R, std::atoi(e)));
+    const int R = std::min(P * Sout, std::min(64, std::max(fp8 ? 4 * k : 2 * k, k + 1)));
     if (k > 63) throw DeviceError{"the tensor-core form supports k <= 63"};
     ck(cudaMemsetAsync(c->d_acc, 0, 16, st), "acc");
     // auto: no polish round for BF16; for E4M3 one below 2^20 cells (with few

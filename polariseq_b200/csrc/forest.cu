@@ -329,6 +329,22 @@ __device__ __forceinline__ void draw_pair(Rng& r, uint32_t n, uint32_t& pa, uint
     }
 }
 
+// draw_pair with the next two Rng states already computed (la1 =
+// splitmix(r.s), la2 = splitmix(la1)), for n < 2^16; the caller recomputes the
+// look-ahead after every other draw, off the critical path.
+__device__ __forceinline__ void draw_pair_la(Rng& r, uint64_t la1, uint64_t la2, uint32_t n,
+                                             uint32_t& pa, uint32_t& pb) {
+    const uint32_t t32 = (0xFFFFFFFFu % n + 1u) % n;
+    pa = mod_u64_small(la1, n, t32);
+    pb = mod_u64_small(la2, n, t32);
+    r.s = la2;
+    int tries = 0;
+    while (pb == pa && tries < 8) {
+        pb = mod_u64_small(r.next_u64(), n, t32);
+        ++tries;
+    }
+}
+
 // Warp 0 finishes a staged subtree: local positions [0, n0) of the staged
 // ids/slots, rows in `rows` (slot-indexed), normal in `nv`.
 template <int D>
@@ -348,6 +364,8 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
     };
     const int d = a.d, dp = a.dp;
     const unsigned lt = (1u << lane) - 1u;
+    // the next two Rng states, computed while the previous split works
+    uint64_t la1 = splitmix(rng.s), la2 = splitmix(la1);
     int lsp = 1;
     if (lane == 0) {
         S.lS[0] = 0;
@@ -367,7 +385,9 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
         if (a.trace && lane == 0) atomicAdd(&a.trace[SEQ_T_STAGED_NODES], 1ull);
         ++nodes;
         uint32_t pa, pb;
-        draw_pair(rng, ln, pa, pb);
+        draw_pair_la(rng, la1, la2, ln, pa, pb);
+        la1 = splitmix(rng.s);
+        la2 = splitmix(la1);
         phase(SEQ_T_W_DRAW);
         const float* xa = rows + size_t(sslot[ls + pa]) * dp;
         const float* xb = rows + size_t(sslot[ls + pb]) * dp;
@@ -375,16 +395,23 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
         __syncwarp();
         // margins of the positions this lane owns (lane + 32*i): the offset's
         // sequential sum and the dot products are independent chains, issued
-        // together (the dots stay in registers; groups past the node's size
-        // are skipped by the whole warp)
+        // together: the first two groups always (a position past the node
+        // reads its last row, whose product is ignored), the next two only
+        // for nodes above 64 points
         const float off = hyper_offset_t<D>(xa, xb, d);
         float dots[SCAP / 32];
+        const uint32_t last = ln - 1;
 #pragma unroll
-        for (int i = 0; i < SCAP / 32; ++i) {
-            dots[i] = 0.f;
-            if (32u * i < ln) {
-                const uint32_t p = lane + 32 * i;
-                if (p < ln) dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
+        for (int i = 0; i < 2; ++i) {
+            const uint32_t p = min(uint32_t(lane + 32 * i), last);
+            dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
+        }
+        dots[2] = dots[3] = 0.f;
+        if (ln > 64u) {
+#pragma unroll
+            for (int i = 2; i < SCAP / 32; ++i) {
+                const uint32_t p = min(uint32_t(lane + 32 * i), last);
+                dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
             }
         }
         // sides in registers; through shared memory only when a tie draws
@@ -422,6 +449,8 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
                 const uint32_t p = lane + 32 * i;
                 if (p < ln) code[i] = S.code[p];
             }
+            la1 = splitmix(rng.s);  // the tie draws moved the Rng on
+            la2 = splitmix(la1);
         }
         phase(SEQ_T_W_MARGIN);
         unsigned mask[SCAP / 32];
@@ -496,6 +525,8 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
                 __syncwarp();
             }
             split = ln / 2;
+            la1 = splitmix(rng.s);  // the random split moved the Rng on
+            la2 = splitmix(la1);
         }
         if (lsp + 2 > STK) {
             if (lane == 0) atomicExch(a.err, 1);

@@ -39,6 +39,10 @@
 // ascending runs of S (and, when asked, the number of finite entries of each
 // run).
 //
+// BF16 launches with 16-entry shortlists run k_ivf_wide (further down), the
+// same scheme with jobs of 256 query entries, 128-candidate tiles and 16
+// epilogue warps.
+//
 // Every wait is bounded: a wait that gives up raises the CTA's abort flag,
 // every role leaves its loop, in-flight copies and MMAs are waited for (again
 // bounded), TMEM is freed and the kernel reports error 2.

@@ -31,8 +31,13 @@ def check_structure(g, n, k):
     assert (np.diff(dx.reshape(n, k), axis=1) >= 0).all(), "not sorted"
 
 
+@pytest.mark.parametrize("wide", ["1", "0"])
 @pytest.mark.parametrize("n,comps", [(20_000, 20), (120_000, 40)])
-def test_bf16_form_recall_and_structure(n, comps):
+def test_bf16_form_recall_and_structure(n, comps, wide, monkeypatch):
+    """Both tile kernels of the 16-entry shortlists: the wide one (jobs of 256
+    query entries, 128-candidate tiles, 16 epilogue warps; the default) and
+    the standard one (128 entries, 256-candidate tiles)."""
+    monkeypatch.setenv("POLARISEQ_TILES_WIDE", wide)
     x = synth.mixture_lognormal(n, 50, comps, seed=5)
     g = pq.nndescent_dense(x, 15, mode="bf16")
     check_structure(g, n, 15)
