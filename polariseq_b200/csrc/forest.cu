@@ -329,6 +329,56 @@ __device__ __forceinline__ void draw_pair(Rng& r, uint32_t n, uint32_t& pa, uint
     }
 }
 
+// The normal nv = xa - xb in registers and the hyperplane offset in one pass
+// over the two rows (16-byte loads), in hyper_offset_t's sequential order.
+template <int D>
+__device__ __forceinline__ float normal_offset_reg(const float* __restrict__ xa,
+                                                   const float* __restrict__ xb, float (&nvr)[D]) {
+    float s = -0.0f;
+    const float4* a4 = reinterpret_cast<const float4*>(xa);
+    const float4* b4 = reinterpret_cast<const float4*>(xb);
+#pragma unroll
+    for (int q = 0; q < D / 4; ++q) {
+        const float4 x = a4[q], y = b4[q];
+        const float av[4] = {x.x, x.y, x.z, x.w}, bv[4] = {y.x, y.y, y.z, y.w};
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const float t = __fsub_rn(av[u], bv[u]);
+            nvr[4 * q + u] = t;
+            s = __fadd_rn(s, __fmul_rn(__fmul_rn(t, 0.5f), __fadd_rn(av[u], bv[u])));
+        }
+    }
+#pragma unroll
+    for (int j = D / 4 * 4; j < D; ++j) {
+        const float t = __fsub_rn(xa[j], xb[j]);
+        nvr[j] = t;
+        s = __fadd_rn(s, __fmul_rn(__fmul_rn(t, 0.5f), __fadd_rn(xa[j], xb[j])));
+    }
+    return -s;
+}
+
+// dot_exact_t<D>(nv, x) with the normal in registers (the same lanes, order
+// and rounding; a product is the same either way round).
+template <int D>
+__device__ __forceinline__ float dot_reg(const float (&nvr)[D], const float* __restrict__ x) {
+    constexpr int FULL = D / 8;
+    float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    const float4* x4 = reinterpret_cast<const float4*>(x);
+#pragma unroll
+    for (int c = 0; c < FULL; ++c) {
+        const float4 y0 = x4[2 * c], y1 = x4[2 * c + 1];
+        const float y[8] = {y0.x, y0.y, y0.z, y0.w, y1.x, y1.y, y1.z, y1.w};
+#pragma unroll
+        for (int l = 0; l < 8; ++l) acc[l] = __fadd_rn(acc[l], __fmul_rn(nvr[8 * c + l], y[l]));
+    }
+    float tail = 0.0f;
+#pragma unroll
+    for (int j = FULL * 8; j < D; ++j) tail = __fadd_rn(tail, __fmul_rn(nvr[j], x[j]));
+    const float r = __fadd_rn(__fadd_rn(__fadd_rn(acc[0], acc[4]), __fadd_rn(acc[1], acc[5])),
+                              __fadd_rn(__fadd_rn(acc[2], acc[6]), __fadd_rn(acc[3], acc[7])));
+    return __fadd_rn(r, tail);
+}
+
 // draw_pair with the next two Rng states already computed (la1 =
 // splitmix(r.s), la2 = splitmix(la1)), for n < 2^16; the caller recomputes the
 // look-ahead after every other draw, off the critical path.
@@ -391,27 +441,48 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
         phase(SEQ_T_W_DRAW);
         const float* xa = rows + size_t(sslot[ls + pa]) * dp;
         const float* xb = rows + size_t(sslot[ls + pb]) * dp;
-        for (int j = lane; j < dp; j += 32) nv[j] = j < d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
-        __syncwarp();
         // margins of the positions this lane owns (lane + 32*i): the offset's
         // sequential sum and the dot products are independent chains, issued
         // together: the first two groups always (a position past the node
         // reads its last row, whose product is ignored), the next two only
         // for nodes above 64 points
-        const float off = hyper_offset_t<D>(xa, xb, d);
         float dots[SCAP / 32];
+        float off;
         const uint32_t last = ln - 1;
+        if constexpr (D > 0) {
+            // every lane holds the normal in registers (no shared-memory round
+            // trip), built in the same pass as the offset
+            float nvr[D];
+            off = normal_offset_reg<D>(xa, xb, nvr);
 #pragma unroll
-        for (int i = 0; i < 2; ++i) {
-            const uint32_t p = min(uint32_t(lane + 32 * i), last);
-            dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
-        }
-        dots[2] = dots[3] = 0.f;
-        if (ln > 64u) {
+            for (int i = 0; i < 2; ++i) {
+                const uint32_t p = min(uint32_t(lane + 32 * i), last);
+                dots[i] = dot_reg<D>(nvr, rows + size_t(sslot[ls + p]) * dp);
+            }
+            dots[2] = dots[3] = 0.f;
+            if (ln > 64u) {
 #pragma unroll
-            for (int i = 2; i < SCAP / 32; ++i) {
+                for (int i = 2; i < SCAP / 32; ++i) {
+                    const uint32_t p = min(uint32_t(lane + 32 * i), last);
+                    dots[i] = dot_reg<D>(nvr, rows + size_t(sslot[ls + p]) * dp);
+                }
+            }
+        } else {
+            for (int j = lane; j < dp; j += 32) nv[j] = j < d ? __fsub_rn(xa[j], xb[j]) : 0.0f;
+            __syncwarp();
+            off = hyper_offset_t<D>(xa, xb, d);
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
                 const uint32_t p = min(uint32_t(lane + 32 * i), last);
                 dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
+            }
+            dots[2] = dots[3] = 0.f;
+            if (ln > 64u) {
+#pragma unroll
+                for (int i = 2; i < SCAP / 32; ++i) {
+                    const uint32_t p = min(uint32_t(lane + 32 * i), last);
+                    dots[i] = dot_exact_t<D>(nv, rows + size_t(sslot[ls + p]) * dp, d);
+                }
             }
         }
         // sides in registers; through shared memory only when a tie draws
