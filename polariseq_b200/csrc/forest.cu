@@ -524,18 +524,30 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
             la2 = splitmix(la1);
         }
         phase(SEQ_T_W_MARGIN);
+        // groups of 32 positions past the node's size are skipped by the whole
+        // warp; the ids and slots this lane moves are read ahead of the tables
         unsigned mask[SCAP / 32];
+        uint32_t mid[SCAP / 32], msl[SCAP / 32];
         uint32_t nL = 0;
 #pragma unroll
         for (int i = 0; i < SCAP / 32; ++i) {
             const uint32_t p = lane + 32 * i;
-            mask[i] = __ballot_sync(0xFFFFFFFFu, p < ln && code[i] == 1);
-            nL += __popc(mask[i]);
+            mask[i] = 0;
+            mid[i] = msl[i] = 0;
+            if (32u * i < ln) {
+                mask[i] = __ballot_sync(0xFFFFFFFFu, p < ln && code[i] == 1);
+                nL += __popc(mask[i]);
+                if (p < ln) {
+                    mid[i] = sid[ls + p];
+                    msl[i] = sslot[ls + p];
+                }
+            }
         }
         uint32_t c = 0;
         uint32_t pre = 0;
 #pragma unroll
         for (int i = 0; i < SCAP / 32; ++i) {
+            if (32u * i >= ln) break;
             const uint32_t p = lane + 32 * i;
             const uint32_t lp = pre + __popc(mask[i] & lt);
             const bool isL = (mask[i] >> lane) & 1u;
@@ -555,6 +567,7 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
         pre = 0;
 #pragma unroll
         for (int i = 0; i < SCAP / 32; ++i) {
+            if (32u * i >= ln) break;
             const uint32_t p = lane + 32 * i;
             const uint32_t lp = pre + __popc(mask[i] & lt);
             const bool isL = (mask[i] >> lane) & 1u;
@@ -570,8 +583,8 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
                 } else {
                     dst = (c == 0 ? ln : S.tabB[c - 1]) - 1;
                 }
-                S.sid2[dst] = sid[ls + p];
-                S.sslot2[dst] = sslot[ls + p];
+                S.sid2[dst] = mid[i];
+                S.sslot2[dst] = msl[i];
             }
             pre += __popc(mask[i]);
         }
