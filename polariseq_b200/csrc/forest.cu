@@ -673,8 +673,8 @@ __device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids,
     }
     uint32_t cnt = 0;
     bool tie = false;
-    // margins: each thread reads its rows directly, U in flight
     {
+        // margins: each thread reads its rows directly, U in flight
         constexpr int U = NT >= 512 ? 2 : 4;  // rows in flight per thread
         for (uint32_t p0 = tid; p0 < sz; p0 += U * NT) {
             uint32_t id[U];
@@ -1147,16 +1147,19 @@ __global__ void k_leaf_scatter(const uint8_t* f, const uint32_t* pre, uint32_t n
 // members' heap rows in shared memory once (the heap rows column-major, one
 // column per position, so that the pushes of a warp hit distinct banks),
 // computes each pair's distance once into a per-position table, and then each
-// thread replays its own member's pushes on the staged row and writes the row
-// back if it changed.  A push whose distance is not below the row's root (its
+// thread replays its own member's pushes on the staged row; the changed rows
+// go back.  The heap rows move between global and shared memory in position x
+// slot order (consecutive threads on one row's slots: coalesced), the staged
+// columns LCAP + 1 apart so that those accesses spread over the banks.  A push whose distance is not below the row's root (its
 // current worst) is rejected unchanged (nndescent.rs:176).  Tiles whose span
 // exceeds LCAP or whose leaves exceed LMAX members take the direct path.
 constexpr int LPB = 8;      // leaves per CTA, at most
 constexpr int LCAP = 128;   // staged positions per CTA (= threads)
 constexpr int LMAXC = 64;   // largest leaf of the staged path
+constexpr int HS = LCAP + 1;  // column stride of the staged heap rows
 
 size_t leaf_pairs_smem(int dp, int lmax, int k) {
-    return size_t(LCAP) * dp * 4 + size_t(LCAP) * lmax * 4 + size_t(LCAP) * k * 9;
+    return size_t(LCAP) * dp * 4 + size_t(LCAP) * lmax * 4 + size_t(HS) * k * 9;
 }
 
 template <int D>
@@ -1169,10 +1172,11 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
     __shared__ int staged;
     float* R = lsm;                               // LCAP * dp
     float* Dt = lsm + size_t(LCAP) * dp;          // LCAP * LMAX (LMAX: 16 or 32)
-    uint32_t* hI = reinterpret_cast<uint32_t*>(Dt + size_t(LCAP) * LMAX);  // k x LCAP
-    float* hD = reinterpret_cast<float*>(hI + size_t(k) * LCAP);           // k x LCAP
-    uint8_t* hF = reinterpret_cast<uint8_t*>(hD + size_t(k) * LCAP);       // k x LCAP
+    uint32_t* hI = reinterpret_cast<uint32_t*>(Dt + size_t(LCAP) * LMAX);  // k x HS
+    float* hD = reinterpret_cast<float*>(hI + size_t(k) * HS);             // k x HS
+    uint8_t* hF = reinterpret_cast<uint8_t*>(hD + size_t(k) * HS);         // k x HS
     __shared__ uint32_t sid[LCAP];
+    __shared__ uint8_t chg[LCAP];  // the staged heap row changed
     __shared__ uint16_t sl0[LCAP], sl1[LCAP];     // leaf bounds of each staged position
     const uint32_t L0 = blockIdx.x * uint32_t(lpb);
     const uint32_t L1 = min(nleaves, L0 + uint32_t(lpb));
@@ -1223,13 +1227,12 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
         const uint32_t r = t / q4, j = t - r * q4;
         reinterpret_cast<float4*>(R)[t] = reinterpret_cast<const float4*>(X + size_t(sid[r]) * dp)[j];
     }
-    if (own) {
-        const size_t hb = size_t(p) * k;
-        for (int s = 0; s < k; ++s) {
-            hI[s * LCAP + tid] = hidx[hb + s];
-            hD[s * LCAP + tid] = hdist[hb + s];
-            hF[s * LCAP + tid] = hflag[hb + s];
-        }
+    for (uint32_t t = tid; t < span * uint32_t(k); t += LCAP) {
+        const uint32_t r = t / uint32_t(k), sl = t - r * uint32_t(k);
+        const size_t g = size_t(sid[r]) * k + sl;
+        hI[sl * HS + r] = hidx[g];
+        hD[sl * HS + r] = hdist[g];
+        hF[sl * HS + r] = hflag[g];
     }
     __syncthreads();
     if (own) {  // each pair once: this position with its later mates
@@ -1251,16 +1254,18 @@ __global__ void __launch_bounds__(LCAP) k_leaf_pairs(
             if (j == uint32_t(tid)) continue;
             const float dd = Dt[size_t(tid) * LMAX + (j - l0)];
             if (dd >= rd[0]) continue;  // heap_push would reject it unchanged
-            changed |= heap_push_strided(ri, rd, rf, k, LCAP, sid[j], dd, 1);
+            changed |= heap_push_strided(ri, rd, rf, k, HS, sid[j], dd, 1);
         }
-        if (changed) {
-            const size_t hb = size_t(p) * k;
-            for (int s = 0; s < k; ++s) {
-                hidx[hb + s] = ri[s * LCAP];
-                hdist[hb + s] = rd[s * LCAP];
-                hflag[hb + s] = rf[s * LCAP];
-            }
-        }
+        chg[tid] = changed ? 1 : 0;
+    }
+    __syncthreads();
+    for (uint32_t t = tid; t < span * uint32_t(k); t += LCAP) {
+        const uint32_t r = t / uint32_t(k), sl = t - r * uint32_t(k);
+        if (!chg[r]) continue;
+        const size_t g = size_t(sid[r]) * k + sl;
+        hidx[g] = hI[sl * HS + r];
+        hdist[g] = hD[sl * HS + r];
+        hflag[g] = hF[sl * HS + r];
     }
 }
 
