@@ -149,6 +149,28 @@ float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, in
     return X;
 }
 
+float* load_embedding_rows(pq_ctx* c, const float* data, uint32_t n, int d, int dp, uint32_t r0,
+                           uint32_t r1, cudaStream_t st) {
+    float* X = c->get<float>("X", size_t(n) * dp);
+    if (r1 <= r0) return X;
+    const size_t rows = r1 - r0;
+    if (dp == d) {
+        ck(cudaMemcpyAsync(X + size_t(r0) * dp, data + size_t(r0) * d, rows * d * sizeof(float),
+                           cudaMemcpyHostToDevice, st),
+           "copy embedding");
+        return X;
+    }
+    float* stage = c->get<float>("X_stage", size_t(n) * d);
+    ck(cudaMemcpyAsync(stage + size_t(r0) * d, data + size_t(r0) * d, rows * d * sizeof(float),
+                       cudaMemcpyHostToDevice, st),
+       "copy embedding");
+    k_pad_rows<<<blocks(rows * dp, 256), 256, 0, st>>>(stage + size_t(r0) * d, rows, d, dp,
+                                                        X + size_t(r0) * dp);
+    pq::count_launch();
+    ck(cudaGetLastError(), "pad embedding");
+    return X;
+}
+
 // The records of source rows [a, b) (offsets row_off[a..b) local to the
 // chunk, `total` of them): written in generation order, sorted stably by
 // destination and replayed into the heaps.  `rows` lists the chunk's rows in

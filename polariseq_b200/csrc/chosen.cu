@@ -908,19 +908,15 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     tot.start();
     const unsigned long long launches0 = g_launches;
 
-    // host data: the k-means sample (a strided set of rows) is copied first
-    // and the whole embedding follows on the second stream while k-means
-    // runs; the first use of all rows waits for it
-    EventSet xev(2);
-    float* X = nullptr;
-    if (data_on_host) {
-        ck(cudaEventRecord(xev.ev[0], st), "event");
-        ck(cudaStreamWaitEvent(c->stream2, xev.ev[0], 0), "event");
-        X = load_embedding(c, data, true, n, d, dp, c->stream2);
-        ck(cudaEventRecord(xev.ev[1], c->stream2), "event");
-    } else {
-        X = load_embedding(c, data, false, n, d, dp);
-    }
+    // host data: the k-means sample (blocks of rows) is copied first; the
+    // whole embedding follows on the second stream in XCH row chunks, one
+    // event each, while k-means runs, and each chunk's cells are assigned to
+    // their centroids as soon as the chunk has landed
+    constexpr int XCH = 8;
+    EventSet xev(data_on_host ? XCH + 1 : 0);
+    auto xrow = [&](int i) { return uint32_t(uint64_t(n) * uint32_t(i) / XCH); };
+    float* X = data_on_host ? c->get<float>("X", size_t(n) * dp)
+                            : load_embedding(c, data, false, n, d, dp);
 
     // ── 1. buckets ──
     tm.start();
@@ -969,6 +965,13 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
         ck(cudaMemcpy2DAsync(xraw, run, data, all_rows ? run : size_t(s_stride) * d * 4, run,
                              all_rows ? 1 : KB, cudaMemcpyHostToDevice, st),
            "copy sample");
+        // the embedding's chunks start once the sample is across
+        ck(cudaEventRecord(xev.ev[0], st), "event");
+        ck(cudaStreamWaitEvent(c->stream2, xev.ev[0], 0), "event");
+        for (int i = 0; i < XCH; ++i) {
+            load_embedding_rows(c, data, n, d, dp, xrow(i), xrow(i + 1), c->stream2);
+            ck(cudaEventRecord(xev.ev[i + 1], c->stream2), "event");
+        }
         k_pad_cols<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(xraw, ns, d, dp, xs); count_launch();
     } else {
         k_block_rows<<<blocks(size_t(ns) * dp, 256), 256, 0, st>>>(X, dp, s_stride, bl, ns, xs);
@@ -1068,20 +1071,36 @@ uint64_t build_chosen(pq_ctx* c, const float* data, bool data_on_host, uint64_t 
     }
     k_to_bf16<<<cvt_blocks(C), 256, 0, st>>>(cent, d, dp, nullptr, zeros, mean, C, 2, cb, cbn); count_launch();
     // every cell's P nearest centroids, ascending; the first is its primary bucket
-    if (data_on_host) ck(cudaStreamWaitEvent(st, xev.ev[1], 0), "event");
     __nv_bfloat16* qa = c->get<__nv_bfloat16>("assign_q", size_t(n) * 64);
     float* qan = c->get<float>("assign_qn", n);
-    k_to_bf16<<<cvt_blocks(n), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan); count_launch();
     uint32_t* probes = c->get<uint32_t>("probes", size_t(n) * P);
     float* probe_d = c->get<float>("probe_d", size_t(n) * P);
     double ms_train = 0.0, ms_route = 0.0;
+    if (!learned && data_on_host) {
+        // chunk by chunk as the embedding lands
+        for (int i = 0; i < XCH; ++i) {
+            const uint32_t r0 = xrow(i), r1 = xrow(i + 1);
+            ck(cudaStreamWaitEvent(st, xev.ev[i + 1], 0), "event");
+            if (r1 <= r0) continue;
+            k_to_bf16<<<cvt_blocks(r1 - r0), 256, 0, st>>>(X + size_t(r0) * dp, d, dp, nullptr,
+                                                           zeros, mean, r1 - r0, 1,
+                                                           qa + size_t(r0) * 64, qan + r0);
+            count_launch();
+            centroid_search(qa + size_t(r0) * 64, qan + r0, r1 - r0, P,
+                            probe_d + size_t(r0) * P, probes + size_t(r0) * P);
+        }
+    } else {
+        if (data_on_host) ck(cudaStreamWaitEvent(st, xev.ev[XCH], 0), "event");
+        k_to_bf16<<<cvt_blocks(n), 256, 0, st>>>(X, d, dp, nullptr, zeros, mean, n, 1, qa, qan);
+        count_launch();
+    }
     if (learned) {  // own bucket by k-means, the other probes from the MLP
         uint32_t* prim = c->get<uint32_t>("primary", n);
         float* prim_d = c->get<float>("primary_d", n);
         centroid_search(qa, qan, n, 1, prim_d, prim);
         ms_route = learned_probes(c, X, d, dp, n, C, prim, prim_d, cent, P, o.seed, probes,
                                   &ms_train, &S_.learn_loss_first, &S_.learn_loss_last);
-    } else {
+    } else if (!data_on_host) {
         centroid_search(qa, qan, n, P, probe_d, probes);
     }
     int herr0 = 0;

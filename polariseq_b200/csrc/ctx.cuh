@@ -185,6 +185,10 @@ inline void kg_collect(pq_ctx* c) {
 // stream st (null: the context's stream) (api.cu).
 float* load_embedding(pq_ctx* c, const float* data, bool on_host, uint32_t n, int d, int dp,
                       cudaStream_t st = nullptr);
+// Host rows [r0, r1) of the caller's n x d embedding into the padded rows X
+// (the same workspace as load_embedding), on stream st; returns X.
+float* load_embedding_rows(pq_ctx* c, const float* data, uint32_t n, int d, int dp, uint32_t r0,
+                           uint32_t r1, cudaStream_t st);
 
 // NN-Descent rounds on heaps in place (api.cu).
 int run_rounds(pq_ctx* c, const float* X, int d, int dp, uint32_t n, int k, int m, uint64_t seed,
