@@ -207,38 +207,64 @@ __global__ void k_probe_dist(const float* __restrict__ xp, const uint32_t* __res
                              const float* __restrict__ cent, const float* __restrict__ un,
                              float* __restrict__ dist, unsigned* __restrict__ rad2,
                              unsigned* __restrict__ umax2) {
-    const uint32_t p = blockIdx.x * (blockDim.x / 32) + (threadIdx.x >> 5);
-    if (p >= n) return;
-    const uint32_t i = perm[p];
+    // one warp per candidate position; the block's 8 positions are
+    // consecutive, mostly of one bucket, so the bucket maxima are reduced in
+    // the block first and each run of equal buckets does one atomic pair
+    __shared__ uint32_t sb[8];
+    __shared__ unsigned sr[8], su[8];
+    const int w = threadIdx.x >> 5;
+    const uint32_t p = blockIdx.x * (blockDim.x / 32) + w;
+    const bool valid = p < n;
     const int lane = threadIdx.x & 31, h = lane & 15, half = lane >> 4;
     const unsigned hm = 0xFFFFu << (lane & 16);
-    float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (4 * h < dp) x4 = reinterpret_cast<const float4*>(xp + size_t(p) * dp)[h];
-    const float xs[4] = {x4.x, x4.y, x4.z, x4.w};
-    // both halves run the same number of rounds (the shuffles need their lanes)
-    for (int r0 = 0; r0 < P; r0 += 2) {
-        const int r = r0 + half;
-        const bool live = r < P;
-        const uint32_t c = live ? probes[size_t(i) * P + r] : 0u;
-        float s = 0.f;
-        if (live && 4 * h < dp) {
-            const float4 c4 = reinterpret_cast<const float4*>(cent + size_t(c) * dp)[h];
-            const float cs[4] = {c4.x, c4.y, c4.z, c4.w};
+    if (valid) {
+        const uint32_t i = perm[p];
+        // every probe id at once (P <= 16), each round takes its two by shuffle
+        const uint32_t pr = lane < P ? probes[size_t(i) * P + lane] : 0u;
+        float4 x4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (4 * h < dp) x4 = reinterpret_cast<const float4*>(xp + size_t(p) * dp)[h];
+        const float xs[4] = {x4.x, x4.y, x4.z, x4.w};
+        // both halves run the same number of rounds (the shuffles need their lanes)
+        for (int r0 = 0; r0 < P; r0 += 2) {
+            const int r = r0 + half;
+            const bool live = r < P;
+            const uint32_t c = __shfl_sync(0xFFFFFFFFu, pr, live ? r : 0);
+            float s = 0.f;
+            if (live && 4 * h < dp) {
+                const float4 c4 = reinterpret_cast<const float4*>(cent + size_t(c) * dp)[h];
+                const float cs[4] = {c4.x, c4.y, c4.z, c4.w};
 #pragma unroll
-            for (int u = 0; u < 4; ++u)
-                if (4 * h + u < d) {
-                    const float df = xs[u] - cs[u];
-                    s = fmaf(df, df, s);
-                }
-        }
-#pragma unroll
-        for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(hm, s, o);
-        if (live && h == 0) {
-            dist[size_t(p) * P + r] = s;
-            if (r == 0) {
-                atomicMax(&rad2[c], __float_as_uint(s));
-                atomicMax(&umax2[c], __float_as_uint(un[i]));
+                for (int u = 0; u < 4; ++u)
+                    if (4 * h + u < d) {
+                        const float df = xs[u] - cs[u];
+                        s = fmaf(df, df, s);
+                    }
             }
+#pragma unroll
+            for (int o = 8; o > 0; o >>= 1) s += __shfl_xor_sync(hm, s, o);
+            if (live && h == 0) {
+                dist[size_t(p) * P + r] = s;
+                if (r == 0 && lane == 0) {
+                    sb[w] = c;
+                    sr[w] = __float_as_uint(s);
+                    su[w] = __float_as_uint(un[i]);
+                }
+            }
+        }
+    }
+    __syncthreads();
+    // one atomic pair per run of equal buckets among the block's positions
+    if (threadIdx.x < 8) {
+        const int t = threadIdx.x;
+        const uint32_t nv = min(8u, n > blockIdx.x * 8u ? n - blockIdx.x * 8u : 0u);
+        if (uint32_t(t) < nv && (t == 0 || sb[t] != sb[t - 1])) {
+            unsigned mr = sr[t], mu = su[t];
+            for (uint32_t q = t + 1; q < nv && sb[q] == sb[t]; ++q) {
+                mr = max(mr, sr[q]);
+                mu = max(mu, su[q]);
+            }
+            atomicMax(&rad2[sb[t]], mr);
+            atomicMax(&umax2[sb[t]], mu);
         }
     }
 }
@@ -649,23 +675,30 @@ __global__ void __launch_bounds__(128) k_rerank(
         slot[lane] = ~0ull;
         slot[lane + 32] = ~0ull;
         __syncwarp();
-        float4 v4[8];
-        uint4 i4[8];
+        // RS / 4 lanes per run (16 bytes each), 128 / RS runs per pass: each
+        // load touches a few cache lines rather than one per lane
+        const int nruns = P * NR;
+        const int lpr = RS / 4, rpp = 32 / lpr;
+        for (int r0 = 0; r0 < nruns; r0 += rpp) {
+            const int r = r0 + lane / lpr, c = lane % lpr;
+            const uint32_t blo = __shfl_sync(0xFFFFFFFFu, uint32_t(base), r & 31);
+            const uint32_t bhi = __shfl_sync(0xFFFFFFFFu, uint32_t(base >> 32), r & 31);
+            const int fr = __shfl_sync(0xFFFFFFFFu, fin, r & 31);
+            const int orr = __shfl_sync(0xFFFFFFFFu, off, r & 31);
+            if (r < nruns) {
+                const size_t br = (size_t(bhi) << 32) | blo;
+                for (int q = c; 4 * q < fr; q += lpr) {
+                    const float4 v4 = *reinterpret_cast<const float4*>(sd + br + 4 * q);
+                    const uint4 i4 = *reinterpret_cast<const uint4*>(si + br + 4 * q);
+                    const float vv[4] = {v4.x, v4.y, v4.z, v4.w};
+                    const uint32_t ii[4] = {i4.x, i4.y, i4.z, i4.w};
 #pragma unroll
-        for (int q = 0; q < 8; ++q)
-            if (4 * q < fin) {
-                v4[q] = *reinterpret_cast<const float4*>(sd + base + 4 * q);
-                i4[q] = *reinterpret_cast<const uint4*>(si + base + 4 * q);
+                    for (int t = 0; t < 4; ++t)
+                        if (4 * q + t < fr)
+                            slot[orr + 4 * q + t] =
+                                (uint64_t(__float_as_uint(fmaxf(vv[t], 0.0f))) << 32) | ii[t];
+                }
             }
-#pragma unroll
-        for (int q = 0; q < 8; ++q) {
-            const float vv[4] = {v4[q].x, v4[q].y, v4[q].z, v4[q].w};
-            const uint32_t ii[4] = {i4[q].x, i4[q].y, i4[q].z, i4[q].w};
-#pragma unroll
-            for (int t = 0; t < 4; ++t)
-                if (4 * q + t < fin)
-                    slot[off + 4 * q + t] =
-                        (uint64_t(__float_as_uint(fmaxf(vv[t], 0.0f))) << 32) | ii[t];
         }
         __syncwarp();
         uint64_t key[2] = {slot[lane], slot[lane + 32]};
@@ -706,13 +739,15 @@ __global__ void __launch_bounds__(128) k_rerank(
     //    (rows from the candidate-ordered copy: this cell is position wg)
     const float* xi = xp + size_t(wg) * dp;
     uint64_t key[2];
+    {
 #pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        key[h] = ~0ull;
-        if (cand[h] != 0xFFFFFFFFu) {
-            const uint32_t j = perm[cand[h]];
-            const float dd = sq_dist_exact_t<D>(xi, xp + size_t(cand[h]) * dp, d);
-            key[h] = (uint64_t(__float_as_uint(dd)) << 32) | j;
+        for (int h = 0; h < 2; ++h) {
+            key[h] = ~0ull;
+            if (cand[h] != 0xFFFFFFFFu) {
+                const uint32_t j = perm[cand[h]];
+                const float dd = sq_dist_exact_t<D>(xi, xp + size_t(cand[h]) * dp, d);
+                key[h] = (uint64_t(__float_as_uint(dd)) << 32) | j;
+            }
         }
     }
     // 3. sort by (distance, index): non-negative floats order as their bits
