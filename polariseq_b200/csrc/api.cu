@@ -504,6 +504,23 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
                      "%llu partition %llu cycles\n",
                      h[SEQ_T_W_LEAF], h[SEQ_T_W_DRAW], h[SEQ_T_W_MARGIN], h[SEQ_T_W_PART],
                      h[SEQ_T_M_STAGE], h[SEQ_T_M_DRAW], h[SEQ_T_M_MARGIN], h[SEQ_T_M_PART]);
+        // timeline of the two subtree kernels (globaltimer): each large root's
+        // CTA against the span of the 128-thread kernel
+        uint32_t nb = 0;
+        while (nb < roots.size() && nb < 148 && roots[nb].size > 65536) ++nb;
+        unsigned long long t0 = ~h[SEQ_T_SMALL_T0], t1s = h[SEQ_T_SMALL_T1];
+        for (uint32_t b = 0; b < nb && b < uint32_t(SEQ_T_BIG_N); ++b)
+            t0 = std::min(t0, h[SEQ_T_BIG + 2 * b]);
+        std::fprintf(stderr,
+                     "[nndescent]   subtree timeline: %u roots above 65536 points, %zu below; "
+                     "128-thread kernel ends at %.2f ms\n",
+                     nb, roots.size() - nb, (t1s - t0) * 1e-6);
+        for (uint32_t b = 0; b < nb && b < uint32_t(SEQ_T_BIG_N); ++b) {
+            if (b >= 24 && b % 16 != 0 && b + 1 != nb) continue;
+            std::fprintf(stderr, "[nndescent]     root %u: %u points, %.2f .. %.2f ms\n", b,
+                         roots[b].size, (h[SEQ_T_BIG + 2 * b] - t0) * 1e-6,
+                         (h[SEQ_T_BIG + 2 * b + 1] - t0) * 1e-6);
+        }
     }
     if (herr) throw DeviceError{"forest: a subtree exceeded the depth-first stack"};
 

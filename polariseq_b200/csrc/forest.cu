@@ -285,6 +285,13 @@ struct SeqShared {
     int sp, anytie;
 };
 
+// The global nanosecond timer (comparable across SMs; trace only).
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+    return t;
+}
+
 // 16-byte asynchronous global -> shared copies (both addresses 16-byte
 // aligned), bypassing L1.
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -379,18 +386,34 @@ __device__ __forceinline__ float dot_reg(const float (&nvr)[D], const float* __r
     return __fadd_rn(r, tail);
 }
 
+// x mod n for a 32-bit x from m = floor((2^32 - 1) / n): m >= (2^32 - n) / n,
+// so q = floor(x m / 2^32) > x / n - 2, i.e. q is floor(x / n) or one below,
+// and one conditional subtraction of n finishes the remainder.
+__device__ __forceinline__ uint32_t mod_magic(uint32_t x, uint32_t n, uint32_t m) {
+    const uint32_t r = x - __umulhi(x, m) * n;
+    return r >= n ? r - n : r;
+}
+// mod_u64_small with the node's one division shared by all its draws.
+__device__ __forceinline__ uint32_t mod_u64_magic(uint64_t x, uint32_t n, uint32_t m,
+                                                  uint32_t t32) {
+    const uint32_t hi = mod_magic(uint32_t(x >> 32), n, m), lo = mod_magic(uint32_t(x), n, m);
+    return mod_magic(hi * t32 + lo, n, m);
+}
+
 // draw_pair with the next two Rng states already computed (la1 =
 // splitmix(r.s), la2 = splitmix(la1)), for n < 2^16; the caller recomputes the
 // look-ahead after every other draw, off the critical path.
 __device__ __forceinline__ void draw_pair_la(Rng& r, uint64_t la1, uint64_t la2, uint32_t n,
                                              uint32_t& pa, uint32_t& pb) {
-    const uint32_t t32 = (0xFFFFFFFFu % n + 1u) % n;
-    pa = mod_u64_small(la1, n, t32);
-    pb = mod_u64_small(la2, n, t32);
+    const uint32_t m = 0xFFFFFFFFu / n;
+    const uint32_t r1 = 0xFFFFFFFFu - m * n + 1u;  // (2^32 - 1) mod n, plus one
+    const uint32_t t32 = r1 == n ? 0u : r1;        // 2^32 mod n
+    pa = mod_u64_magic(la1, n, m, t32);
+    pb = mod_u64_magic(la2, n, m, t32);
     r.s = la2;
     int tries = 0;
     while (pb == pa && tries < 8) {
-        pb = mod_u64_small(r.next_u64(), n, t32);
+        pb = mod_u64_magic(r.next_u64(), n, m, t32);
         ++tries;
     }
 }
@@ -443,9 +466,9 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
         const float* xb = rows + size_t(sslot[ls + pb]) * dp;
         // margins of the positions this lane owns (lane + 32*i): the offset's
         // sequential sum and the dot products are independent chains, issued
-        // together: the first two groups always (a position past the node
-        // reads its last row, whose product is ignored), the next two only
-        // for nodes above 64 points
+        // together: the first group always, the second for nodes above 32
+        // points (a position past the node reads its last row, whose product
+        // is ignored), the next two only for nodes above 64 points
         float dots[SCAP / 32];
         float off;
         const uint32_t last = ln - 1;
@@ -454,12 +477,16 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
             // trip), built in the same pass as the offset
             float nvr[D];
             off = normal_offset_reg<D>(xa, xb, nvr);
+            dots[1] = dots[2] = dots[3] = 0.f;
+            if (ln > 32u) {
 #pragma unroll
-            for (int i = 0; i < 2; ++i) {
-                const uint32_t p = min(uint32_t(lane + 32 * i), last);
-                dots[i] = dot_reg<D>(nvr, rows + size_t(sslot[ls + p]) * dp);
+                for (int i = 0; i < 2; ++i) {
+                    const uint32_t p = min(uint32_t(lane + 32 * i), last);
+                    dots[i] = dot_reg<D>(nvr, rows + size_t(sslot[ls + p]) * dp);
+                }
+            } else {
+                dots[0] = dot_reg<D>(nvr, rows + size_t(sslot[ls + min(uint32_t(lane), last)]) * dp);
             }
-            dots[2] = dots[3] = 0.f;
             if (ln > 64u) {
 #pragma unroll
                 for (int i = 2; i < SCAP / 32; ++i) {
@@ -583,15 +610,12 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
                 } else {
                     dst = (c == 0 ? ln : S.tabB[c - 1]) - 1;
                 }
-                S.sid2[dst] = mid[i];
-                S.sslot2[dst] = msl[i];
+                // in place: every lane read its ids and slots before the
+                // barrier after the tables
+                sid[ls + dst] = mid[i];
+                sslot[ls + dst] = msl[i];
             }
             pre += __popc(mask[i]);
-        }
-        __syncwarp();
-        for (uint32_t p = lane; p < ln; p += 32) {
-            sid[ls + p] = S.sid2[p];
-            sslot[ls + p] = S.sslot2[p];
         }
         __syncwarp();
         uint32_t split = nL;
@@ -1073,6 +1097,7 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
     unsigned long long* tr = a.trace;
     const bool tb0 = tr && rt.size == tr[SEQ_T_ROOT0] && tid == 0;
     long long t_start = clock64(), tclk = 0;
+    const unsigned long long g_start = tr ? globaltimer_ns() : 0ull;
     if (tid == 0) {
         S.sp = 1;
         S.stS[0] = rt.start;
@@ -1125,6 +1150,18 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
         __syncthreads();
     }
     if (tb0) tr[SEQ_T_CYC_TOTAL] = clock64() - t_start;
+    if (tr && tid == 0) {
+        const unsigned long long g_end = globaltimer_ns();
+        if (NT == MCAP) {
+            if (blockIdx.x < unsigned(SEQ_T_BIG_N)) {
+                tr[SEQ_T_BIG + 2 * blockIdx.x] = g_start;
+                tr[SEQ_T_BIG + 2 * blockIdx.x + 1] = g_end;
+            }
+        } else {
+            atomicMax(&tr[SEQ_T_SMALL_T0], ~g_start);  // the earliest start, complemented
+            atomicMax(&tr[SEQ_T_SMALL_T1], g_end);
+        }
+    }
 }
 
 // Compact leaf starts of one tree: flags (u8) -> u32 -> exclusive scan -> positions.

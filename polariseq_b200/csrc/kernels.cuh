@@ -71,7 +71,12 @@ enum {
     SEQ_T_M_MARGIN = 25,      //   normal, offset, margins, sides
     SEQ_T_M_PART = 26,        //   partition
     SEQ_T_M_STAGE = 27,       //   staging ids and rows
-    SEQ_TRACE_N = 32
+    SEQ_T_SMALL_T0 = 28,      // 128-thread CTAs: earliest start (globaltimer ns)
+    SEQ_T_SMALL_T1 = 29,      //   latest end
+    SEQ_T_BIG = 32,           // 512-thread CTAs: start and end (globaltimer ns) of each of
+                              // the first SEQ_T_BIG_N, slots SEQ_T_BIG + 2 * block (+ 1)
+    SEQ_T_BIG_N = 148,
+    SEQ_TRACE_N = SEQ_T_BIG + 2 * SEQ_T_BIG_N
 };
 
 constexpr int FOREST_CHUNK = 2048;

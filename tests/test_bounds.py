@@ -71,3 +71,33 @@ def test_assignment_error_bound(offset):
         approx = tile_distance(u, w)
         err = 2 ** -7 * np.sqrt(exact) * (un + wn) + 2 ** -16 * (un + wn) ** 2 + 2 ** -18 * (un * un + wn * wn)
         assert abs(approx - exact) <= err, (approx, exact, err)
+
+
+def test_magic_remainder_of_the_warp_split_draws():
+    """The one-warp RP splits (polariseq_b200/csrc/forest.cu, draw_pair_la)
+    take x mod n for node sizes n < 2^16 from m = floor((2^32 - 1) / n):
+    q = floor(x m / 2^32) is floor(x / n) or one below, so one conditional
+    subtraction gives the remainder; a 64-bit draw is reduced as
+    ((hi mod n) * (2^32 mod n) + lo mod n) mod n.  Checked here against
+    Python's % for every n below 2^16 on edge and random 64-bit draws."""
+    rng = np.random.default_rng(7)
+    n = np.arange(2, 1 << 16, dtype=np.uint64)[:, None]
+    m = np.uint64(0xFFFFFFFF) // n
+    x = np.concatenate([
+        np.array([0, 1, 0xFFFFFFFF, 0x100000000, 0xFFFFFFFFFFFFFFFF], np.uint64),
+        rng.integers(0, 1 << 63, 27, dtype=np.uint64) * np.uint64(2)
+        + rng.integers(0, 2, 27, dtype=np.uint64)])[None, :]
+
+    def mod_magic(v):
+        r = v - ((v * m) >> np.uint64(32)) * n
+        return np.where(r >= n, r - n, r)
+
+    r1 = np.uint64(0xFFFFFFFF) - m * n + np.uint64(1)
+    t32 = np.where(r1 == n, np.uint64(0), r1)
+    assert np.array_equal(t32, np.uint64(1 << 32) % n)
+    lo32 = np.uint64(0xFFFFFFFF)
+    hi = mod_magic(x >> np.uint64(32))
+    lo = mod_magic(x & lo32)
+    got = mod_magic(hi * t32 + lo)
+    want = np.array([[int(xv) % int(nv) for xv in x[0]] for nv in n[:, 0]], np.uint64)
+    assert np.array_equal(got, want)
