@@ -5,6 +5,7 @@
 // 16-byte rows in HBM, then runs the plain form's phases on the context's
 // stream: RP forest, leaf pairs, random fill, rounds, extract.
 #include <cstdio>
+#include <cstring>
 #include <functional>
 
 #include "ctx.cuh"
@@ -378,11 +379,19 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
     fa.tabB = c->get<uint32_t>("tabB", TN);
     fa.leafflag = c->get<uint8_t>("leafflag", TN);
     fa.err = c->d_err;
-    const bool trace = std::getenv("POLARISEQ_TRACE") != nullptr;
+    // POLARISEQ_TRACE=timeline keeps only the subtree CTAs' start and end
+    // stamps (no counters, so the kernels run at their untraced speed)
+    const char* tv = std::getenv("POLARISEQ_TRACE");
+    const bool trace = tv != nullptr;
+    const bool timeline_only = trace && std::strcmp(tv, "timeline") == 0;
     fa.trace = nullptr;
+    fa.tl = nullptr;
+    unsigned long long* tbuf = nullptr;
     if (trace) {
-        fa.trace = c->get<unsigned long long>("seq_trace", SEQ_TRACE_N);
-        ck(cudaMemsetAsync(fa.trace, 0, SEQ_TRACE_N * 8, st), "trace");
+        tbuf = c->get<unsigned long long>("seq_trace", SEQ_TRACE_N);
+        ck(cudaMemsetAsync(tbuf, 0, SEQ_TRACE_N * 8, st), "trace");
+        fa.tl = tbuf;
+        if (!timeline_only) fa.trace = tbuf;
     }
     k_iota_trees<<<blocks(TN, 256), 256, 0, st>>>(fa.ids, n, T); count_launch();
     ck(cudaMemsetAsync(fa.leafflag, 0, TN, st), "memset leafflag");
@@ -460,7 +469,7 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
         KGScope kg(c, PQ_KG_SEQTREE);
         uint32_t n_big = 0;
         while (n_big < roots.size() && n_big < 148 && roots[n_big].size > 65536) ++n_big;
-        if (trace) {
+        if (fa.trace) {
             uint64_t r0 = roots.empty() ? 0 : roots[0].size;
             ck(cudaMemcpyAsync(fa.trace + SEQ_T_ROOT0, &r0, 8, cudaMemcpyHostToDevice, st), "tr");
         }
@@ -478,7 +487,7 @@ uint64_t build_plain(pq_ctx* c, const float* data, bool data_on_host, uint64_t n
     S.ms_forest = tm.stop();
     if (trace) {
         unsigned long long h[SEQ_TRACE_N];
-        ck(cudaMemcpy(h, fa.trace, sizeof(h), cudaMemcpyDeviceToHost), "trace");
+        ck(cudaMemcpy(h, tbuf, sizeof(h), cudaMemcpyDeviceToHost), "trace");
         std::fprintf(stderr,
                      "[nndescent] rp-forest build (%u trees, leaf %llu): %.2f ms; %zu subtree "
                      "roots, largest %llu\n",

@@ -268,6 +268,10 @@ constexpr int SCAP = 128;   // staged capacity (points): 4 per lane of warp 0
 // points take one point per thread, the smaller ones go to warp 0.
 constexpr int MCAP = 512;
 
+// Shared state of one subtree CTA; CAP staged points (MCAP in 512-thread
+// CTAs, which stage whole subtrees of up to 512 points, SCAP otherwise: the
+// smaller CTAs never stage more, and hold 7 KB instead of 17 KB).
+template <int CAP>
 struct SeqShared {
     uint32_t stS[STK], stN[STK];
     uint16_t stD[STK];
@@ -275,9 +279,9 @@ struct SeqShared {
     uint16_t lD[STK];
     uint32_t mS[STK], mN[STK];
     uint16_t mD[STK];
-    uint32_t sid[MCAP], sslot[MCAP], sid2[MCAP], sslot2[MCAP];
-    uint8_t code[MCAP];
-    uint32_t tabA[MCAP], tabB[MCAP];
+    uint32_t sid[CAP], sslot[CAP], sid2[CAP], sslot2[CAP];
+    uint8_t code[CAP];
+    uint32_t tabA[CAP], tabB[CAP];
     uint32_t ws[32];
     uint64_t rng;
     float off;
@@ -420,8 +424,8 @@ __device__ __forceinline__ void draw_pair_la(Rng& r, uint64_t la1, uint64_t la2,
 
 // Warp 0 finishes a staged subtree: local positions [0, n0) of the staged
 // ids/slots, rows in `rows` (slot-indexed), normal in `nv`.
-template <int D>
-__device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* sid, uint32_t* sslot,
+template <int D, class SS>
+__device__ uint32_t warp_subtree(const ForestArgs& a, SS& S, uint32_t* sid, uint32_t* sslot,
                                  float* rows, float* nv, uint32_t st, uint32_t n0, uint32_t dep0,
                                  Rng& rng, uint8_t* leaf, bool tb0 = false) {
     const int lane = threadIdx.x & 31;
@@ -661,8 +665,8 @@ __device__ uint32_t warp_subtree(const ForestArgs& a, SeqShared& S, uint32_t* si
 // [st, st + sz) of `ids`, with the per-tree scratch arrays tmp / side / tabA /
 // tabB at the same positions.  Every thread holds the same Rng.  Returns the
 // split point.
-template <int NT, int D>
-__device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t* tmp,
+template <int NT, int D, class SS>
+__device__ uint32_t split_node(const ForestArgs& a, SS& S, uint32_t* ids, uint32_t* tmp,
                                uint8_t* side, uint32_t* tabA, uint32_t* tabB, uint32_t st,
                                uint32_t sz, Rng& rng, float* nv, float* xab, bool tb0,
                                long long& tclk) {
@@ -839,8 +843,8 @@ __device__ uint32_t split_node(const ForestArgs& a, SeqShared& S, uint32_t* ids,
 // sid/sslot, rows in shared memory), one point per thread: the same draws,
 // margins, tie draws, closed-form partition and random split as the
 // global-mode split.  Returns the split point.
-template <int NT, int D>
-__device__ uint32_t cta_split(const ForestArgs& a, SeqShared& S, uint32_t* sid, uint32_t* sslot,
+template <int NT, int D, class SS>
+__device__ uint32_t cta_split(const ForestArgs& a, SS& S, uint32_t* sid, uint32_t* sslot,
                               uint32_t m, Rng& rng, float* rows, float* nv, bool tb0) {
     const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
     const int d = a.d, dp = a.dp;
@@ -962,8 +966,8 @@ __device__ uint32_t cta_split(const ForestArgs& a, SeqShared& S, uint32_t* sid, 
 // rows are staged once; its nodes of more than SCAP points are split by the
 // whole CTA (cta_split), the smaller ones finished by warp 0; the ids come
 // back in tree order.  `gpos` is its first position in the tree.
-template <int NT, int D>
-__device__ void mid_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t gpos,
+template <int NT, int D, class SS>
+__device__ void mid_subtree(const ForestArgs& a, SS& S, uint32_t* ids, uint32_t gpos,
                             uint32_t sz, uint32_t dep, Rng& rng, float* rows, float* nv,
                             uint8_t* leaf, bool tb0) {
     const int tid = threadIdx.x;
@@ -1040,8 +1044,8 @@ __device__ void mid_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, ui
 // A staged subtree of at most smax points: ids[0, sz) with their rows in
 // shared memory, finished by warp 0; the ids come back in tree order.  `gpos`
 // is its first position in the tree (for the leaf flags).
-template <int NT, int D>
-__device__ void staged_subtree(const ForestArgs& a, SeqShared& S, uint32_t* ids, uint32_t gpos,
+template <int NT, int D, class SS>
+__device__ void staged_subtree(const ForestArgs& a, SS& S, uint32_t* ids, uint32_t gpos,
                                uint32_t sz, uint32_t dep, Rng& rng, float* rows, float* nv,
                                uint8_t* leaf, bool tb0) {
     const int tid = threadIdx.x;
@@ -1080,7 +1084,7 @@ template <int NT, int D>
 __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots, int smax,
                                                 int trows) {
     extern __shared__ __align__(16) float dyn[];
-    __shared__ SeqShared S;
+    __shared__ SeqShared<NT == MCAP ? MCAP : SCAP> S;
     float* nv = dyn;                 // dp
     float* xab = dyn + a.dp;         // 2 * dp: the two hyperplane rows
     float* rows = dyn + 3 * a.dp;    // max(smax, trows) * dp: staged subtrees
@@ -1097,7 +1101,7 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
     unsigned long long* tr = a.trace;
     const bool tb0 = tr && rt.size == tr[SEQ_T_ROOT0] && tid == 0;
     long long t_start = clock64(), tclk = 0;
-    const unsigned long long g_start = tr ? globaltimer_ns() : 0ull;
+    const unsigned long long g_start = a.tl ? globaltimer_ns() : 0ull;
     if (tid == 0) {
         S.sp = 1;
         S.stS[0] = rt.start;
@@ -1114,11 +1118,13 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
             __syncthreads();
             continue;
         }
-        if (NT == MCAP && trows >= MCAP && sz > uint32_t(smax) && sz <= uint32_t(MCAP)) {
-            if (tb0) tclk = clock64();
-            mid_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf, tb0);
-            if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
-            continue;
+        if constexpr (NT == MCAP) {
+            if (trows >= MCAP && sz > uint32_t(smax) && sz <= uint32_t(MCAP)) {
+                if (tb0) tclk = clock64();
+                mid_subtree<NT, D>(a, S, ids + st, st, sz, dep, rng, rows, nv, leaf, tb0);
+                if (tb0) tr[SEQ_T_CYC_STAGED] += clock64() - tclk;
+                continue;
+            }
         }
         if (sz <= uint32_t(smax)) {
             if (tb0) tclk = clock64();
@@ -1150,16 +1156,17 @@ __global__ void __launch_bounds__(NT) k_seqtree(ForestArgs a, const SRoot* roots
         __syncthreads();
     }
     if (tb0) tr[SEQ_T_CYC_TOTAL] = clock64() - t_start;
-    if (tr && tid == 0) {
+    if (a.tl && tid == 0) {
+        unsigned long long* tl = a.tl;
         const unsigned long long g_end = globaltimer_ns();
         if (NT == MCAP) {
             if (blockIdx.x < unsigned(SEQ_T_BIG_N)) {
-                tr[SEQ_T_BIG + 2 * blockIdx.x] = g_start;
-                tr[SEQ_T_BIG + 2 * blockIdx.x + 1] = g_end;
+                tl[SEQ_T_BIG + 2 * blockIdx.x] = g_start;
+                tl[SEQ_T_BIG + 2 * blockIdx.x + 1] = g_end;
             }
         } else {
-            atomicMax(&tr[SEQ_T_SMALL_T0], ~g_start);  // the earliest start, complemented
-            atomicMax(&tr[SEQ_T_SMALL_T1], g_end);
+            atomicMax(&tl[SEQ_T_SMALL_T0], ~g_start);  // the earliest start, complemented
+            atomicMax(&tl[SEQ_T_SMALL_T1], g_end);
         }
     }
 }
@@ -1372,6 +1379,9 @@ void launch_seqtrees(const ForestArgs& a, const SRoot* roots, uint32_t n_big, ui
     int smax = int(std::min<size_t>(SCAP, (28 * 1024) / row));
     if (smax < 2) smax = 0;
     // roots[0, n_big) are the largest subtrees: 512 threads each, own stream
+    // (64-thread CTAs for the rest, six per SM instead of four, took 1065
+    // instead of 926 ms per 4M build: their global-mode nodes slow down more
+    // than the extra CTAs gain)
     if (a.d == 50) {
         seqtree_launch<512, 50>(a, roots, n_big, smax, st_big);
         seqtree_launch<128, 50>(a, roots + n_big, nr - n_big, smax, st);

@@ -40,6 +40,7 @@ struct ForestArgs {
     uint8_t* leafflag;   // T x n: 1 where a leaf starts
     int* err;            // device error flag
     unsigned long long* trace;  // optional: SEQ_TRACE_N counters (POLARISEQ_TRACE)
+    unsigned long long* tl;     // optional: the same buffer, for the CTA timeline stamps only
 };
 
 // Trace counters of the depth-first subtree kernel.
